@@ -1,0 +1,135 @@
+/*
+ * phox.h : C ABI of the B200 optical-photon engine (drop-in for the Opticks simulate path).
+ *
+ * All entry points return 0 on success and a negative code on failure; phx_last_error()
+ * gives the message of the last failure on the calling thread.  No C++ exception crosses
+ * this boundary.  Arrays are plain pointers with the Opticks byte layouts (see
+ * opticks_b200/csrc/phx_pod.h).  One engine per device; calls on one engine are serialised
+ * by the caller (the reference uses a process-wide singleton per GPU: QSim::INSTANCE,
+ * CSGOptiX::INSTANCE).
+ *
+ * Reference interfaces replaced (paths within simoncblyth/opticks):
+ *   phx_create            CSGOptiX::Create            CSGOptiX/CSGOptiX.cc:349
+ *                         QSim::UploadComponents      qudarap/QSim.cc:119-262
+ *                         CSGFoundry::upload          CSG/CSGFoundry.cc:3392
+ *   phx_simulate          CSGOptiX::simulate(gs,eid)  CSGOptiX/CSGOptiX.cc:780
+ *                         (python twin _CSGOptiXService.simulate  CSGOptiX/opticks_CSGOptiX.cc:24-110)
+ *   phx_simulate_device   SSimulator::simulate_launch sysrap/SSimulator.h:16-37,
+ *                         CSGOptiX::launch            CSGOptiX/CSGOptiX.cc:1091-1190
+ *   phx_count_photons     SGenstep::GetNumPhoton / QEvt::setGenstepUpload  qudarap/QEvt.cc:199-330
+ *   phx_csg_scan[_device] CSGScan / _CSGScan_intersect  CSG/CSGScan.cc:29-130, CSG/CSGScan.cu:11-25
+ *   phx_rng_sequence      QSim::rng_sequence          qudarap/QSim.cc:1070-1168, qudarap/QSim.cu:43-68
+ *   phx_simulate_batched  (no counterpart: the reference loops QSim::simulate per event,
+ *                          qudarap/QSim.cc:436-595)
+ *   phx_adjoint_device    (no counterpart: score-function gradients of expected hits)
+ *   phx_destroy           CSGOptiX / QSim teardown
+ */
+#ifndef PHOX_H
+#define PHOX_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct phx_engine phx_engine;
+
+/* CSGFoundry arrays (CSG/CSGFoundry.cc:2978-3016 load) */
+typedef struct {
+    const float*   node;  int32_t num_node;   /* (num_node,4,4)  CSGNode  */
+    const float*   prim;  int32_t num_prim;   /* (num_prim,4,4)  CSGPrim  */
+    const int32_t* solid; int32_t num_solid;  /* (num_solid,3,4) CSGSolid */
+    const float*   inst;  int32_t num_inst;   /* (num_inst,4,4)  qat4 instance transforms; the .w
+                                                 column holds ins_idx, gas_idx, sensor_identifier+1,
+                                                 sensor_index as int32 (sysrap/sqat4.h:345-389) */
+    const float*   itra;  int32_t num_itra;   /* (num_itra,4,4)  inverse node transforms */
+    const float*   plan;  int32_t num_plan;   /* (num_plan,4)    planes (convexpolyhedron) */
+} phx_geometry;
+
+/* SSim standard arrays: bnd (qudarap/QBnd.cc:130-165), optical (sysrap/sstandard.h:311-420),
+ * scintillation inverse CDF (qudarap/QScint.cc:84-120) */
+typedef struct {
+    const float*    bnd;      int32_t num_bnd;  int32_t num_wl;   /* (num_bnd,4,2,num_wl,4) */
+    float           wl_low;   float   wl_step;                    /* nm : 60, 1 */
+    const uint32_t* optical;                                      /* (num_bnd*4,4) */
+    const float*    icdf;     int32_t icdf_layers; int32_t icdf_width; int32_t hd_factor; /* (3,4096,1), 20 */
+} phx_physics;
+
+/* SEventConfig defaults (sysrap/SEventConfig.cc:40-110) */
+typedef struct {
+    uint64_t seed;                    /* curand_init seed                          0 */
+    uint64_t offset;                  /* curand_init offset                        0 */
+    uint64_t skipahead_event_offset;  /* OPTICKS_EVENT_SKIPAHEAD             100000 */
+    int64_t  max_photon;              /* RNG state slots prepared at create  1000000 */
+    int32_t  max_bounce;              /* OPTICKS_MAX_BOUNCE                       31 */
+    float    max_time;                /* OPTICKS_MAX_TIME (ns)                 1e27 */
+    float    propagate_epsilon;       /* OPTICKS_PROPAGATE_EPSILON (mm)        0.05 */
+    float    propagate_epsilon0;      /* OPTICKS_PROPAGATE_EPSILON0 (mm)       0.05 */
+    uint32_t epsilon0_mask;           /* OPTICKS_PROPAGATE_EPSILON0_MASK  TO,CK,SI,SC,RE */
+    uint32_t hit_mask;                /* OPTICKS_HIT_MASK                          SD */
+    int32_t  root_polish;             /* FP64 polish of quadratic leaf roots       0 */
+    int32_t  num_sensor;              /* length of the per-sensor hit count output 0 */
+} phx_config;
+
+typedef struct {
+    float*    photon;       /* (num_photon,4,4) sphoton, or NULL */
+    uint64_t* seq;          /* (num_photon,2,2) seqhis[2],seqbnd[2], or NULL */
+    float*    hit;          /* (hit_capacity,4,4) sphoton of selected photons in photon order, or NULL */
+    int64_t   hit_capacity;
+    uint32_t* sensor_hits;  /* (num_sensor) hits per sensor (identity-1), or NULL */
+    int64_t   num_photon;   /* out */
+    int64_t   num_hit;      /* out : hits selected (may exceed hit_capacity; then status has HIT_OVERFLOW) */
+    uint32_t  status;       /* out : PHX_STATUS_* bits */
+} phx_outputs;
+
+void        phx_config_default(phx_config* cfg);
+const char* phx_last_error(void);
+const char* phx_version(void);
+
+int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_config* cfg, int device, phx_engine** out);
+int phx_destroy(phx_engine* e);
+
+/* sum of quad6 q0.w photon counts */
+int64_t phx_count_photons(const float* gensteps, int32_t num_genstep);
+
+/* host arrays in, host arrays out: gensteps (num_genstep,6,4) */
+int phx_simulate(phx_engine* e, const float* gensteps, int32_t num_genstep, int32_t event_index, phx_outputs* out);
+
+/* device arrays in and out (pointers in *out are device pointers); stream is a cudaStream_t or NULL.
+ * num_photon must equal the sum of the genstep photon counts.  photon_offset is the absolute index of
+ * the first photon (its RNG slot and sphoton.index), as params.photon_slot_offset of a genstep slice
+ * launch (CSGOptiX/CSGOptiX7.cu:441); outputs still start at 0.  num_hit/status are returned to the host. */
+int phx_simulate_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                        int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream);
+
+/* many events in one persistent launch: gensteps (num_genstep,6,4) with genstep_event[g] the event index
+ * of genstep g (non-decreasing).  Outputs are the concatenation of the events' photons in genstep order;
+ * event_photon_offset (num_event+1) receives the photon offsets of the events (host array). */
+int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const int32_t* d_genstep_event,
+                                int32_t num_genstep, int64_t num_photon, int32_t block, int32_t chunk,
+                                int32_t regroup, phx_outputs* d_out, void* stream);
+
+/* ray scan against one CSGPrim (CSGScan): rays SoA (6,n) = ox,oy,oz,dx,dy,dz ;
+ * isect (n,4) = normal.xyz, t (t=0 for a miss) */
+int phx_csg_scan(phx_engine* e, int32_t prim, float t_min, const float* rays, int64_t n, float* isect);
+int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d_rays, int64_t n, float* d_isect,
+                        int32_t polish, void* stream);
+
+/* per-photon uniform streams (QSim::rng_sequence): out (num_photon, num_per_photon) float32,
+ * photon slots photon_offset..photon_offset+num_photon-1 advanced by the event skipahead */
+int phx_rng_sequence(phx_engine* e, int32_t event_index, int64_t photon_offset, int64_t num_photon,
+                     int32_t num_per_photon, float* out);
+
+/* score-function adjoint of the expected hits per sensor.  theta (32) = absorption length,
+ * Rayleigh length, reemission probability, refractive index in 8 wavelength bins of the
+ * material line mat_line over [wl_lo, wl_hi).  Runs the forward pass with those properties
+ * and accumulates grad (num_sensor,32) = sum over hits of d log p(path)/d theta, and
+ * hits (num_sensor).  All pointers are device pointers. */
+int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                       int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
+                       float* d_hits, float* d_grad, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

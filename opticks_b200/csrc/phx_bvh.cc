@@ -1,0 +1,226 @@
+// phx_bvh.cc : host builder of the 4-wide BVH that replaces the OptiX IAS/GAS.
+//
+// The reference hands one AABB per CSGPrim to OptiX (CSGOptiX/GAS_Builder.cc:112-130) and
+// one instance per qat4 transform (CSGOptiX/SBT.cc:393-460); OptiX builds the hierarchy.
+// Here every (instance, prim) pair becomes one leaf with a world-space box, a binned-SAH
+// binary BVH is built over the leaves and collapsed to 4-wide nodes whose child boxes are
+// stored per axis (phx_bvh4_node) so the traversal tests four boxes with coalesced loads.
+// Boxes are padded so that FP32 slab tests never cull a leaf that the CSG intersector hits.
+#include "phx_bvh.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace {
+
+struct Box {
+    double lo[3], hi[3];
+    Box() { for (int k = 0; k < 3; k++) { lo[k] = std::numeric_limits<double>::infinity(); hi[k] = -std::numeric_limits<double>::infinity(); } }
+    void grow(const Box& b) { for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); } }
+    void grow(const double* p) { for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); } }
+    bool empty() const { return !(lo[0] <= hi[0]); }
+    double area() const
+    {
+        if (empty()) return 0.0;
+        double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        return 2.0 * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Node2 {
+    Box box;
+    int left = -1, right = -1;  // inner: children ; leaf: left=-1
+    int first = 0, count = 0;   // leaf range in the reordered leaf list
+};
+
+struct Builder {
+    std::vector<Box> boxes;
+    std::vector<double> cent;   // 3 per leaf
+    std::vector<int> idx;
+    std::vector<Node2> nodes;
+    int max_leaf = 4;
+
+    int build(int first, int count, int depth)
+    {
+        Node2 n;
+        for (int i = first; i < first + count; i++) n.box.grow(boxes[idx[i]]);
+        int me = (int)nodes.size();
+        nodes.push_back(n);
+        if (count <= 1 || depth > 60) { nodes[me].first = first; nodes[me].count = count; return me; }
+        // centroid bounds
+        Box cb;
+        for (int i = first; i < first + count; i++) cb.grow(&cent[3 * idx[i]]);
+        const int NB = 16;
+        double best_cost = std::numeric_limits<double>::infinity();
+        int best_axis = -1, best_split = -1;
+        for (int ax = 0; ax < 3; ax++) {
+            double lo = cb.lo[ax], hi = cb.hi[ax];
+            if (!(hi > lo)) continue;
+            Box bb[NB]; int bc[NB] = {0};
+            double scale = NB / (hi - lo);
+            for (int i = first; i < first + count; i++) {
+                int b = (int)((cent[3 * idx[i] + ax] - lo) * scale);
+                b = std::min(NB - 1, std::max(0, b));
+                bc[b]++; bb[b].grow(boxes[idx[i]]);
+            }
+            Box lb[NB]; int lc[NB];
+            Box acc; int ac = 0;
+            for (int b = 0; b < NB; b++) { acc.grow(bb[b]); ac += bc[b]; lb[b] = acc; lc[b] = ac; }
+            Box racc; int rc = 0;
+            for (int b = NB - 1; b > 0; b--) {
+                racc.grow(bb[b]); rc += bc[b];
+                int lcount = lc[b - 1];
+                if (lcount == 0 || rc == 0) continue;
+                double cost = lb[b - 1].area() * lcount + racc.area() * rc;
+                if (cost < best_cost) { best_cost = cost; best_axis = ax; best_split = b; }
+            }
+        }
+        double leaf_cost = nodes[me].box.area() * count;
+        if (best_axis < 0 || (count <= max_leaf && best_cost >= leaf_cost)) {
+            if (count <= max_leaf || best_axis < 0) {
+                if (count > max_leaf) {
+                    // all centroids coincide: split the range in the middle
+                    int half = count / 2;
+                    int l = build(first, half, depth + 1);
+                    int r = build(first + half, count - half, depth + 1);
+                    nodes[me].left = l; nodes[me].right = r;
+                    return me;
+                }
+                nodes[me].first = first; nodes[me].count = count;
+                return me;
+            }
+        }
+        double lo = cb.lo[best_axis], hi = cb.hi[best_axis];
+        double scale = NB / (hi - lo);
+        int* mid = std::partition(idx.data() + first, idx.data() + first + count, [&](int i) {
+            int b = (int)((cent[3 * i + best_axis] - lo) * scale);
+            b = std::min(NB - 1, std::max(0, b));
+            return b < best_split;
+        });
+        int lcount = (int)(mid - (idx.data() + first));
+        if (lcount == 0 || lcount == count) lcount = count / 2;
+        int l = build(first, lcount, depth + 1);
+        int r = build(first + lcount, count - lcount, depth + 1);
+        nodes[me].left = l; nodes[me].right = r;
+        return me;
+    }
+};
+
+inline bool is_leaf(const Node2& n) { return n.left < 0; }
+
+void set_child(phx_bvh4_node& out, int c, const Box& b, int child)
+{
+    out.lo_x[c] = (float)b.lo[0]; out.hi_x[c] = (float)b.hi[0];
+    out.lo_y[c] = (float)b.lo[1]; out.hi_y[c] = (float)b.hi[1];
+    out.lo_z[c] = (float)b.lo[2]; out.hi_z[c] = (float)b.hi[2];
+    out.child[c] = child;
+}
+
+void set_empty(phx_bvh4_node& out, int c)
+{
+    out.lo_x[c] = out.lo_y[c] = out.lo_z[c] = 1e30f;
+    out.hi_x[c] = out.hi_y[c] = out.hi_z[c] = -1e30f;
+    out.child[c] = 0;
+}
+
+}  // namespace
+
+// corners of the prim box mapped to world by a row-vector 4x4 (rows q0..q3), in double
+static Box world_box(const float* bb6, const float* m)
+{
+    Box b;
+    for (int i = 0; i < 8; i++) {
+        double p[3] = { (i & 1) ? bb6[3] : bb6[0], (i & 2) ? bb6[4] : bb6[1], (i & 4) ? bb6[5] : bb6[2] };
+        double w[3];
+        for (int k = 0; k < 3; k++) w[k] = m[0 * 4 + k] * p[0] + m[1 * 4 + k] * p[1] + m[2 * 4 + k] * p[2] + m[3 * 4 + k];
+        b.grow(w);
+    }
+    return b;
+}
+
+int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out)
+{
+    const int n = (int)in.size();
+    out.nodes.clear();
+    out.leaves.clear();
+    out.leaf_count = n;
+    Builder B;
+    B.boxes.resize(n);
+    B.cent.resize(3 * (size_t)n);
+    B.idx.resize(n);
+    for (int i = 0; i < n; i++) {
+        Box b = world_box(in[i].bbox, in[i].xform);
+        // pad: relative to extent and to coordinate magnitude so FP32 slabs stay conservative
+        double ext = std::max(b.hi[0] - b.lo[0], std::max(b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]));
+        double mag = 0.0;
+        for (int k = 0; k < 3; k++) mag = std::max(mag, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
+        double pad = 1e-4 * ext + 4e-6 * mag + 1e-3;
+        for (int k = 0; k < 3; k++) { b.lo[k] -= pad; b.hi[k] += pad; }
+        B.boxes[i] = b;
+        for (int k = 0; k < 3; k++) B.cent[3 * i + k] = 0.5 * (b.lo[k] + b.hi[k]);
+        B.idx[i] = i;
+    }
+    if (n == 0) return 0;
+    B.nodes.reserve(2 * (size_t)n);
+    int root2 = B.build(0, n, 0);
+    // reorder leaves
+    out.leaves.resize(n);
+    for (int i = 0; i < n; i++) out.leaves[i] = in[B.idx[i]].leaf;
+
+    // collapse to 4-wide. Each BVH2 inner node becomes one BVH4 node whose children are
+    // the up-to-4 descendants obtained by opening the largest inner child.
+    struct Item { int n2; int n4; };
+    std::vector<Item> work;
+    auto leaf_child = [&](const Node2& nd) { return -(1 + ((nd.first << 3) | (std::max(1, nd.count) - 1))); };
+    // a root that is a leaf is wrapped in one BVH4 node with a single child
+    out.nodes.push_back(phx_bvh4_node());
+    std::memset(&out.nodes[0], 0, sizeof(phx_bvh4_node));
+    work.push_back({ root2, 0 });
+    while (!work.empty()) {
+        Item it = work.back(); work.pop_back();
+        const Node2& nd = B.nodes[it.n2];
+        int kids[4]; int nk = 0;
+        if (is_leaf(nd)) { kids[nk++] = it.n2; }
+        else {
+            kids[nk++] = nd.left; kids[nk++] = nd.right;
+            while (nk < 4) {
+                int best = -1; double ba = -1.0;
+                for (int k = 0; k < nk; k++) {
+                    const Node2& c = B.nodes[kids[k]];
+                    if (!is_leaf(c) && c.box.area() > ba) { ba = c.box.area(); best = k; }
+                }
+                if (best < 0) break;
+                const Node2& c = B.nodes[kids[best]];
+                kids[best] = c.left;
+                kids[nk++] = c.right;
+            }
+        }
+        phx_bvh4_node& o4 = out.nodes[it.n4];
+        for (int c = 0; c < 4; c++) {
+            if (c >= nk) { set_empty(out.nodes[it.n4], c); continue; }
+            const Node2& cn = B.nodes[kids[c]];
+            if (is_leaf(cn)) {
+                if (cn.count > 8) return -1;   // leaf ranges hold at most 8
+                set_child(out.nodes[it.n4], c, cn.box, leaf_child(cn));
+            } else {
+                int idx4 = (int)out.nodes.size();
+                out.nodes.push_back(phx_bvh4_node());
+                std::memset(&out.nodes.back(), 0, sizeof(phx_bvh4_node));
+                set_child(out.nodes[it.n4], c, cn.box, idx4);
+                work.push_back({ kids[c], idx4 });
+            }
+        }
+        (void)o4;
+    }
+    // depth for the traversal stack bound
+    std::vector<int> depth(out.nodes.size(), 0);
+    int maxd = 0;
+    for (size_t i = 0; i < out.nodes.size(); i++)
+        for (int c = 0; c < 4; c++) {
+            int ch = out.nodes[i].child[c];
+            if (ch > 0) { depth[ch] = depth[i] + 1; maxd = std::max(maxd, depth[ch]); }
+        }
+    out.max_depth = maxd;
+    return 0;
+}

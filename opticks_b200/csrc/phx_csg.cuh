@@ -1,0 +1,557 @@
+// phx_csg.cuh : ray intersection with one CSG prim (a complete binary tree of CSGNode).
+//
+// Semantics follow the reference's IS path:
+//   intersect_prim  CSG/csg_intersect_tree.h:684-719
+//   intersect_tree  CSG/csg_intersect_tree.h:277-672  (Kensler single-hit CSG over a postorder
+//                   walk of the complete tree, re-walking sub-trees from an advanced tmin)
+//   intersect_leaf  CSG/csg_intersect_leaf.h:175-300  (node transform, normal back-transform,
+//                   complement signalled by the sign of isect.x)
+//   leaves          sphere  CSG/csg_intersect_leaf_sphere.h:15-40
+//                   zsphere CSG/csg_intersect_leaf_zsphere.h:45-153
+//                   cylinder CSG/csg_intersect_leaf_cylinder.h:34-95
+//                   box3    CSG/csg_intersect_leaf_box3.h:64-157
+//                   roots   CSG/csg_robust_quadratic_roots.h:95-122
+// The torus leaf has no counterpart in the current reference intersector; it is a new FP64
+// quartic solve (monotone-interval Newton/bisection) written for this engine.
+//
+// The node table is read through the read-only data path; nodes are 64 B (4 x float4).
+#pragma once
+#include "phx_vec.cuh"
+#include "phx_pod.h"
+
+#define PHX_CSG_STACK 15
+#define PHX_TRANCHE_STACK 4
+#define PHX_CSG_PROPAGATE_EPSILON 0.0001f
+
+enum { PHX_CSG_ERR_OVERFLOW = 1, PHX_CSG_ERR_POP_EMPTY = 2, PHX_CSG_ERR_XOR_SIDE = 4,
+       PHX_CSG_ERR_END_EMPTY = 8, PHX_CSG_ERR_TRANCHE = 16 };
+
+enum { PHX_STATE_ENTER = 0, PHX_STATE_EXIT = 1, PHX_STATE_MISS = 2 };
+enum { PHX_CTRL_RETURN_MISS = 0, PHX_CTRL_RETURN_A = 1, PHX_CTRL_RETURN_B = 2,
+       PHX_CTRL_RETURN_FLIP_B = 3, PHX_CTRL_LOOP_A = 4, PHX_CTRL_LOOP_B = 5 };
+
+// Kensler's single-hit boolean action table, resolved for "A closer" and "B closer".
+// Each operation maps (stateA, stateB) to an action; the eight non-miss/miss pairs are
+// packed four bits each at offset 3*stateA+stateB.  The values are generated from the rules
+// of the paper in phx_csg_ctrl() below and checked against this packing on the host.
+struct PhxCsgRules {
+    // returns the action for op in {1:union,2:intersection,3:difference}
+    static __host__ __device__ constexpr int ctrl(int op, int a, int b, bool aCloser)
+    {
+        // union
+        return op == PHX_CSG_UNION ? (
+                   a == PHX_STATE_ENTER && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_RETURN_B) :
+                   a == PHX_STATE_ENTER && b == PHX_STATE_EXIT  ? (aCloser ? PHX_CTRL_LOOP_A : PHX_CTRL_RETURN_B) :
+                   a == PHX_STATE_EXIT  && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_LOOP_B) :
+                   a == PHX_STATE_EXIT  && b == PHX_STATE_EXIT  ? (aCloser ? PHX_CTRL_RETURN_B : PHX_CTRL_RETURN_A) :
+                   a == PHX_STATE_MISS  && b == PHX_STATE_MISS  ? PHX_CTRL_RETURN_MISS :
+                   b == PHX_STATE_MISS ? PHX_CTRL_RETURN_A : PHX_CTRL_RETURN_B )
+             : op == PHX_CSG_INTERSECTION ? (
+                   a == PHX_STATE_MISS || b == PHX_STATE_MISS ? PHX_CTRL_RETURN_MISS :
+                   a == PHX_STATE_ENTER && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_LOOP_A : PHX_CTRL_LOOP_B) :
+                   a == PHX_STATE_ENTER && b == PHX_STATE_EXIT  ? (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_LOOP_B) :
+                   a == PHX_STATE_EXIT  && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_LOOP_A : PHX_CTRL_RETURN_B) :
+                   (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_RETURN_B) )
+             : /* difference A - B */ (
+                   a == PHX_STATE_MISS ? PHX_CTRL_RETURN_MISS :
+                   b == PHX_STATE_MISS ? PHX_CTRL_RETURN_A :
+                   a == PHX_STATE_ENTER && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_LOOP_B) :
+                   a == PHX_STATE_ENTER && b == PHX_STATE_EXIT  ? (aCloser ? PHX_CTRL_LOOP_A : PHX_CTRL_LOOP_B) :
+                   a == PHX_STATE_EXIT  && b == PHX_STATE_ENTER ? (aCloser ? PHX_CTRL_RETURN_A : PHX_CTRL_RETURN_FLIP_B) :
+                   (aCloser ? PHX_CTRL_LOOP_A : PHX_CTRL_RETURN_FLIP_B) );
+    }
+    static __host__ __device__ constexpr unsigned packed(int op, bool aCloser)
+    {
+        return  (unsigned)ctrl(op, 0, 0, aCloser)       | (unsigned)ctrl(op, 0, 1, aCloser) << 4
+              | (unsigned)ctrl(op, 0, 2, aCloser) << 8  | (unsigned)ctrl(op, 1, 0, aCloser) << 12
+              | (unsigned)ctrl(op, 1, 1, aCloser) << 16 | (unsigned)ctrl(op, 1, 2, aCloser) << 20
+              | (unsigned)ctrl(op, 2, 0, aCloser) << 24 | (unsigned)ctrl(op, 2, 1, aCloser) << 28;
+    }
+};
+
+PHX_D int phx_csg_lookup(int op, int sa, int sb, bool aCloser)
+{
+    // the packed words are compile-time constants; one shift+mask per combine
+    const unsigned wA = op == PHX_CSG_UNION ? PhxCsgRules::packed(1, true)
+                      : op == PHX_CSG_INTERSECTION ? PhxCsgRules::packed(2, true) : PhxCsgRules::packed(3, true);
+    const unsigned wB = op == PHX_CSG_UNION ? PhxCsgRules::packed(1, false)
+                      : op == PHX_CSG_INTERSECTION ? PhxCsgRules::packed(2, false) : PhxCsgRules::packed(3, false);
+    const unsigned w = aCloser ? wA : wB;
+    const unsigned off = 3u * (unsigned)sa + (unsigned)sb;
+    return off < 8u ? (int)((w >> (off * 4u)) & 0xfu) : PHX_CTRL_RETURN_MISS;
+}
+
+struct PhxCsgCtx {
+    const float4* node;   // (Nn*4) float4 : CSGNode table
+    const float4* itra;   // (Nt*4) float4 : inverse node transforms
+    int polish;           // 1: FP64 root polish in quadratic leaves
+};
+
+PHX_D unsigned nd_u(const float4& q, int k) { return __float_as_uint(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w); }
+
+// ---------------------------------------------------------------- quadratic roots
+// Solve d t^2 + 2 b t + c = 0 choosing the form of each root that avoids cancellation.
+PHX_D void robust_roots(float& t1, float& t2, float& disc, float& sdisc, const float d, const float b, const float c)
+{
+    disc = b * b - d * c;
+    sdisc = disc > 0.f ? sqrtf(disc) : 0.f;
+    float q = b > 0.f ? -(b + sdisc) : -(b - sdisc);
+    float root1 = q / d;
+    float root2 = c / q;
+    t1 = fminf(root1, root2);
+    t2 = fmaxf(root1, root2);
+}
+PHX_D void robust_roots_disq(const float t_min, float& t1, float& t2, float& disc, float& sdisc, const float d, const float b, const float c)
+{
+    disc = b * b - d * c;
+    sdisc = disc > 0.f ? sqrtf(disc) : 0.f;
+    float q = b > 0.f ? -(b + sdisc) : -(b - sdisc);
+    float root1 = sdisc > 0.f ? q / d : t_min;
+    float root2 = sdisc > 0.f ? c / q : t_min;
+    t1 = fminf(root1, root2);
+    t2 = fmaxf(root1, root2);
+}
+// FP64 re-solve of the same quadratic from the same (FP32) ray and shape inputs: the
+// coefficients are formed in double so |O|^2 - r^2 keeps its low digits for large radii
+// and grazing rays.  Only the two root values change; the disc sign test stays FP32 so the
+// hit/miss topology matches the FP32 path unless the FP32 discriminant itself was wrong.
+PHX_D void polish_roots(float& t1, float& t2, double d, double b, double c)
+{
+    double disc = b * b - d * c;
+    if (disc <= 0.0) return;
+    double sd = sqrt(disc);
+    double q = b > 0.0 ? -(b + sd) : -(b - sd);
+    double r1 = q / d, r2 = c / q;
+    t1 = (float)fmin(r1, r2);
+    t2 = (float)fmax(r1, r2);
+}
+
+// ---------------------------------------------------------------- leaves
+PHX_D bool leaf_sphere(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir, int polish)
+{
+    float3 center = make_float3(q0.x, q0.y, q0.z);
+    float radius = q0.w;
+    float3 O = o - center;
+    float3 D = dir;
+    float b = dot(O, D);
+    float c = dot(O, O) - radius * radius;
+    float d = dot(D, D);
+    float root1, root2, disc, sdisc;
+    robust_roots(root1, root2, disc, sdisc, d, b, c);
+    if (polish && sdisc > 0.f) {
+        double ox = (double)o.x - center.x, oy = (double)o.y - center.y, oz = (double)o.z - center.z;
+        double bb = ox * D.x + oy * D.y + oz * D.z;
+        double cc = ox * ox + oy * oy + oz * oz - (double)radius * radius;
+        double dd = (double)D.x * D.x + (double)D.y * D.y + (double)D.z * D.z;
+        polish_roots(root1, root2, dd, bb, cc);
+    }
+    float t_cand = sdisc > 0.f ? (root1 > t_min ? root1 : root2) : t_min;
+    bool valid = t_cand > t_min;
+    if (valid) {
+        isect.x = (O.x + t_cand * D.x) / radius;
+        isect.y = (O.y + t_cand * D.y) / radius;
+        isect.z = (O.z + t_cand * D.z) / radius;
+        isect.w = t_cand;
+    }
+    return valid;
+}
+
+PHX_D bool leaf_zsphere(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir, int polish)
+{
+    const float3 center = make_float3(q0.x, q0.y, q0.z);
+    float3 O = o - center;
+    float3 D = dir;
+    const float radius = q0.w;
+    float b = dot(O, D);
+    float c = dot(O, O) - radius * radius;
+    if (c > 0.f && b > 0.f) return false;   // outside and moving away
+    const float zmax = center.z + q1.y;
+    const float zmin = center.z + q1.x;
+    float d = dot(D, D);
+    float t1sph, t2sph, disc, sdisc;
+    robust_roots(t1sph, t2sph, disc, sdisc, d, b, c);
+    if (polish && sdisc > 0.f) {
+        double ox = (double)o.x - center.x, oy = (double)o.y - center.y, oz = (double)o.z - center.z;
+        double bb = ox * D.x + oy * D.y + oz * D.z;
+        double cc = ox * ox + oy * oy + oz * oz - (double)radius * radius;
+        double dd = (double)D.x * D.x + (double)D.y * D.y + (double)D.z * D.z;
+        polish_roots(t1sph, t2sph, dd, bb, cc);
+    }
+    float z1sph = o.z + t1sph * dir.z;
+    float z2sph = o.z + t2sph * dir.z;
+    float idz = 1.f / dir.z;
+    float t_QCAP = (zmax - o.z) * idz;
+    float t_PCAP = (zmin - o.z) * idz;
+    float t1cap = fminf(t_QCAP, t_PCAP);
+    float t2cap = fmaxf(t_QCAP, t_PCAP);
+    if (t1cap < t1sph || t1cap > t2sph) t1cap = t_min;
+    if (t2cap < t1sph || t2cap > t2sph) t2cap = t_min;
+    float t_cand = t_min;
+    if (sdisc > 0.f) {
+        if (t1sph > t_min && z1sph > zmin && z1sph <= zmax) t_cand = t1sph;
+        else if (t1cap > t_min) t_cand = t1cap;
+        else if (t2cap > t_min) t_cand = t2cap;
+        else if (t2sph > t_min && z2sph > zmin && z2sph <= zmax) t_cand = t2sph;
+    }
+    bool valid = t_cand > t_min;
+    if (valid) {
+        isect.w = t_cand;
+        if (t_cand == t1sph || t_cand == t2sph) {
+            isect.x = (O.x + t_cand * D.x) / radius;
+            isect.y = (O.y + t_cand * D.y) / radius;
+            isect.z = (O.z + t_cand * D.z) / radius;
+        } else {
+            isect.x = 0.f;
+            isect.y = 0.f;
+            isect.z = t_cand == t_PCAP ? -1.f : 1.f;
+        }
+    }
+    return valid;
+}
+
+PHX_D bool leaf_cylinder(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir, int polish)
+{
+    const float r = q0.w;
+    const float z1 = q1.x;
+    const float z2 = q1.y;
+    const float ox = o.x, oy = o.y, oz = o.z;
+    const float vx = dir.x, vy = dir.y, vz = dir.z;
+    const float r2 = r * r;
+    const float a = vx * vx + vy * vy;
+    const float b = ox * vx + oy * vy;
+    const float c = ox * ox + oy * oy - r2;
+    float t_near, t_far, disc, sdisc;
+    robust_roots_disq(t_min, t_near, t_far, disc, sdisc, a, b, c);
+    if (polish && sdisc > 0.f) {
+        double aa = (double)vx * vx + (double)vy * vy;
+        double bb = (double)ox * vx + (double)oy * vy;
+        double cc = (double)ox * ox + (double)oy * oy - (double)r * r;
+        polish_roots(t_near, t_far, aa, bb, cc);
+    }
+    float z_near = oz + t_near * vz;
+    float z_far = oz + t_far * vz;
+    const float t_z1cap = (z1 - oz) / vz;
+    const float r2_z1cap = (ox + t_z1cap * vx) * (ox + t_z1cap * vx) + (oy + t_z1cap * vy) * (oy + t_z1cap * vy);
+    const float t_z2cap = (z2 - oz) / vz;
+    const float r2_z2cap = (ox + t_z2cap * vx) * (ox + t_z2cap * vx) + (oy + t_z2cap * vy) * (oy + t_z2cap * vy);
+    const float INF = __int_as_float(0x7f800000);
+    float t_cand = INF;
+    if (t_near > t_min && z_near > z1 && z_near < z2 && t_near < t_cand) t_cand = t_near;
+    if (t_far > t_min && z_far > z1 && z_far < z2 && t_far < t_cand) t_cand = t_far;
+    if (t_z1cap > t_min && r2_z1cap <= r2 && t_z1cap < t_cand) t_cand = t_z1cap;
+    if (t_z2cap > t_min && r2_z2cap <= r2 && t_z2cap < t_cand) t_cand = t_z2cap;
+    bool valid = t_cand > t_min && t_cand < INF;
+    if (valid) {
+        bool sheet = (t_cand == t_near || t_cand == t_far);
+        isect.x = sheet ? (ox + t_cand * vx) / r : 0.f;
+        isect.y = sheet ? (oy + t_cand * vy) / r : 0.f;
+        isect.z = sheet ? 0.f : (t_cand == t_z1cap ? -1.f : 1.f);
+        isect.w = t_cand;
+    }
+    return valid;
+}
+
+PHX_D bool leaf_box3(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir)
+{
+    const float3 bmin = make_float3(-q0.x / 2.f, -q0.y / 2.f, -q0.z / 2.f);
+    const float3 bmax = make_float3(q0.x / 2.f, q0.y / 2.f, q0.z / 2.f);
+    float3 idir = f3s(1.f) / dir;
+    float3 t0 = (bmin - o) * idir;
+    float3 t1 = (bmax - o) * idir;
+    float3 nr = fminf3(t0, t1);
+    float3 fr = fmaxf3(t0, t1);
+    float t_near = hmax(nr);
+    float t_far = hmin(fr);
+    bool along_x = dir.x != 0.f && dir.y == 0.f && dir.z == 0.f;
+    bool along_y = dir.x == 0.f && dir.y != 0.f && dir.z == 0.f;
+    bool along_z = dir.x == 0.f && dir.y == 0.f && dir.z != 0.f;
+    bool in_x = o.x > bmin.x && o.x < bmax.x;
+    bool in_y = o.y > bmin.y && o.y < bmax.y;
+    bool in_z = o.z > bmin.z && o.z < bmax.z;
+    bool has = false;
+    if (along_x) has = in_y && in_z;
+    else if (along_y) has = in_x && in_z;
+    else if (along_z) has = in_x && in_y;
+    else has = (t_far > t_near && t_far > 0.f);
+    bool valid = false;
+    if (has) {
+        float t_cand = t_min < t_near ? t_near : (t_min < t_far ? t_far : t_min);
+        float3 p = o + t_cand * dir;
+        float3 pa = make_float3(fabsf(p.x) / (bmax.x - bmin.x), fabsf(p.y) / (bmax.y - bmin.y), fabsf(p.z) / (bmax.z - bmin.z));
+        float3 n = f3s(0.f);
+        if (pa.x >= pa.y && pa.x >= pa.z) n.x = copysignf(1.f, p.x);
+        else if (pa.y >= pa.x && pa.y >= pa.z) n.y = copysignf(1.f, p.y);
+        else if (pa.z >= pa.x && pa.z >= pa.y) n.z = copysignf(1.f, p.z);
+        if (t_cand > t_min) {
+            valid = true;
+            isect.x = n.x; isect.y = n.y; isect.z = n.z; isect.w = t_cand;
+        }
+    }
+    return valid;
+}
+
+// ---------------------------------------------------------------- torus (FP64)
+// f(u) = (|p|^2 + R^2 - r^2)^2 - 4 R^2 (px^2 + py^2),  p = o + u*n  (|n| = 1)
+// Real roots of the quartic are bracketed between the real roots of its derivative
+// (a cubic, solved in closed form) and refined by safeguarded Newton/bisection.
+PHX_D double q4eval(const double* c, double u) { return (((u + c[3]) * u + c[2]) * u + c[1]) * u + c[0]; }
+PHX_D double q4deriv(const double* c, double u) { return ((4.0 * u + 3.0 * c[3]) * u + 2.0 * c[2]) * u + c[1]; }
+
+// real roots of x^3 + a x^2 + b x + c, ascending; returns count
+PHX_D int cubic_real_roots(double a, double b, double c, double* x)
+{
+    const double a3 = a / 3.0;
+    const double p = b - a * a3;                       // depressed: t^3 + p t + q
+    const double q = 2.0 * a3 * a3 * a3 - a3 * b + c;
+    const double disc = 0.25 * q * q + p * p * p / 27.0;
+    if (disc > 0.0) {
+        double s = sqrt(disc);
+        double A = cbrt(-0.5 * q + s);
+        double B = cbrt(-0.5 * q - s);
+        x[0] = A + B - a3;
+        return 1;
+    }
+    if (p == 0.0) { x[0] = -a3; return 1; }
+    double m = 2.0 * sqrt(-p / 3.0);
+    double arg = 3.0 * q / (p * m);
+    arg = fmin(1.0, fmax(-1.0, arg));
+    double th = acos(arg) / 3.0;
+    const double TWO_PI_3 = 2.0943951023931954923;
+    double r0 = m * cos(th) - a3, r1 = m * cos(th - TWO_PI_3) - a3, r2 = m * cos(th - 2.0 * TWO_PI_3) - a3;
+    // ascending
+    if (r0 > r1) { double t = r0; r0 = r1; r1 = t; }
+    if (r1 > r2) { double t = r1; r1 = r2; r2 = t; }
+    if (r0 > r1) { double t = r0; r0 = r1; r1 = t; }
+    x[0] = r0; x[1] = r1; x[2] = r2;
+    return 3;
+}
+
+// smallest root of the monic quartic in (lo, hi]; returns false if none
+PHX_D bool quartic_first_root(const double* c, double lo, double hi, double& root, unsigned& err)
+{
+    double crit[3];
+    int nc = cubic_real_roots(0.75 * c[3], 0.5 * c[2], 0.25 * c[1], crit);
+    double edges[5];
+    int ne = 0;
+    edges[ne++] = lo;
+    for (int i = 0; i < nc; i++) if (crit[i] > lo && crit[i] < hi) edges[ne++] = crit[i];
+    edges[ne++] = hi;
+    for (int i = 0; i + 1 < ne; i++) {
+        double a = edges[i], b = edges[i + 1];
+        double fa = q4eval(c, a), fb = q4eval(c, b);
+        if (fa == 0.0 && i > 0) { root = a; return true; }
+        if ((fa < 0.0) == (fb < 0.0) && fb != 0.0) continue;
+        // safeguarded Newton inside [a,b]
+        double x = 0.5 * (a + b);
+        int it = 0;
+        for (; it < 100; it++) {
+            double fx = q4eval(c, x);
+            if (fx == 0.0) break;
+            if ((fx < 0.0) == (fa < 0.0)) { a = x; fa = fx; } else { b = x; }
+            double dfx = q4deriv(c, x);
+            double xn = dfx != 0.0 ? x - fx / dfx : 0.5 * (a + b);
+            if (!(xn > a && xn < b)) xn = 0.5 * (a + b);
+            if (fabs(xn - x) <= 1e-12 * fmax(1.0, fabs(x))) { x = xn; break; }
+            x = xn;
+        }
+        if (it == 100) err |= PHX_STATUS_LOOP_CAP;
+        root = x;
+        return true;
+    }
+    return false;
+}
+
+// q0.y = minor radius r (rmax), q0.z = major radius R (rtor) ; full phi range
+PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir, unsigned& err)
+{
+    const double r = q0.y, R = q0.z;
+    const double dx = dir.x, dy = dir.y, dz = dir.z;
+    const double dl = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(dl > 0.0)) return false;
+    const double nx = dx / dl, ny = dy / dl, nz = dz / dl;
+    double ox = o.x, oy = o.y, oz = o.z;
+    // clip to the bounding sphere |p| <= R + r, and shift the origin near the torus
+    const double Rb = R + r;
+    const double bb = ox * nx + oy * ny + oz * nz;
+    const double cc = ox * ox + oy * oy + oz * oz - Rb * Rb;
+    const double dsc = bb * bb - cc;
+    if (dsc <= 0.0) return false;
+    const double sq = sqrt(dsc);
+    const double s_in = -bb - sq, s_out = -bb + sq;
+    const double s_min = (double)t_min * dl;
+    if (s_out <= s_min) return false;
+    const double s0 = fmax(s_in, 0.0);
+    ox += s0 * nx; oy += s0 * ny; oz += s0 * nz;
+    const double B = 2.0 * (ox * nx + oy * ny + oz * nz);
+    const double C = ox * ox + oy * oy + oz * oz + R * R - r * r;
+    const double R4 = 4.0 * R * R;
+    double c[4];
+    c[3] = 2.0 * B;
+    c[2] = B * B + 2.0 * C - R4 * (nx * nx + ny * ny);
+    c[1] = 2.0 * B * C - 2.0 * R4 * (ox * nx + oy * ny);
+    c[0] = C * C - R4 * (ox * ox + oy * oy);
+    const double lo = fmax(s_min - s0, 0.0);
+    const double hi = s_out - s0 + 1e-9 * Rb;
+    double u;
+    if (!quartic_first_root(c, lo, hi, u, err)) return false;
+    const double s = s0 + u;
+    const float t = (float)(s / dl);
+    if (!(t > t_min)) return false;
+    const double px = ox + u * nx, py = oy + u * ny, pz = oz + u * nz;
+    const double k = px * px + py * py + pz * pz + R * R - r * r;
+    double gx = px * (k - 2.0 * R * R), gy = py * (k - 2.0 * R * R), gz = pz * k;
+    const double gl = sqrt(gx * gx + gy * gy + gz * gz);
+    isect.x = (float)(gx / gl);
+    isect.y = (float)(gy / gl);
+    isect.z = (float)(gz / gl);
+    isect.w = t;
+    return true;
+}
+
+// ---------------------------------------------------------------- leaf with transform
+PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
+{
+    isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 q0 = __ldg(g.node + 4 * ni + 0);
+    const float4 q1 = __ldg(g.node + 4 * ni + 1);
+    const float4 q3 = __ldg(g.node + 4 * ni + 3);
+    const unsigned typecode = __float_as_uint(q3.z);
+    const unsigned tc_w = __float_as_uint(q3.w);
+    const unsigned gtransformIdx = tc_w & 0x7fffffffu;
+    const bool complement = (tc_w & 0x80000000u) != 0u;
+    float4 t4[4];
+    const float4* q = nullptr;
+    if (gtransformIdx > 0) {
+        const float4* src = g.itra + 4 * (gtransformIdx - 1);
+        t4[0] = __ldg(src + 0); t4[1] = __ldg(src + 1); t4[2] = __ldg(src + 2); t4[3] = __ldg(src + 3);
+        q = t4;
+    }
+    float3 origin = q ? xform_row(q, ray_o, 1.f) : ray_o;
+    float3 direction = q ? xform_row(q, ray_d, 0.f) : ray_d;
+    bool valid = false;
+    switch (typecode) {
+        case PHX_CSG_SPHERE:   valid = leaf_sphere(isect, q0, t_min, origin, direction, g.polish); break;
+        case PHX_CSG_ZSPHERE:  valid = leaf_zsphere(isect, q0, q1, t_min, origin, direction, g.polish); break;
+        case PHX_CSG_CYLINDER: valid = leaf_cylinder(isect, q0, q1, t_min, origin, direction, g.polish); break;
+        case PHX_CSG_BOX3:     valid = leaf_box3(isect, q0, t_min, origin, direction); break;
+        case PHX_CSG_TORUS:    valid = leaf_torus(isect, q0, t_min, origin, direction, err); break;
+        default: break;
+    }
+    if (valid && q) {
+        float3 n = xform_col(q, make_float3(isect.x, isect.y, isect.z), 0.f);
+        isect.x = n.x; isect.y = n.y; isect.z = n.z;
+    }
+    if (complement) {
+        isect.x = valid ? -isect.x : -0.f;
+        isect.y = valid ? -isect.y : isect.y;
+        isect.z = valid ? -isect.z : isect.z;
+    }
+    return valid;
+}
+
+PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
+{
+    return fabsf(ise.w) > tmin ? (ise.x * d.x + ise.y * d.y + ise.z * d.z < 0.f ? PHX_STATE_ENTER : PHX_STATE_EXIT) : PHX_STATE_MISS;
+}
+
+#define PHX_POSTORDER_NEXT(i, elev) (((i) & 1u) ? (i) >> 1 : ((i) << (elev)) + (1u << (elev)))
+
+// ---------------------------------------------------------------- tree
+PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
+{
+    const unsigned numNode = __float_as_uint(__ldg(g.node + 4 * root).x);   // subNum
+    const unsigned height = (unsigned)(__ffs((int)numNode + 1) - 2);
+    float4 stk[PHX_CSG_STACK];
+    int sp = -1;
+    unsigned tslice[PHX_TRANCHE_STACK];
+    float ttmin[PHX_TRANCHE_STACK];
+    int tp = 0;
+    tslice[0] = ((1u << height) << 16) | 0u;
+    ttmin[0] = t_min;
+    unsigned ierr = 0;
+    while (tp > -1) {
+        const unsigned slice = tslice[tp];
+        const float tmin = ttmin[tp];
+        tp--;
+        const unsigned beginIdx = slice >> 16;
+        const unsigned endIdx = slice & 0xffffu;
+        unsigned nodeIdx = beginIdx;
+        while (nodeIdx != endIdx) {
+            const unsigned depth = 31u - __clz(nodeIdx);
+            const unsigned elevation = height - depth;
+            const int ni = root + (int)nodeIdx - 1;
+            const unsigned typecode = __float_as_uint(__ldg(g.node + 4 * ni + 3).z);
+            if (typecode == PHX_CSG_ZERO) { nodeIdx = PHX_POSTORDER_NEXT(nodeIdx, elevation); continue; }
+            if (typecode >= PHX_CSG_NODE) {
+                float4 nd_isect;
+                intersect_leaf(nd_isect, g, ni, tmin, o, d, err);
+                nd_isect.w = copysignf(nd_isect.w, nodeIdx % 2u == 0u ? -1.f : 1.f);
+                if (sp >= PHX_CSG_STACK - 1) { ierr |= PHX_CSG_ERR_OVERFLOW; break; }
+                stk[++sp] = nd_isect;
+            } else {
+                if (sp < 1) { ierr |= PHX_CSG_ERR_POP_EMPTY; break; }
+                const bool firstLeft = signbit(stk[sp].w);
+                const bool secondLeft = signbit(stk[sp - 1].w);
+                if (!(firstLeft ^ secondLeft)) { ierr |= PHX_CSG_ERR_XOR_SIDE; break; }
+                const int left = firstLeft ? sp : sp - 1;
+                const int right = firstLeft ? sp - 1 : sp;
+                const float4 L = stk[left];
+                const float4 Rr = stk[right];
+                int l_state = phx_classify(L, d, tmin);
+                int r_state = phx_classify(Rr, d, tmin);
+                const float t_left = fabsf(L.w);
+                const float t_right = fabsf(Rr.w);
+                bool leftIsCloser = t_left <= t_right;
+                const bool l_promote = l_state == PHX_STATE_MISS && (signbit(L.x) || signbit(L.y));
+                const bool r_promote = r_state == PHX_STATE_MISS && (signbit(Rr.x) || signbit(Rr.y));
+                if (r_promote) { r_state = PHX_STATE_EXIT; leftIsCloser = true; }
+                if (l_promote) { l_state = PHX_STATE_EXIT; leftIsCloser = false; }
+                const int ctrl = phx_csg_lookup((int)typecode, l_state, r_state, leftIsCloser);
+                if (ctrl < PHX_CTRL_LOOP_A) {
+                    float4 result = ctrl == PHX_CTRL_RETURN_MISS ? make_float4(0.f, 0.f, 0.f, 0.f) : (ctrl == PHX_CTRL_RETURN_A ? L : Rr);
+                    if (ctrl == PHX_CTRL_RETURN_FLIP_B) { result.x = -result.x; result.y = -result.y; result.z = -result.z; }
+                    result.w = copysignf(result.w, nodeIdx % 2u == 0u ? -1.f : 1.f);
+                    sp -= 2;
+                    stk[++sp] = result;
+                } else {
+                    const bool loopA = ctrl == PHX_CTRL_LOOP_A;
+                    const float4 loopv = loopA ? L : Rr;
+                    const float4 other = loopA ? Rr : L;
+                    const unsigned leftIdx = 2u * nodeIdx;
+                    const unsigned rightIdx = leftIdx + 1u;
+                    const unsigned otherIdx = loopA ? rightIdx : leftIdx;
+                    (void)otherIdx;
+                    const float tminAdvanced = fabsf(loopv.w) + PHX_CSG_PROPAGATE_EPSILON;
+                    sp -= 2;
+                    stk[++sp] = other;
+                    const unsigned endTree = (nodeIdx << 16) | endIdx;
+                    const unsigned leftTree = ((leftIdx << (elevation - 1u)) << 16) | (rightIdx << (elevation - 1u));
+                    const unsigned rightTree = ((rightIdx << (elevation - 1u)) << 16) | nodeIdx;
+                    const unsigned loopTree = loopA ? leftTree : rightTree;
+                    if (tp >= PHX_TRANCHE_STACK - 1) { ierr |= PHX_CSG_ERR_TRANCHE; break; }
+                    tp++; tslice[tp] = endTree; ttmin[tp] = tmin;
+                    if (tp >= PHX_TRANCHE_STACK - 1) { ierr |= PHX_CSG_ERR_TRANCHE; break; }
+                    tp++; tslice[tp] = loopTree; ttmin[tp] = tminAdvanced;
+                    break;
+                }
+            }
+            nodeIdx = PHX_POSTORDER_NEXT(nodeIdx, elevation);
+        }
+        if (ierr) break;
+    }
+    if (sp != 0) ierr |= PHX_CSG_ERR_END_EMPTY;
+    isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sp == 0) isect = stk[0];
+    if (ierr) err |= PHX_STATUS_CSG_STACK;
+    return isect.w > 0.f;
+}
+
+// one prim: leaf at the root, or a boolean tree
+PHX_D bool intersect_prim(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
+{
+    const unsigned typecode = __float_as_uint(__ldg(g.node + 4 * root + 3).z);
+    isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (typecode >= PHX_CSG_LEAF) return intersect_leaf(isect, g, root, t_min, o, d, err);
+    if (typecode < PHX_CSG_NODE) return intersect_tree(isect, g, root, t_min, o, d, err);
+    return false;
+}

@@ -1,0 +1,809 @@
+// phx_engine.cu : kernels and the C ABI of the photon engine (include/phox.h).
+//
+// Data layout in HBM (one engine per device):
+//   node/itra/plan      CSGFoundry arrays, uploaded unchanged (float4 rows)
+//   bvh, leaves         4-wide BVH over (instance, prim) leaves, built on the host (phx_bvh.cc)
+//   inst_inv            world->object transform per instance (4 float4 rows)
+//   bnd texture         float4 (num_wl x num_bnd*8), hardware linear filter like qudarap/QBnd.cc:155
+//   icdf texture        float  (4096 x 3), hardware linear filter like qudarap/QScint.cc:104
+//   rng                 cuRAND XORWOW state per photon slot, SoA of six u32 words (24 B/slot)
+//   photon, seq, hit    sphoton (64 B), sseq (32 B), sphoton per hit
+//   hitword             one bit per photon (hit mask ballot), scanned to compact hits in order
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "phox.h"
+#include "phx_pod.h"
+#include "phx_bvh.h"
+#include "phx_kernels.cuh"
+
+// ------------------------------------------------------------------ error plumbing
+static thread_local std::string g_last_error;
+static int phx_fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+#define PHX_CU(call)                                                                         \
+    do {                                                                                     \
+        cudaError_t _e = (call);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return phx_fail(-2, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+    } while (0)
+
+// ------------------------------------------------------------------ engine state
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t want)
+    {
+        if (want <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr; n = 0;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(want, 1) * sizeof(T));
+        if (e == cudaSuccess) n = want;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+struct phx_engine {
+    int device = 0;
+    phx_config cfg;
+    cudaStream_t stream = nullptr;
+    // geometry
+    DevBuf<float4> node, itra, plan, inst_inv;
+    DevBuf<phx_bvh4_node> bvh;
+    DevBuf<phx_leaf> leaves;
+    int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
+    std::vector<int> prim_node_offset;
+    // physics
+    cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr;
+    cudaTextureObject_t bnd_tex = 0, icdf_tex = 0;
+    DevBuf<uint4> optical;
+    float nm0 = 60.f, nms = 1.f;
+    unsigned nx = 0, ny = 0, hd_factor = 20;
+    int num_bnd = 0;
+    std::vector<float> bnd_host;   // kept for the adjoint (property re-tabulation)
+    int num_wl = 0;
+    // rng
+    DevBuf<uint32_t> rng;
+    long long rng_slots = 0;
+    // scratch
+    DevBuf<float4> gs;
+    DevBuf<long long> gs_off;
+    DevBuf<int> gs_event;
+    DevBuf<phx_photon> photon;
+    DevBuf<phx_seq> seq;
+    DevBuf<phx_photon> hit;
+    DevBuf<uint32_t> hitword, wordoff, blocksum, sensor;
+    DevBuf<long long> counters;   // [0] num_hit, [1] queue head, [2..] misc
+    DevBuf<unsigned> status;
+    unsigned* h_pinned = nullptr;  // 16 words of pinned readback
+};
+
+static PhxScene scene_of(const phx_engine* e, int polish)
+{
+    PhxScene S;
+    S.bvh = e->bvh.p;
+    S.leaves = e->leaves.p;
+    S.inst_inv = e->inst_inv.p;
+    S.csg.node = e->node.p;
+    S.csg.itra = e->itra.p;
+    S.csg.polish = polish;
+    S.empty = e->num_leaf == 0;
+    return S;
+}
+
+static PhxProps props_of(const phx_engine* e)
+{
+    PhxProps P;
+    P.bnd_tex = e->bnd_tex;
+    P.optical = e->optical.p;
+    P.nm0 = e->nm0;
+    P.nms = e->nms;
+    P.nx = e->nx;
+    P.ny = e->ny;
+    P.icdf_tex = e->icdf_tex;
+    P.hd_factor = e->hd_factor;
+    return P;
+}
+
+static PhxLoopCfg loop_of(const phx_engine* e)
+{
+    PhxLoopCfg C;
+    C.max_bounce = e->cfg.max_bounce;
+    C.max_time = e->cfg.max_time;
+    C.tmin = e->cfg.propagate_epsilon;
+    C.tmin0 = e->cfg.propagate_epsilon0;
+    C.tmax = 1000000.f;
+    C.eps0_mask = e->cfg.epsilon0_mask;
+    return C;
+}
+
+// ------------------------------------------------------------------ kernels
+// curand_init(seed, subsequence=slot, offset) per photon slot : qudarap/QCurandState.cu:22-27
+__global__ void k_rng_init(unsigned long long seed, unsigned long long offset, long long first, long long count, long long slots, uint32_t* rng)
+{
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    long long slot = first + i;
+    curandStateXORWOW s;
+    curand_init(seed, (unsigned long long)slot, offset, &s);
+    rng[slot] = s.d;
+    rng[slots * 1 + slot] = s.v[0];
+    rng[slots * 2 + slot] = s.v[1];
+    rng[slots * 3 + slot] = s.v[2];
+    rng[slots * 4 + slot] = s.v[3];
+    rng[slots * 5 + slot] = s.v[4];
+}
+
+// exclusive scan of genstep photon counts (quad6 q0.w) into off[G+1] : replaces the
+// thrust reduce + iexpand seed buffer of qudarap/QEvt.cu:180-230 (photons find their genstep by
+// binary search over off, so no per-photon seed array is written or read)
+__global__ void k_genstep_offsets(const float4* gs, int G, long long* off)
+{
+    __shared__ long long warp_tot[32];
+    __shared__ long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < G; base += blockDim.x) {
+        int g = base + threadIdx.x;
+        long long v = g < G ? (long long)__float_as_int(gs[6 * g].w) : 0;
+        if (v < 0) v = 0;
+        long long x = v;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) { long long y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            long long t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) { long long y = __shfl_up_sync(0xffffffffu, t, o); if (lane >= o) t += y; }
+            warp_tot[lane] = t;
+        }
+        __syncthreads();
+        long long incl = x + (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
+        if (g < G) off[g + 1] = incl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) off[0] = 0;
+}
+
+PHX_D int phx_find_genstep(const long long* off, int G, long long idx)
+{
+    int lo = 0, hi = G;   // off[lo] <= idx < off[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= idx) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+struct SimArgs {
+    PhxScene S;
+    PhxProps P;
+    PhxLoopCfg C;
+    const float4* gs;
+    const long long* gs_off;
+    int G;
+    long long N;
+    long long photon_offset;
+    unsigned long long event_index;
+    unsigned long long skip;
+    const uint32_t* rng;
+    long long rng_slots;
+    phx_photon* photon;
+    phx_seq* seq;
+    uint32_t* hitword;
+    unsigned hit_mask;
+    unsigned* status;
+};
+
+// one thread per photon : CSGOptiX/CSGOptiX7.cu:432-530 simulate()
+__global__ void __launch_bounds__(128) k_simulate(SimArgs a)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned status = 0;
+    bool is_hit = false;
+    if (idx < a.N) {
+        const int gi = phx_find_genstep(a.gs_off, a.G, idx);
+        float4 g[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) g[k] = __ldg(a.gs + 6 * gi + k);
+        const long long photon_idx = a.photon_offset + idx;
+        curandStateXORWOW rng;
+        if (photon_idx < a.rng_slots) {
+            phx_load_rng(rng, a.rng, a.rng_slots, photon_idx);
+        } else {
+            status |= PHX_STATUS_RNG_RANGE;
+            curand_init(0ull, (unsigned long long)photon_idx, 0ull, &rng);
+        }
+        if (a.event_index > 0ull) skipahead(a.skip * a.event_index, &rng);
+        PhxPhoton p;
+        memset(&p, 0, sizeof(p));
+        generate_photon(p, rng, g, (unsigned long long)photon_idx, a.P, status);
+        unsigned long long seqhis[2] = { 0ull, 0ull }, seqbnd[2] = { 0ull, 0ull };
+        phx_bounce_loop(p, rng, a.S, a.P, a.C, seqhis, seqbnd, status);
+        if (a.photon) phx_store_photon(a.photon + idx, p);
+        if (a.seq) {
+            ulonglong2* s = reinterpret_cast<ulonglong2*>(a.seq + idx);
+            s[0] = make_ulonglong2(seqhis[0], seqhis[1]);
+            s[1] = make_ulonglong2(seqbnd[0], seqbnd[1]);
+        }
+        is_hit = (p.flagmask & a.hit_mask) == a.hit_mask;
+    }
+    const unsigned word = __ballot_sync(0xffffffffu, is_hit);
+    if (a.hitword && (threadIdx.x & 31) == 0 && idx < a.N) a.hitword[idx >> 5] = word;
+    if (status) atomicOr(a.status, status);
+}
+
+// per-word exclusive popcount offsets within blocks of 256 words, block totals
+__global__ void k_word_scan(const uint32_t* word, long long nword, uint32_t* wordoff, uint32_t* blocksum)
+{
+    __shared__ uint32_t wt[8];
+    const long long w = (long long)blockIdx.x * 256 + threadIdx.x;
+    uint32_t c = w < nword ? __popc(word[w]) : 0u;
+    uint32_t x = c;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) wt[wid] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int k = 0; k < wid; k++) before += wt[k];
+    if (w < nword) wordoff[w] = before + x - c;
+    if (threadIdx.x == 255) blocksum[blockIdx.x] = before + x;
+}
+
+// exclusive scan of block totals in place, total into *total
+__global__ void k_block_scan(uint32_t* blocksum, int nblock, long long* total)
+{
+    __shared__ uint32_t wt[32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nblock; base += blockDim.x) {
+        int b = base + threadIdx.x;
+        uint32_t v = b < nblock ? blocksum[b] : 0u;
+        uint32_t x = v;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) wt[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t t = lane < (int)(blockDim.x >> 5) ? wt[lane] : 0u;
+            for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, t, o); if (lane >= o) t += y; }
+            wt[lane] = t;
+        }
+        __syncthreads();
+        unsigned long long incl = (unsigned long long)x + (wid > 0 ? wt[wid - 1] : 0u) + carry;
+        if (b < nblock) blocksum[b] = (uint32_t)(incl - v);
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = (long long)carry;
+}
+
+// warp w handles hit word w : ordered copy of the selected photons (QEvt::gatherHit with
+// SU::copy_if sphoton_selector, qudarap/QEvt.cc:934-985, sysrap/SU.cu:139-166) plus the
+// per-sensor tally (identity-1).
+__global__ void k_compact(const phx_photon* photon, long long N, const uint32_t* word, const uint32_t* wordoff,
+                          const uint32_t* blocksum, phx_photon* hit, long long hit_capacity,
+                          uint32_t* sensor, int num_sensor, unsigned* status)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= N) return;
+    const long long w = idx >> 5;
+    const uint32_t bits = word[w];
+    const int lane = threadIdx.x & 31;
+    if (!((bits >> lane) & 1u)) return;
+    const uint32_t rank = __popc(bits & ((1u << lane) - 1u));
+    const long long dst = (long long)blocksum[w >> 8] + wordoff[w] + rank;
+    const float4* src = reinterpret_cast<const float4*>(photon + idx);
+    const float4 q0 = src[0], q1 = src[1], q2 = src[2], q3 = src[3];
+    if (hit) {
+        if (dst < hit_capacity) {
+            float4* o = reinterpret_cast<float4*>(hit + dst);
+            o[0] = q0; o[1] = q1; o[2] = q2; o[3] = q3;
+        } else {
+            atomicOr(status, (unsigned)PHX_STATUS_HIT_OVERFLOW);
+        }
+    }
+    if (sensor) {
+        const unsigned id = __float_as_uint(q3.y) & 0xffffffu;
+        if (id > 0u && (int)(id - 1u) < num_sensor) atomicAdd(sensor + (id - 1u), 1u);
+    }
+}
+
+// CSGScan : one thread per ray, SoA rays
+__global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* rays, long long n, float4* out, unsigned* status)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 o = make_float3(__ldg(rays + i), __ldg(rays + n + i), __ldg(rays + 2 * n + i));
+    const float3 d = make_float3(__ldg(rays + 3 * n + i), __ldg(rays + 4 * n + i), __ldg(rays + 5 * n + i));
+    unsigned st = 0;
+    float4 is;
+    const bool valid = intersect_prim(is, csg, root, t_min, o, d, st);
+    out[i] = valid ? is : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (st) atomicOr(status, st);
+}
+
+// QSim::rng_sequence : uniforms of each photon slot after the event skipahead
+__global__ void k_rng_sequence(const uint32_t* rng, long long slots, unsigned long long skip, long long first, long long n, int K, float* out)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    curandStateXORWOW s;
+    phx_load_rng(s, rng, slots, first + j);
+    if (skip) skipahead(skip, &s);
+    for (int k = 0; k < K; k++) out[j * K + k] = curand_uniform(&s);
+}
+
+// ------------------------------------------------------------------ host helpers
+static double det3(const double m[3][3])
+{
+    return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) + m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+}
+
+// inverse of a row-vector affine 4x4 (rows 0..2 linear, row 3 translation), .w column ignored
+static bool invert_affine(const float* q, float* out)
+{
+    double a[3][3];
+    for (int r = 0; r < 3; r++) for (int c = 0; c < 3; c++) a[r][c] = q[4 * r + c];
+    double det = det3(a);
+    if (!(std::fabs(det) > 0.0)) return false;
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    double t[3] = { q[12], q[13], q[14] };
+    double ti[3];
+    for (int c = 0; c < 3; c++) ti[c] = -(t[0] * inv[0][c] + t[1] * inv[1][c] + t[2] * inv[2][c]);
+    for (int r = 0; r < 3; r++) { for (int c = 0; c < 3; c++) out[4 * r + c] = (float)inv[r][c]; out[4 * r + 3] = 0.f; }
+    out[12] = (float)ti[0]; out[13] = (float)ti[1]; out[14] = (float)ti[2]; out[15] = 1.f;
+    return true;
+}
+
+static int make_texture_f4(cudaArray_t& arr, cudaTextureObject_t& tex, const float* data, int width, int height)
+{
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
+    PHX_CU(cudaMallocArray(&arr, &ch, width, height));
+    PHX_CU(cudaMemcpy2DToArray(arr, 0, 0, data, width * sizeof(float4), width * sizeof(float4), height, cudaMemcpyHostToDevice));
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    PHX_CU(cudaCreateTextureObject(&tex, &rd, &td, nullptr));
+    return 0;
+}
+
+static int make_texture_f1(cudaArray_t& arr, cudaTextureObject_t& tex, const float* data, int width, int height)
+{
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    PHX_CU(cudaMallocArray(&arr, &ch, width, height));
+    PHX_CU(cudaMemcpy2DToArray(arr, 0, 0, data, width * sizeof(float), width * sizeof(float), height, cudaMemcpyHostToDevice));
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    PHX_CU(cudaCreateTextureObject(&tex, &rd, &td, nullptr));
+    return 0;
+}
+
+static int ensure_rng(phx_engine* e, long long want)
+{
+    if (want <= e->rng_slots) return 0;
+    long long slots = std::max<long long>(want, e->rng_slots * 2);
+    DevBuf<uint32_t> nb;
+    PHX_CU(nb.ensure((size_t)slots * 6));
+    if (e->rng_slots > 0) {
+        for (int k = 0; k < 6; k++)
+            PHX_CU(cudaMemcpyAsync(nb.p + (size_t)k * slots, e->rng.p + (size_t)k * e->rng_slots, e->rng_slots * sizeof(uint32_t), cudaMemcpyDeviceToDevice, e->stream));
+    }
+    long long first = e->rng_slots, count = slots - e->rng_slots;
+    const int B = 256;
+    k_rng_init<<<(unsigned)((count + B - 1) / B), B, 0, e->stream>>>(e->cfg.seed, e->cfg.offset, first, count, slots, nb.p);
+    PHX_CU(cudaGetLastError());
+    PHX_CU(cudaStreamSynchronize(e->stream));
+    e->rng.release();
+    e->rng = nb;
+    e->rng_slots = slots;
+    return 0;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* phx_version(void) { return "phox 0.1 sm_100a"; }
+const char* phx_last_error(void) { return g_last_error.c_str(); }
+
+void phx_config_default(phx_config* c)
+{
+    memset(c, 0, sizeof(*c));
+    c->seed = 0;
+    c->offset = 0;
+    c->skipahead_event_offset = 100000;
+    c->max_photon = 1000000;
+    c->max_bounce = 31;
+    c->max_time = 1.e27f;
+    c->propagate_epsilon = 0.05f;
+    c->propagate_epsilon0 = 0.05f;
+    c->epsilon0_mask = PHX_TORCH | PHX_CERENKOV | PHX_SCINTILLATION | PHX_BULK_SCATTER | PHX_BULK_REEMIT;
+    c->hit_mask = PHX_SURFACE_DETECT;
+    c->root_polish = 0;
+    c->num_sensor = 0;
+}
+
+int64_t phx_count_photons(const float* gensteps, int32_t num_genstep)
+{
+    int64_t n = 0;
+    for (int g = 0; g < num_genstep; g++) {
+        int32_t v;
+        memcpy(&v, gensteps + 24 * g + 3, 4);
+        if (v > 0) n += v;
+    }
+    return n;
+}
+
+int phx_destroy(phx_engine* e)
+{
+    if (!e) return 0;
+    cudaSetDevice(e->device);
+    if (e->bnd_tex) cudaDestroyTextureObject(e->bnd_tex);
+    if (e->icdf_tex) cudaDestroyTextureObject(e->icdf_tex);
+    if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
+    if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
+    e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release();
+    e->bvh.release(); e->leaves.release(); e->optical.release(); e->rng.release();
+    e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
+    e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
+    e->counters.release(); e->status.release();
+    if (e->h_pinned) cudaFreeHost(e->h_pinned);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return 0;
+}
+
+int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_config* cfg_in, int device, phx_engine** out)
+{
+    if (!geo || !phys || !out) return phx_fail(-1, "phx_create: null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return phx_fail(-3, "phx_create: no CUDA device");
+    if (device < 0 || device >= ndev) return phx_fail(-1, "phx_create: device %d out of range (%d devices)", device, ndev);
+    phx_engine* e = new phx_engine();
+    e->device = device;
+    if (cfg_in) e->cfg = *cfg_in; else phx_config_default(&e->cfg);
+    int rc = 0;
+#define PHX_TRY(x) do { rc = (x); if (rc) { phx_destroy(e); return rc; } } while (0)
+#define PHX_TRYCU(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) { rc = phx_fail(-2, "%s failed: %s", #call, cudaGetErrorString(_e)); phx_destroy(e); return rc; } } while (0)
+    PHX_TRYCU(cudaSetDevice(device));
+    PHX_TRYCU(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    PHX_TRYCU(cudaMallocHost(&e->h_pinned, 64 * sizeof(unsigned)));
+
+    // ---- geometry
+    if (geo->num_node <= 0 || !geo->node) { phx_destroy(e); return phx_fail(-1, "phx_create: no CSGNode"); }
+    e->num_node = geo->num_node;
+    e->num_prim = geo->num_prim;
+    e->num_inst = geo->num_inst;
+    PHX_TRYCU(e->node.ensure((size_t)geo->num_node * 4));
+    PHX_TRYCU(cudaMemcpy(e->node.p, geo->node, (size_t)geo->num_node * 64, cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->itra.ensure((size_t)std::max(1, geo->num_itra) * 4));
+    if (geo->num_itra > 0) PHX_TRYCU(cudaMemcpy(e->itra.p, geo->itra, (size_t)geo->num_itra * 64, cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->plan.ensure((size_t)std::max(1, geo->num_plan)));
+    if (geo->num_plan > 0) PHX_TRYCU(cudaMemcpy(e->plan.p, geo->plan, (size_t)geo->num_plan * 16, cudaMemcpyHostToDevice));
+
+    e->prim_node_offset.resize(geo->num_prim);
+    for (int p = 0; p < geo->num_prim; p++) {
+        int32_t no;
+        memcpy(&no, geo->prim + 16 * p + 1, 4);
+        e->prim_node_offset[p] = no;
+        int32_t nn;
+        memcpy(&nn, geo->prim + 16 * p + 0, 4);
+        if (no < 0 || no + std::max(nn, 1) > geo->num_node) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d node range out of bounds", p); }
+    }
+    std::vector<float> inv((size_t)std::max(1, geo->num_inst) * 16, 0.f);
+    std::vector<PhxLeafInput> leaves;
+    for (int i = 0; i < geo->num_inst; i++) {
+        const float* q = geo->inst + 16 * i;
+        float m[16];
+        memcpy(m, q, sizeof(m));
+        m[3] = m[7] = m[11] = 0.f; m[15] = 1.f;   // clear identity info in the .w column
+        if (!invert_affine(m, &inv[16 * (size_t)i])) { phx_destroy(e); return phx_fail(-1, "phx_create: instance %d transform is singular", i); }
+        int32_t gas_idx, sensor_id1;
+        memcpy(&gas_idx, q + 7, 4);
+        memcpy(&sensor_id1, q + 11, 4);
+        if (gas_idx < 0 || gas_idx >= geo->num_solid) { phx_destroy(e); return phx_fail(-1, "phx_create: instance %d gas_idx %d out of range", i, gas_idx); }
+        const int32_t* so = geo->solid + 12 * gas_idx;
+        const int numPrim = so[4], primOffset = so[5];
+        for (int p = primOffset; p < primOffset + numPrim; p++) {
+            if (p < 0 || p >= geo->num_prim) { phx_destroy(e); return phx_fail(-1, "phx_create: solid %d prim %d out of range", gas_idx, p); }
+            const float* pr = geo->prim + 16 * p;
+            PhxLeafInput L;
+            L.bbox[0] = pr[8]; L.bbox[1] = pr[9]; L.bbox[2] = pr[10];
+            L.bbox[3] = pr[11]; L.bbox[4] = pr[12]; L.bbox[5] = pr[13];
+            memcpy(L.xform, m, sizeof(m));
+            int32_t gpi;
+            memcpy(&gpi, pr + 15, 4);
+            const int no = e->prim_node_offset[p];
+            uint32_t boundary;
+            memcpy(&boundary, geo->node + 16 * no + 6, 4);
+            L.leaf.inst = i;
+            L.leaf.node_offset = no;
+            L.leaf.gp_bd = ((uint32_t)(gpi & 0xffff) << 16) | (boundary & 0xffffu);
+            L.leaf.ii_id = ((uint32_t)(i & 0xffff) << 16) | ((uint32_t)sensor_id1 & 0xffffu);
+            leaves.push_back(L);
+        }
+    }
+    PhxBvh4Result bv;
+    if (phx_build_bvh4(leaves, bv) != 0) { phx_destroy(e); return phx_fail(-1, "phx_create: BVH build failed"); }
+    e->num_leaf = (int)bv.leaves.size();
+    e->bvh_depth = bv.max_depth;
+    if (3 * (bv.max_depth + 1) + 4 > PHX_BVH_STACK) { phx_destroy(e); return phx_fail(-1, "phx_create: BVH depth %d exceeds traversal stack", bv.max_depth); }
+    PHX_TRYCU(e->bvh.ensure(std::max<size_t>(1, bv.nodes.size())));
+    if (!bv.nodes.empty()) PHX_TRYCU(cudaMemcpy(e->bvh.p, bv.nodes.data(), bv.nodes.size() * sizeof(phx_bvh4_node), cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->leaves.ensure(std::max<size_t>(1, bv.leaves.size())));
+    if (!bv.leaves.empty()) PHX_TRYCU(cudaMemcpy(e->leaves.p, bv.leaves.data(), bv.leaves.size() * sizeof(phx_leaf), cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->inst_inv.ensure(inv.size() / 4));
+    PHX_TRYCU(cudaMemcpy(e->inst_inv.p, inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice));
+
+    // ---- physics
+    if (!phys->bnd || phys->num_bnd <= 0 || phys->num_wl <= 1 || !phys->optical) { phx_destroy(e); return phx_fail(-1, "phx_create: bnd/optical missing"); }
+    e->num_bnd = phys->num_bnd;
+    e->num_wl = phys->num_wl;
+    e->nx = (unsigned)phys->num_wl;
+    e->ny = (unsigned)phys->num_bnd * 8u;
+    e->nm0 = phys->wl_low;
+    e->nms = phys->wl_step;
+    e->bnd_host.assign(phys->bnd, phys->bnd + (size_t)phys->num_bnd * 8 * phys->num_wl * 4);
+    PHX_TRY(make_texture_f4(e->bnd_arr, e->bnd_tex, phys->bnd, (int)e->nx, (int)e->ny));
+    PHX_TRYCU(e->optical.ensure((size_t)phys->num_bnd * 4));
+    PHX_TRYCU(cudaMemcpy(e->optical.p, phys->optical, (size_t)phys->num_bnd * 4 * 16, cudaMemcpyHostToDevice));
+    if (phys->icdf && phys->icdf_width > 1 && phys->icdf_layers > 0) {
+        e->hd_factor = (unsigned)phys->hd_factor;
+        PHX_TRY(make_texture_f1(e->icdf_arr, e->icdf_tex, phys->icdf, phys->icdf_width, phys->icdf_layers));
+    } else {
+        e->hd_factor = 0xffffffffu;  // no scintillator table : reemission wavelength 0
+        float dummy[4] = { 0.f, 0.f, 0.f, 0.f };
+        PHX_TRY(make_texture_f1(e->icdf_arr, e->icdf_tex, dummy, 2, 2));
+    }
+    // ---- rng + small buffers
+    PHX_TRYCU(e->status.ensure(4));
+    PHX_TRYCU(e->counters.ensure(8));
+    PHX_TRY(ensure_rng(e, std::max<long long>(1, e->cfg.max_photon)));
+    PHX_TRYCU(cudaStreamSynchronize(e->stream));
+#undef PHX_TRY
+#undef PHX_TRYCU
+    *out = e;
+    return 0;
+}
+
+// shared device path : gensteps already on device
+static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long long N, int event_index, long long photon_offset,
+                                phx_photon* d_photon, phx_seq* d_seq, phx_photon* d_hit, long long hit_capacity,
+                                uint32_t* d_sensor, long long* num_hit, unsigned* status, cudaStream_t st)
+{
+    if (G < 0 || N < 0) return phx_fail(-1, "simulate: negative sizes");
+    if (photon_offset < 0) return phx_fail(-1, "simulate: negative photon_offset");
+    int rc = ensure_rng(e, photon_offset + N);
+    if (rc) return rc;
+    PHX_CU(e->gs_off.ensure((size_t)G + 1));
+    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
+    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gs), G, e->gs_off.p);
+    PHX_CU(cudaGetLastError());
+    const long long nword = (N + 31) / 32;
+    const bool want_hits = d_hit != nullptr || d_sensor != nullptr;
+    phx_photon* photon = d_photon;
+    if (want_hits && !photon) { PHX_CU(e->photon.ensure((size_t)N)); photon = e->photon.p; }
+    if (want_hits) PHX_CU(e->hitword.ensure((size_t)std::max<long long>(1, nword)));
+    SimArgs a;
+    a.S = scene_of(e, e->cfg.root_polish);
+    a.P = props_of(e);
+    a.C = loop_of(e);
+    a.gs = reinterpret_cast<const float4*>(d_gs);
+    a.gs_off = e->gs_off.p;
+    a.G = G;
+    a.N = N;
+    a.photon_offset = photon_offset;
+    a.event_index = (unsigned long long)event_index;
+    a.skip = e->cfg.skipahead_event_offset;
+    a.rng = e->rng.p;
+    a.rng_slots = e->rng_slots;
+    a.photon = photon;
+    a.seq = d_seq;
+    a.hitword = want_hits ? e->hitword.p : nullptr;
+    a.hit_mask = e->cfg.hit_mask;
+    a.status = e->status.p;
+    if (N > 0) {
+        const int B = 128;
+        k_simulate<<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        PHX_CU(cudaGetLastError());
+    }
+    long long nh = 0;
+    if (want_hits && N > 0) {
+        const long long nblock = (nword + 255) / 256;
+        PHX_CU(e->wordoff.ensure((size_t)nword));
+        PHX_CU(e->blocksum.ensure((size_t)nblock));
+        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(e->hitword.p, nword, e->wordoff.p, e->blocksum.p);
+        k_block_scan<<<1, 1024, 0, st>>>(e->blocksum.p, (int)nblock, e->counters.p);
+        if (d_sensor) PHX_CU(cudaMemsetAsync(d_sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
+        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(photon, N, e->hitword.p, e->wordoff.p, e->blocksum.p,
+                                                              d_hit, hit_capacity, d_sensor, e->cfg.num_sensor, e->status.p);
+        PHX_CU(cudaGetLastError());
+        PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, e->counters.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    } else if (d_sensor) {
+        PHX_CU(cudaMemsetAsync(d_sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
+    }
+    PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaStreamSynchronize(st));
+    if (want_hits && N > 0) memcpy(&nh, e->h_pinned + 2, sizeof(long long));
+    *num_hit = nh;
+    *status = e->h_pinned[0];
+    return 0;
+}
+
+int phx_simulate_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                        int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream)
+{
+    if (!e || !d_out) return phx_fail(-1, "phx_simulate_device: null argument");
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    long long nh = 0;
+    unsigned status = 0;
+    int rc = simulate_device_impl(e, d_gensteps, num_genstep, num_photon, event_index, photon_offset,
+                                  reinterpret_cast<phx_photon*>(d_out->photon), reinterpret_cast<phx_seq*>(d_out->seq),
+                                  reinterpret_cast<phx_photon*>(d_out->hit), d_out->hit_capacity, d_out->sensor_hits, &nh, &status, st);
+    if (rc) return rc;
+    d_out->num_photon = num_photon;
+    d_out->num_hit = nh;
+    d_out->status = status;
+    return 0;
+}
+
+int phx_simulate(phx_engine* e, const float* gensteps, int32_t num_genstep, int32_t event_index, phx_outputs* out)
+{
+    if (!e || !out || (num_genstep > 0 && !gensteps)) return phx_fail(-1, "phx_simulate: null argument");
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const long long N = phx_count_photons(gensteps, num_genstep);
+    PHX_CU(e->gs.ensure((size_t)std::max(1, num_genstep) * 6));
+    if (num_genstep > 0) PHX_CU(cudaMemcpyAsync(e->gs.p, gensteps, (size_t)num_genstep * 96, cudaMemcpyHostToDevice, st));
+    PHX_CU(e->photon.ensure((size_t)std::max<long long>(1, N)));
+    if (out->seq) PHX_CU(e->seq.ensure((size_t)std::max<long long>(1, N)));
+    if (out->hit) PHX_CU(e->hit.ensure((size_t)std::max<long long>(1, std::min<long long>(N, out->hit_capacity))));
+    if (out->sensor_hits) PHX_CU(e->sensor.ensure((size_t)std::max(1, e->cfg.num_sensor)));
+    long long nh = 0;
+    unsigned status = 0;
+    const long long hcap = std::min<long long>(N, out->hit_capacity);
+    int rc = simulate_device_impl(e, reinterpret_cast<const float*>(e->gs.p), num_genstep, N, event_index, 0, e->photon.p,
+                                  out->seq ? e->seq.p : nullptr, out->hit ? e->hit.p : nullptr, hcap,
+                                  out->sensor_hits ? e->sensor.p : nullptr, &nh, &status, st);
+    if (rc) return rc;
+    if (out->photon && N > 0) PHX_CU(cudaMemcpyAsync(out->photon, e->photon.p, (size_t)N * 64, cudaMemcpyDeviceToHost, st));
+    if (out->seq && N > 0) PHX_CU(cudaMemcpyAsync(out->seq, e->seq.p, (size_t)N * 32, cudaMemcpyDeviceToHost, st));
+    if (out->hit && nh > 0) PHX_CU(cudaMemcpyAsync(out->hit, e->hit.p, (size_t)std::min(nh, hcap) * 64, cudaMemcpyDeviceToHost, st));
+    if (out->sensor_hits && e->cfg.num_sensor > 0) PHX_CU(cudaMemcpyAsync(out->sensor_hits, e->sensor.p, (size_t)e->cfg.num_sensor * 4, cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaStreamSynchronize(st));
+    out->num_photon = N;
+    out->num_hit = nh;
+    out->status = status;
+    return 0;
+}
+
+int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d_rays, int64_t n, float* d_isect, int32_t polish, void* stream)
+{
+    if (!e || (n > 0 && (!d_rays || !d_isect))) return phx_fail(-1, "phx_csg_scan_device: null argument");
+    if (prim < 0 || prim >= e->num_prim) return phx_fail(-1, "phx_csg_scan_device: prim %d out of range", prim);
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
+    PhxCsgCtx csg;
+    csg.node = e->node.p;
+    csg.itra = e->itra.p;
+    csg.polish = polish;
+    if (n > 0) {
+        const int B = 128;
+        k_csg_scan<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
+        PHX_CU(cudaGetLastError());
+    }
+    return 0;
+}
+
+int phx_csg_scan(phx_engine* e, int32_t prim, float t_min, const float* rays, int64_t n, float* isect)
+{
+    if (!e || (n > 0 && (!rays || !isect))) return phx_fail(-1, "phx_csg_scan: null argument");
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    float* d_r = nullptr;
+    float* d_o = nullptr;
+    PHX_CU(cudaMallocAsync(&d_r, std::max<int64_t>(1, n) * 24, st));
+    PHX_CU(cudaMallocAsync(&d_o, std::max<int64_t>(1, n) * 16, st));
+    if (n > 0) PHX_CU(cudaMemcpyAsync(d_r, rays, n * 24, cudaMemcpyHostToDevice, st));
+    int rc = phx_csg_scan_device(e, prim, t_min, d_r, n, d_o, e->cfg.root_polish, st);
+    if (!rc && n > 0) {
+        cudaError_t ce = cudaMemcpyAsync(isect, d_o, n * 16, cudaMemcpyDeviceToHost, st);
+        if (ce != cudaSuccess) rc = phx_fail(-2, "phx_csg_scan: copy back failed: %s", cudaGetErrorString(ce));
+    }
+    cudaFreeAsync(d_r, st);
+    cudaFreeAsync(d_o, st);
+    PHX_CU(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int phx_rng_sequence(phx_engine* e, int32_t event_index, int64_t photon_offset, int64_t num_photon, int32_t num_per_photon, float* out)
+{
+    if (!e || !out || num_photon < 0 || num_per_photon <= 0 || photon_offset < 0) return phx_fail(-1, "phx_rng_sequence: bad argument");
+    PHX_CU(cudaSetDevice(e->device));
+    int rc = ensure_rng(e, photon_offset + num_photon);
+    if (rc) return rc;
+    cudaStream_t st = e->stream;
+    float* d_o = nullptr;
+    size_t bytes = (size_t)std::max<int64_t>(1, num_photon) * num_per_photon * sizeof(float);
+    PHX_CU(cudaMallocAsync(&d_o, bytes, st));
+    if (num_photon > 0) {
+        const int B = 128;
+        k_rng_sequence<<<(unsigned)((num_photon + B - 1) / B), B, 0, st>>>(e->rng.p, e->rng_slots,
+            e->cfg.skipahead_event_offset * (unsigned long long)event_index, photon_offset, num_photon, num_per_photon, d_o);
+        PHX_CU(cudaGetLastError());
+        PHX_CU(cudaMemcpyAsync(out, d_o, (size_t)num_photon * num_per_photon * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
+    cudaFreeAsync(d_o, st);
+    PHX_CU(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const int32_t* d_genstep_event,
+                                int32_t num_genstep, int64_t num_photon, int32_t block, int32_t chunk,
+                                int32_t regroup, phx_outputs* d_out, void* stream)
+{
+    (void)e; (void)d_gensteps; (void)d_genstep_event; (void)num_genstep; (void)num_photon;
+    (void)block; (void)chunk; (void)regroup; (void)d_out; (void)stream;
+    return phx_fail(-9, "phx_simulate_batched_device: not built yet");
+}
+
+int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                       int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
+                       float* d_hits, float* d_grad, void* stream)
+{
+    (void)e; (void)d_gensteps; (void)num_genstep; (void)num_photon; (void)event_index; (void)theta;
+    (void)mat_line; (void)wl_lo; (void)wl_hi; (void)d_hits; (void)d_grad; (void)stream;
+    return phx_fail(-9, "phx_adjoint_device: not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,188 @@
+// phx_kernels.cuh : device-side scene description, closest-hit traversal and the per-photon
+// bounce loop shared by the plain, batched and adjoint kernels.
+#pragma once
+#include "phx_pod.h"
+#include "phx_vec.cuh"
+#include "phx_csg.cuh"
+#include "phx_physics.cuh"
+
+#define PHX_BVH_STACK 48
+
+struct PhxScene {
+    const phx_bvh4_node* bvh;   // root at 0
+    const phx_leaf* leaves;
+    const float4* inst_inv;     // (num_inst*4) rows of the world->object 4x4 (row-vector convention)
+    PhxCsgCtx csg;
+    int empty;                  // no leaves at all
+};
+
+// Closest hit over all (instance, prim) leaves: restates optixTrace over the IAS with the
+// IS program CSGOptiX/CSGOptiX7.cu:896-967 (object-frame intersect_prim, lposcost) and the
+// CH program :776-874 (object->world normal, iindex<<16|identity, globalPrimIdx<<16|boundary).
+// Returns false for a miss (prd boundary 0xffff).
+PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float tmin, float tmax, PhxPRD& prd, unsigned& status)
+{
+    prd.gp_bd = 0xffffffffu;
+    prd.ii_id = 0xffffffffu;
+    prd.normal = make_float3(0.f, 0.f, 0.f);
+    prd.distance = 0.f;
+    prd.lposcost = 0.f;
+    if (S.empty) return false;
+    const float3 dd = make_float3(fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x,
+                                  fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y,
+                                  fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
+    const float3 inv = make_float3(1.f / dd.x, 1.f / dd.y, 1.f / dd.z);
+    const float3 oi = make_float3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
+    float best_t = tmax;
+    int best_leaf = -1;
+    float4 best_isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    float best_lposcost = 0.f;
+
+    int stk[PHX_BVH_STACK];
+    float stt[PHX_BVH_STACK];
+    int sp = 0;
+    stk[sp] = 0; stt[sp] = tmin; sp++;
+    while (sp > 0) {
+        sp--;
+        const int ni = stk[sp];
+        if (stt[sp] > best_t) continue;
+        const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
+        const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
+        const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
+        const int4 ch = __ldg(reinterpret_cast<const int4*>(nf + 6));
+        const float lxa[4] = { lx.x, lx.y, lx.z, lx.w }, hxa[4] = { hx.x, hx.y, hx.z, hx.w };
+        const float lya[4] = { ly.x, ly.y, ly.z, ly.w }, hya[4] = { hy.x, hy.y, hy.z, hy.w };
+        const float lza[4] = { lz.x, lz.y, lz.z, lz.w }, hza[4] = { hz.x, hz.y, hz.z, hz.w };
+        const int cha[4] = { ch.x, ch.y, ch.z, ch.w };
+        float tn[4];
+        int hitmask = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float tx0 = fmaf(lxa[c], inv.x, oi.x), tx1 = fmaf(hxa[c], inv.x, oi.x);
+            const float ty0 = fmaf(lya[c], inv.y, oi.y), ty1 = fmaf(hya[c], inv.y, oi.y);
+            const float tz0 = fmaf(lza[c], inv.z, oi.z), tz1 = fmaf(hza[c], inv.z, oi.z);
+            const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+            const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), best_t));
+            // slab arithmetic slack: boxes are padded on the host, and a relative slack here
+            tn[c] = tnear;
+            if (tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
+        }
+        // leaves first (closest box first), then push inner nodes far-to-near
+        int order[4] = { 0, 1, 2, 3 };
+#pragma unroll
+        for (int i = 1; i < 4; i++)
+#pragma unroll
+            for (int j = i; j > 0; j--) {
+                if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
+            }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int c = order[k];
+            if (!(hitmask & (1 << c))) continue;
+            const int child = cha[c];
+            if (child >= 0) continue;
+            if (tn[c] > best_t) continue;
+            const int enc = -child - 1;
+            const int first = enc >> 3;
+            const int count = (enc & 7) + 1;
+            for (int li = first; li < first + count; li++) {
+                const int4 L = __ldg(reinterpret_cast<const int4*>(S.leaves + li));
+                const float4* q = S.inst_inv + 4 * L.x;
+                float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
+                const float3 lo = xform_row(m, o, 1.f);
+                const float3 ld = xform_row(m, d, 0.f);
+                float4 is;
+                const bool valid = intersect_prim(is, S.csg, L.y, tmin, lo, ld, status);
+                if (valid && is.w < best_t) {
+                    best_t = is.w;
+                    best_leaf = li;
+                    best_isect = is;
+                    const float3 lpos = lo + is.w * ld;
+                    best_lposcost = lpos.z / sqrtf(dot(lpos, lpos));
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 3; k >= 0; k--) {
+            const int c = order[k];
+            if (!(hitmask & (1 << c))) continue;
+            const int child = cha[c];
+            if (child <= 0) continue;
+            if (tn[c] > best_t) continue;
+            if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
+            stk[sp] = child; stt[sp] = tn[c]; sp++;
+        }
+    }
+    if (best_leaf < 0) return false;
+    const int4 L = __ldg(reinterpret_cast<const int4*>(S.leaves + best_leaf));
+    const float4* q = S.inst_inv + 4 * L.x;
+    float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
+    prd.normal = xform_col(m, make_float3(best_isect.x, best_isect.y, best_isect.z), 0.f);
+    prd.distance = best_t;
+    prd.lposcost = best_lposcost;
+    prd.gp_bd = (unsigned)L.z;
+    prd.ii_id = (unsigned)L.w;
+    return true;
+}
+
+struct PhxLoopCfg {
+    int max_bounce;
+    float max_time;
+    float tmin, tmin0, tmax;
+    unsigned eps0_mask;
+};
+
+PHX_D void seq_add_nibble(unsigned long long* seqhis, unsigned long long* seqbnd, unsigned slot, unsigned flag, unsigned boundary)
+{
+    const unsigned iseq = slot / 16u;
+    const unsigned shift = 4u * (slot - iseq * 16u);
+    if (iseq < 2u) {
+        const unsigned long long f = (unsigned long long)(__ffs((int)flag) & 0xf);
+        const unsigned long long b = (unsigned long long)(boundary & 0xfu);
+        if (iseq == 0u) { seqhis[0] |= f << shift; seqbnd[0] |= b << shift; }
+        else            { seqhis[1] |= f << shift; seqbnd[1] |= b << shift; }
+    }
+}
+
+// The bounce loop of CSGOptiX/CSGOptiX7.cu:432-530 with sctx::point/end seq recording
+// (sysrap/sctx.h:134-185, sysrap/sseq.h:174-184) always on.
+PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene& S, const PhxProps& P, const PhxLoopCfg& C,
+                           unsigned long long* seqhis, unsigned long long* seqbnd, unsigned& status)
+{
+    int bounce = 0;
+    seq_add_nibble(seqhis, seqbnd, 0u, p.flag(), p.boundary());
+    while (bounce < C.max_bounce && p.time < C.max_time) {
+        const float tmin = (p.obf & C.eps0_mask) ? C.tmin0 : C.tmin;
+        PhxPRD prd;
+        phx_trace(S, p.pos, p.mom, tmin, C.tmax, prd, status);
+        if (prd.boundary() == 0xffffu) break;
+        prd.normal = normalize(prd.normal);
+        const int command = propagate(p, rng, prd, P, status);
+        bounce++;
+        seq_add_nibble(seqhis, seqbnd, (unsigned)bounce, p.flag(), p.boundary());
+        if (command == PHX_BREAK) break;
+    }
+}
+
+PHX_D void phx_load_rng(curandStateXORWOW& s, const uint32_t* rng, long long slots, long long slot)
+{
+    s.d = __ldg(rng + slot);
+    s.v[0] = __ldg(rng + slots * 1 + slot);
+    s.v[1] = __ldg(rng + slots * 2 + slot);
+    s.v[2] = __ldg(rng + slots * 3 + slot);
+    s.v[3] = __ldg(rng + slots * 4 + slot);
+    s.v[4] = __ldg(rng + slots * 5 + slot);
+    s.boxmuller_flag = 0;
+    s.boxmuller_flag_double = 0;
+    s.boxmuller_extra = 0.f;
+    s.boxmuller_extra_double = 0.0;
+}
+
+PHX_D void phx_store_photon(phx_photon* out, const PhxPhoton& p)
+{
+    float4* o = reinterpret_cast<float4*>(out);
+    o[0] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.time);
+    o[1] = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float(p.hitcount_iindex));
+    o[2] = make_float4(p.pol.x, p.pol.y, p.pol.z, p.wavelength);
+    o[3] = make_float4(__uint_as_float(p.obf), __uint_as_float(p.identity), __uint_as_float(p.index), __uint_as_float(p.flagmask));
+}

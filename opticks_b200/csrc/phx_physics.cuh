@@ -1,0 +1,577 @@
+// phx_physics.cuh : optical photon generation and one-bounce propagation physics.
+//
+// Each function restates the reference's device physics with the same random-number
+// consumption order and the same float operation order (bit-exact seqhis is the target):
+//   uniform_sphere          qudarap/qsim.h:180-201
+//   lambertian_direction    qudarap/qsim.h:433-486
+//   random_direction_marsaglia qudarap/qsim.h:554-575
+//   rayleigh_scatter        qudarap/qsim.h:604-692
+//   propagate_to_boundary   qudarap/qsim.h:721-866
+//   propagate_at_boundary   qudarap/qsim.h:1001-1208
+//   propagate_at_surface    qudarap/qsim.h:1680-1758
+//   reflect_diffuse/specular qudarap/qsim.h:1988-2093
+//   propagate (dispatch)    qudarap/qsim.h:2229-2338
+//   fill_state              qudarap/qbnd.h:108-224
+//   torch generation        sysrap/storch.h:192-520
+//   scintillation           qudarap/qscint.h:66-157, 251-258
+//   Cerenkov                qudarap/qcerenkov.h:56-137, 285-320
+// Random numbers are cuRAND XORWOW (called through curand_kernel.h, not reimplemented).
+#pragma once
+#include <curand_kernel.h>
+#include "phx_vec.cuh"
+#include "phx_pod.h"
+
+enum { PHX_CONTINUE = 0, PHX_BREAK = 1, PHX_BOUNDARY = 2 };
+
+struct PhxPhoton {
+    float3 pos; float time;
+    float3 mom; unsigned hitcount_iindex;
+    float3 pol; float wavelength;
+    unsigned obf; unsigned identity; unsigned index; unsigned flagmask;
+
+    PHX_D unsigned flag() const { return obf & 0xffffu; }
+    PHX_D unsigned boundary() const { return (obf & 0x7fff0000u) >> 16; }
+    PHX_D void set_flag(unsigned f) { obf = (obf & 0xffff0000u) | (f & 0xffffu); flagmask |= f; }
+    PHX_D void zero_flags() { obf = 0u; identity = 0u; index = 0u; flagmask = 0u; hitcount_iindex = 0u; }
+    PHX_D void set_index(unsigned long long full)
+    {
+        index = (unsigned)(full & 0xffffffffull);
+        identity = ((unsigned)((full >> 32) & 0xffull) << 24) | (identity & 0xffffffu);
+    }
+    // sphoton::set_prd  sysrap/sphoton.h:499-505
+    PHX_D void set_prd(unsigned bnd, unsigned id, float orient, unsigned ii)
+    {
+        obf = (obf & 0x8000ffffu) | ((bnd & 0x7fffu) << 16);
+        identity = (identity & 0xff000000u) | (id & 0x00ffffffu);
+        obf = (obf & 0x7fffffffu) | ((orient < 0.f ? 0x1u : 0x0u) << 31);
+        hitcount_iindex = 0x00010000u | (0x0000ffffu & ii);
+    }
+};
+
+// per-ray data returned by the closest-hit search (quad2 layout sysrap/squad.h:180-245)
+struct PhxPRD {
+    float3 normal; float distance;
+    float lposcost; unsigned ii_id; unsigned gp_bd;
+    PHX_D unsigned boundary() const { return gp_bd & 0xffffu; }
+    PHX_D unsigned identity() const { return ii_id & 0xffffu; }
+    PHX_D unsigned iindex() const { return ii_id >> 16; }
+};
+
+struct PhxState {
+    float4 material1;   // rindex, absorption length, scattering length, reemission prob
+    float4 m1group2;    // group velocity
+    float4 material2;
+    float4 surface;     // detect, absorb, reflect specular, reflect diffuse
+    uint4 optical;      // x: 1-based surface index (0: none) ; y: ems
+};
+
+struct PhxProps {
+    cudaTextureObject_t bnd_tex;    // (num_wl) x (num_bnd*4*2) float4, linear, normalized, wrap
+    const uint4* optical;           // (num_bnd*4)
+    float nm0, nms;                 // wavelength domain low and step (nm)
+    unsigned nx, ny;                // texture width/height
+    cudaTextureObject_t icdf_tex;   // 4096 x 3 float, linear, normalized, wrap
+    unsigned hd_factor;
+};
+
+PHX_D float phx_uniform(curandStateXORWOW& r) { return curand_uniform(&r); }
+
+PHX_D float4 boundary_lookup(const PhxProps& P, float nm, unsigned line, unsigned k)
+{
+    float fx = (nm - P.nm0) / P.nms;
+    float x = (fx + 0.5f) / float(P.nx);
+    unsigned iy = 2u * line + k;
+    float y = (float(iy) + 0.5f) / float(P.ny);
+    return tex2D<float4>(P.bnd_tex, x, y);
+}
+
+PHX_D void fill_state(PhxState& s, const PhxProps& P, unsigned boundary, float wavelength, float cosTheta)
+{
+    const int line = boundary * 4;
+    const int m1_line = cosTheta > 0.f ? line + 3 : line + 0;
+    const int m2_line = cosTheta > 0.f ? line + 0 : line + 3;
+    const int su_line = cosTheta > 0.f ? line + 2 : line + 1;
+    s.material1 = boundary_lookup(P, wavelength, m1_line, 0);
+    s.m1group2 = boundary_lookup(P, wavelength, m1_line, 1);
+    s.material2 = boundary_lookup(P, wavelength, m2_line, 0);
+    s.surface = boundary_lookup(P, wavelength, su_line, 0);
+    s.optical = __ldg(P.optical + su_line);
+}
+
+// hd20 inverse-CDF lookup qudarap/qscint.h:251-258 (hd10/hd0 for other tables)
+PHX_D float scint_wavelength(const PhxProps& P, float u0)
+{
+    if (P.hd_factor == 20u) {
+        const bool is_lhs = (u0 < 0.05f);
+        const bool is_rhs = (u0 > 0.95f);
+        const float x = is_lhs ? (u0 * 20.f) : (is_rhs ? (u0 - 0.95f) * 20.f : u0);
+        const float y = is_lhs ? 1.5f / 3.f : (is_rhs ? 2.5f / 3.f : 0.5f / 3.f);
+        return tex2D<float>(P.icdf_tex, x, y);
+    } else if (P.hd_factor == 10u) {
+        const bool is_lhs = (u0 < 0.1f);
+        const bool is_rhs = (u0 > 0.9f);
+        const float x = is_lhs ? (u0 * 10.f) : (is_rhs ? (u0 - 0.9f) * 10.f : u0);
+        const float y = is_lhs ? 1.5f / 3.f : (is_rhs ? 2.5f / 3.f : 0.5f / 3.f);
+        return tex2D<float>(P.icdf_tex, x, y);
+    } else if (P.hd_factor == 0u) {
+        return tex2D<float>(P.icdf_tex, u0, 0.5f / 3.f);
+    }
+    return 0.f;
+}
+
+PHX_D float3 uniform_sphere(float u0, float u1)
+{
+    float phi = u0 * 2.f * PHX_PI_F;
+    float cosTheta = 2.f * u1 - 1.f;
+    float sinTheta = sqrtf(1.f - cosTheta * cosTheta);
+    return make_float3(cosf(phi) * sinTheta, sinf(phi) * sinTheta, cosTheta);
+}
+
+// ---------------------------------------------------------------- generation
+// quad6 genstep access: g[0..5] float4 rows
+PHX_D void generate_torch(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id)
+{
+    const float4 q1 = g[1], q2 = g[2], q3 = g[3], q4 = g[4], q5 = g[5];
+    const unsigned numphoton = __float_as_uint(g[0].w);
+    const float3 gpos = make_float3(q1.x, q1.y, q1.z);
+    const float gtime = q1.w;
+    const float3 gmom = make_float3(q2.x, q2.y, q2.z);
+    const float gwl = q3.w;
+    const float2 zenith = make_float2(q4.x, q4.y);
+    const float2 azimuth = make_float2(q4.z, q4.w);
+    const float radius_ = q5.x;
+    const float distance = q5.y;
+    const unsigned type = __float_as_uint(q5.w);
+
+    if (type == PHX_T_DISC) {
+        p.wavelength = gwl; p.time = gtime; p.mom = gmom;
+        float u_zenith = zenith.x + phx_uniform(rng) * (zenith.y - zenith.x);
+        float u_azimuth = azimuth.x + phx_uniform(rng) * (azimuth.y - azimuth.x);
+        float r = radius_ * u_zenith;
+        float phi = 2.f * PHX_PI_F * u_azimuth;
+        float sinPhi = sinf(phi), cosPhi = cosf(phi);
+        p.pos = make_float3(r * cosPhi, r * sinPhi, 0.f);
+        rotate_uz(p.pos, p.mom);
+        p.pos = p.pos + gpos;
+        p.pol = make_float3(sinPhi, -cosPhi, 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_SPHERE || type == PHX_T_SPHERE_RANDPOL) {
+        p.wavelength = gwl; p.time = gtime;
+        float u_zenith = zenith.x + phx_uniform(rng) * (zenith.y - zenith.x);
+        float u_azimuth = azimuth.x + phx_uniform(rng) * (azimuth.y - azimuth.x);
+        float phi = 2.f * PHX_PI_F * u_azimuth;
+        float sinPhi = sinf(phi), cosPhi = cosf(phi);
+        float cosTheta = 1.f - 2.0f * u_zenith;
+        float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
+        float flip = copysignf(1.f, radius_);
+        p.mom = make_float3(flip * sinTheta * cosPhi, flip * sinTheta * sinPhi, flip * cosTheta);
+        float radius = fabsf(radius_);
+        p.pos = make_float3(sinTheta * cosPhi * radius, sinTheta * sinPhi * radius, cosTheta * radius);
+        float frac_twopi = type == PHX_T_SPHERE_RANDPOL ? phx_uniform(rng) : distance;
+        float phase = 2.f * PHX_PI_F * frac_twopi;
+        p.pol = make_float3(cosf(phase), sinf(phase), 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_SPHERE_MARSAGLIA) {
+        p.wavelength = gwl; p.time = gtime;
+        float u0z, u1a, u, v, b, a;
+        int count = 0;
+        do {
+            u0z = zenith.x + phx_uniform(rng) * (zenith.y - zenith.x);
+            u1a = azimuth.x + phx_uniform(rng) * (azimuth.y - azimuth.x);
+            u = 2.f * u0z - 1.f;
+            v = 2.f * u1a - 1.f;
+            b = u * u + v * v;
+        } while (b > 1.f && ++count < 100000);
+        a = 2.f * sqrtf(1.f - b);
+        float radius = fabsf(radius_);
+        float flip = copysignf(1.f, radius_);
+        p.mom = make_float3(flip * a * u, flip * a * v, flip * (2.f * b - 1.f));
+        p.pos = make_float3(a * u * radius, a * v * radius, (2.f * b - 1.f) * radius);
+        float phase = 2.f * PHX_PI_F * distance;
+        p.pol = make_float3(cosf(phase), sinf(phase), 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_LINE) {
+        p.wavelength = gwl; p.time = gtime; p.mom = gmom;
+        float frac = float(photon_id) / float(numphoton);
+        float sfrac = 2.f * (frac - 0.5f);
+        float r = radius_ * sfrac;
+        p.pos = make_float3(r, 0.f, 0.f);
+        rotate_uz(p.pos, p.mom);
+        p.pos = p.pos + gpos;
+        p.pol = make_float3(0.f, -1.f, 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_POINT) {
+        p.wavelength = gwl; p.time = gtime; p.mom = gmom;
+        p.pos = make_float3(0.f, 0.f, 0.f);
+        rotate_uz(p.pos, p.mom);
+        p.pos = p.pos + gpos;
+        p.pol = make_float3(0.f, -1.f, 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_CIRCLE) {
+        p.wavelength = gwl; p.time = gtime;
+        float f = float(photon_id) / float(numphoton);
+        float frac = azimuth.x * (1.f - f) + azimuth.y * (f);
+        float phi = 2.f * PHX_PI_F * frac;
+        float sinPhi = sinf(phi), cosPhi = cosf(phi);
+        float r = radius_ < 0.f ? -radius_ : radius_;
+        p.mom = make_float3(radius_ < 0.f ? -cosPhi : cosPhi, 0.f, radius_ < 0.f ? -sinPhi : sinPhi);
+        p.pos = make_float3(r * cosPhi, 0.f, r * sinPhi);
+        p.pos = p.pos + gpos;
+        p.pol = make_float3(0.f, -1.f, 0.f);
+        rotate_uz(p.pol, p.mom);
+    } else if (type == PHX_T_RECTANGLE) {
+        p.wavelength = gwl; p.time = gtime;
+        int side_size = (int)numphoton / 4;
+        int side = (int)photon_id / side_size;
+        int side_offset = side * side_size;
+        int side_index = (int)photon_id - side_offset;
+        float frac = float(side_index) / float(side_size);
+        if (side == 0 || side == 1) {
+            p.pos = make_float3(side == 0 ? azimuth.x : azimuth.y, 0.f, (1.f - frac) * zenith.x + frac * zenith.y);
+            p.mom = make_float3(side == 0 ? 1.f : -1.f, 0.f, 0.f);
+        } else if (side == 2 || side == 3) {
+            p.pos = make_float3((1.f - frac) * azimuth.x + frac * azimuth.y, 0.f, side == 2 ? zenith.x : zenith.y);
+            p.mom = make_float3(0.f, 0.f, side == 2 ? 1.f : -1.f);
+        }
+        p.pos = p.pos + gpos;
+        p.pol = make_float3(0.f, -1.f, 0.f);
+        rotate_uz(p.pol, p.mom);
+    }
+    p.zero_flags();
+    p.set_flag(PHX_TORCH);
+}
+
+PHX_D void scint_mom_pol_wavelength(PhxPhoton& p, curandStateXORWOW& rng, const PhxProps& P)
+{
+    float u0 = phx_uniform(rng);
+    float u1 = phx_uniform(rng);
+    float u2 = phx_uniform(rng);
+    float u3 = phx_uniform(rng);
+    float cost = 1.f - 2.f * u0;
+    float sint = sqrtf((1.f - cost) * (1.f + cost));
+    float phi = 2.f * PHX_PI_F * u1;
+    float sinp = sinf(phi);
+    float cosp = cosf(phi);
+    p.mom = make_float3(sint * cosp, sint * sinp, cost);
+    p.pol = make_float3(cost * cosp, cost * sinp, -sint);
+    phi = 2.f * PHX_PI_F * u2;
+    sinp = sinf(phi);
+    cosp = cosf(phi);
+    p.pol = normalize(cosp * p.pol + sinp * cross(p.mom, p.pol));
+    p.wavelength = scint_wavelength(P, u3);
+}
+
+PHX_D void generate_scint(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, const PhxProps& P)
+{
+    scint_mom_pol_wavelength(p, rng, P);
+    const float4 q1 = g[1], q2 = g[2], q3 = g[3], q5 = g[5];
+    const float charge = q3.y;
+    float fraction = charge == 0.f ? 1.f : phx_uniform(rng);
+    p.pos = make_float3(q1.x, q1.y, q1.z) + fraction * make_float3(q2.x, q2.y, q2.z);
+    float u4 = phx_uniform(rng);
+    float deltaTime = fraction * q2.w / q3.w - q5.x * logf(u4);
+    p.time = q1.w + deltaTime;
+    p.zero_flags();
+    p.set_flag(PHX_SCINTILLATION);
+}
+
+PHX_D void generate_cerenkov(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, const PhxProps& P, unsigned& status)
+{
+    const float4 q0 = g[0], q1 = g[1], q2 = g[2], q3 = g[3], q4 = g[4], q5 = g[5];
+    const unsigned matline = __float_as_uint(q0.z);
+    const float3 dpos = make_float3(q2.x, q2.y, q2.z);
+    const float step_length = q2.w;
+    const float preVelocity = q3.w;
+    const float BetaInverse = q4.x, Wmin = q4.y, Wmax = q4.z;
+    const float maxSin2 = q5.x, Mean1 = q5.y, Mean2 = q5.z, postVelocity = q5.w;
+    const float3 p0 = normalize(dpos);
+    float wavelength, cosTheta, sin2Theta;
+    {
+        float u0, u1, w, sampledRI, u_maxSin2;
+        unsigned count = 0;
+        do {
+            u0 = phx_uniform(rng);
+            w = Wmin + u0 * (Wmax - Wmin);
+            wavelength = Wmin * Wmax / w;
+            float4 props = boundary_lookup(P, wavelength, matline, 0u);
+            sampledRI = props.x;
+            cosTheta = BetaInverse / sampledRI;
+            sin2Theta = fmaxf(0.f, (1.f - cosTheta) * (1.f + cosTheta));
+            u1 = phx_uniform(rng);
+            u_maxSin2 = u1 * maxSin2;
+            count += 1;
+        } while (u_maxSin2 > sin2Theta && count < 100);
+        if (count >= 100 && u_maxSin2 > sin2Theta) status |= PHX_STATUS_LOOP_CAP;
+    }
+    float sinTheta = sqrtf(sin2Theta);
+    float u0 = phx_uniform(rng);
+    float phi = 2.f * PHX_PI_F * u0;
+    float sinPhi = sinf(phi);
+    float cosPhi = cosf(phi);
+    p.mom = make_float3(sinTheta * cosPhi, sinTheta * sinPhi, cosTheta);
+    rotate_uz(p.mom, p0);
+    p.pol = make_float3(cosTheta * cosPhi, cosTheta * sinPhi, -sinTheta);
+    rotate_uz(p.pol, p0);
+    p.wavelength = wavelength;
+    float fraction, delta;
+    {
+        float NumberOfPhotons, N, u;
+        float MeanMax = fmaxf(Mean1, Mean2);
+        float DeltaN = (Mean1 - Mean2);
+        unsigned count = 0;
+        do {
+            fraction = phx_uniform(rng);
+            delta = fraction * step_length;
+            NumberOfPhotons = Mean1 - fraction * DeltaN;
+            u = phx_uniform(rng);
+            N = u * MeanMax;
+        } while (N > NumberOfPhotons && ++count < 100000);
+        if (count >= 100000) status |= PHX_STATUS_LOOP_CAP;
+    }
+    float midVelocity = preVelocity + fraction * (postVelocity - preVelocity) * 0.5f;
+    p.time = q1.w + delta / midVelocity;
+    p.pos = make_float3(q1.x, q1.y, q1.z) + fraction * dpos;
+    p.zero_flags();
+    p.set_flag(PHX_CERENKOV);
+}
+
+// qsim::generate_photon qudarap/qsim.h:2532-2561
+PHX_D void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
+{
+    const int gencode = __float_as_int(g[0].x);
+    switch (gencode) {
+        case PHX_GS_TORCH: generate_torch(p, rng, g, photon_id); break;
+        case PHX_GS_G4Cerenkov_modified:
+        case PHX_GS_CERENKOV: generate_cerenkov(p, rng, g, P, status); break;
+        case PHX_GS_DsG4Scintillation_r4695:
+        case PHX_GS_SCINTILLATION: generate_scint(p, rng, g, P); break;
+        default: break;
+    }
+    p.set_index(photon_id);
+}
+
+// ---------------------------------------------------------------- propagation
+#define PHX_LOOP_CAP 1000000
+
+PHX_D void rayleigh_scatter(PhxPhoton& p, curandStateXORWOW& rng, unsigned& status)
+{
+    float3 direction, polarization;
+    bool looping = true;
+    int count = 0;
+    do {
+        float u0 = phx_uniform(rng);
+        float u1 = phx_uniform(rng);
+        float u2 = phx_uniform(rng);
+        float u3 = phx_uniform(rng);
+        float u4 = phx_uniform(rng);
+        float cosTheta = u0;
+        float sinTheta = sqrtf(1.0f - u0 * u0);
+        if (u1 < 0.5f) cosTheta = -cosTheta;
+        float sinPhi, cosPhi;
+        sincosf(2.f * PHX_PI_F * u2, &sinPhi, &cosPhi);
+        direction = make_float3(sinTheta * cosPhi, sinTheta * sinPhi, cosTheta);
+        rotate_uz(direction, p.mom);
+        float constant = -dot(direction, p.pol);
+        polarization.x = p.pol.x + constant * direction.x;
+        polarization.y = p.pol.y + constant * direction.y;
+        polarization.z = p.pol.z + constant * direction.z;
+        if (dot(polarization, polarization) == 0.f) {
+            sincosf(2.f * PHX_PI_F * u3, &sinPhi, &cosPhi);
+            polarization = make_float3(cosPhi, sinPhi, 0.f);
+            rotate_uz(polarization, direction);
+        } else {
+            if (u3 < 0.5f) polarization = -polarization;
+        }
+        polarization = normalize(polarization);
+        float doCosTheta = dot(polarization, p.pol);
+        float doCosTheta2 = doCosTheta * doCosTheta;
+        looping = doCosTheta2 < u4;
+    } while (looping && ++count < PHX_LOOP_CAP);
+    if (looping) status |= PHX_STATUS_LOOP_CAP;
+    p.mom = direction;
+    p.pol = polarization;
+}
+
+PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, float distance_to_boundary, const PhxProps& P, unsigned& status)
+{
+    const float absorption_length = s.material1.y;
+    const float scattering_length = s.material1.z;
+    const float reemission_prob = s.material1.w;
+    const float group_velocity = s.m1group2.x;
+    float u_scattering = phx_uniform(rng);
+    float u_absorption = phx_uniform(rng);
+    float scattering_distance = -scattering_length * logf(u_scattering);
+    float absorption_distance = -absorption_length * logf(u_absorption);
+    if (absorption_distance <= scattering_distance) {
+        if (absorption_distance <= distance_to_boundary) {
+            p.time += absorption_distance / group_velocity;
+            p.pos += absorption_distance * (p.mom);
+            float u_reemit = reemission_prob == 0.f ? 2.f : phx_uniform(rng);
+            if (u_reemit < reemission_prob) {
+                float u_re_wavelength = phx_uniform(rng);
+                float u_re_mom_ph = phx_uniform(rng);
+                float u_re_mom_ct = phx_uniform(rng);
+                float u_re_pol_ph = phx_uniform(rng);
+                float u_re_pol_ct = phx_uniform(rng);
+                p.wavelength = scint_wavelength(P, u_re_wavelength);
+                p.mom = uniform_sphere(u_re_mom_ph, u_re_mom_ct);
+                p.pol = normalize(cross(uniform_sphere(u_re_pol_ph, u_re_pol_ct), p.mom));
+                flag = PHX_BULK_REEMIT;
+                return PHX_CONTINUE;
+            } else {
+                flag = PHX_BULK_ABSORB;
+                return PHX_BREAK;
+            }
+        }
+    } else {
+        if (scattering_distance <= distance_to_boundary) {
+            p.time += scattering_distance / group_velocity;
+            p.pos += scattering_distance * (p.mom);
+            rayleigh_scatter(p, rng, status);
+            flag = PHX_BULK_SCATTER;
+            return PHX_CONTINUE;
+        }
+    }
+    p.pos += distance_to_boundary * (p.mom);
+    p.time += distance_to_boundary / group_velocity;
+    return PHX_BOUNDARY;
+}
+
+PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal)
+{
+    const float n1 = s.material1.x;
+    const float n2 = s.material2.x;
+    const float eta = n1 / n2;
+    const float _c1 = -dot(p.mom, normal);
+    const float3 oriented_normal = _c1 < 0.f ? -normal : normal;
+    const float3 trans = cross(p.mom, oriented_normal);
+    const float trans_length = length(trans);
+    const bool normal_incidence = trans_length < 1e-6f;
+    const float3 A_trans = normal_incidence ? p.pol : trans / trans_length;
+    const float E1_perp = dot(p.pol, A_trans);
+    const float c1 = fabsf(_c1);
+    const float c2c2 = 1.f - eta * eta * (1.f - c1 * c1);
+    bool tir = c2c2 < 0.f;
+    const float EdotN = dot(p.pol, oriented_normal);
+    const float c2 = tir ? 0.f : sqrtf(c2c2);
+    const float n1c1 = n1 * c1;
+    const float n2c2 = n2 * c2;
+    const float n2c1 = n2 * c1;
+    const float n1c2 = n1 * c2;
+    const float2 E1 = normal_incidence ? make_float2(0.f, 1.f) : make_float2(E1_perp, length(p.pol - (E1_perp * A_trans)));
+    const float2 E2_t = make_float2(2.f * n1c1 * E1.x / (n1c1 + n2c2), 2.f * n1c1 * E1.y / (n2c1 + n1c2));
+    const float2 E2_r = make_float2(E2_t.x - E1.x, (n2 * E2_t.y / n1) - E1.y);
+    const float2 RR = normalize2(E2_r);
+    const float2 TT = normalize2(E2_t);
+    const float TransCoeff = (tir || n1c1 == 0.f ? 0.f : n2c2 * dot2(E2_t, E2_t) / n1c1);
+    const float u_reflect = phx_uniform(rng);
+    bool reflect = u_reflect > TransCoeff;
+    p.mom = reflect ? p.mom + 2.0f * c1 * oriented_normal : eta * (p.mom) + (eta * c1 - c2) * oriented_normal;
+    const float3 A_paral = normalize(cross(p.mom, A_trans));
+    p.pol = normal_incidence ? (reflect ? p.pol * (n2 > n1 ? -1.f : 1.f) : p.pol)
+                             : (reflect ? (tir ? -p.pol + 2.f * EdotN * oriented_normal : RR.x * A_trans + RR.y * A_paral)
+                                        : TT.x * A_trans + TT.y * A_paral);
+    flag = reflect ? PHX_BOUNDARY_REFLECT : PHX_BOUNDARY_TRANSMIT;
+    return PHX_CONTINUE;
+}
+
+PHX_D void random_direction_marsaglia(float3& dir, curandStateXORWOW& rng)
+{
+    float u0, u1, u, v, b, a;
+    int count = 0;
+    do {
+        u0 = phx_uniform(rng);
+        u1 = phx_uniform(rng);
+        u = 2.f * u0 - 1.f;
+        v = 2.f * u1 - 1.f;
+        b = u * u + v * v;
+    } while (b > 1.f && ++count < PHX_LOOP_CAP);
+    a = 2.f * sqrtf(1.f - b);
+    dir.x = a * u;
+    dir.y = a * v;
+    dir.z = 2.f * b - 1.f;
+}
+
+PHX_D void lambertian_direction(float3& dir, const float3& normal, float orient, curandStateXORWOW& rng)
+{
+    float ndotv;
+    int count = 0;
+    float u;
+    do {
+        count++;
+        random_direction_marsaglia(dir, rng);
+        ndotv = dot(dir, normal) * orient;
+        if (ndotv < 0.f) {
+            dir = -1.f * dir;
+            ndotv = -1.f * ndotv;
+        }
+        u = phx_uniform(rng);
+    } while (!(u < ndotv) && (count < 1024));
+}
+
+PHX_D void reflect_diffuse(PhxPhoton& p, curandStateXORWOW& rng, const float3& normal)
+{
+    float3 old_mom = p.mom;
+    const float orient = dot(old_mom, normal) > 0.f ? -1.f : 1.f;
+    lambertian_direction(p.mom, normal, orient, rng);
+    float3 facet_normal = normalize(p.mom - old_mom);
+    const float EdotN = dot(p.pol, facet_normal);
+    p.pol = -1.f * (p.pol) + 2.f * EdotN * facet_normal;
+}
+
+PHX_D void reflect_specular(PhxPhoton& p, const float3& normal)
+{
+    const float PdotN = dot(p.mom, normal);
+    p.mom = p.mom - 2.f * PdotN * normal;
+    const float EdotN = dot(p.pol, normal);
+    p.pol = -1.f * (p.pol) + 2.f * EdotN * normal;
+}
+
+PHX_D int propagate_at_surface(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal)
+{
+    const float detect = s.surface.x;
+    const float absorb = s.surface.y;
+    const float reflect_diffuse_ = s.surface.w;
+    float u_surface = phx_uniform(rng);
+    int action = u_surface < absorb + detect ? PHX_BREAK : PHX_CONTINUE;
+    if (action == PHX_BREAK) {
+        flag = u_surface < absorb ? PHX_SURFACE_ABSORB : PHX_SURFACE_DETECT;
+    } else {
+        flag = u_surface < absorb + detect + reflect_diffuse_ ? PHX_SURFACE_DREFLECT : PHX_SURFACE_SREFLECT;
+        if (flag == PHX_SURFACE_DREFLECT) reflect_diffuse(p, rng, normal);
+        else reflect_specular(p, normal);
+    }
+    return action;
+}
+
+// qsim::propagate : returns CONTINUE/BREAK, sets the flag
+PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, const PhxProps& P, unsigned& status)
+{
+    const unsigned boundary = prd.boundary();
+    const unsigned identity = prd.identity();
+    const unsigned iindex = prd.iindex();
+    const float lposcost = prd.lposcost;
+    const float3 normal = prd.normal;
+    float cosTheta = dot(p.mom, normal);
+    p.set_prd(boundary, identity, cosTheta, iindex);
+    PhxState s;
+    fill_state(s, P, boundary, p.wavelength, cosTheta);
+    unsigned flag = 0;
+    int command = propagate_to_boundary(flag, p, rng, s, prd.distance, P, status);
+    if (command == PHX_BOUNDARY) {
+        const int ems = (int)s.optical.y;
+        if (ems == PHX_EMS_NOSURFACE) {
+            command = propagate_at_boundary(flag, p, rng, s, normal);
+        } else if (ems == PHX_EMS_SURFACE) {
+            command = propagate_at_surface(flag, p, rng, s, normal);
+        } else if (lposcost < 0.f) {
+            command = propagate_at_surface(flag, p, rng, s, normal);
+        } else if (ems == PHX_EMS_SURFACE_ZPLUS_SENSOR_A) {
+            (void)phx_uniform(rng);   // alignment burn of propagate_at_surface_Detect
+            flag = PHX_SURFACE_DETECT;
+            command = PHX_BREAK;
+        }
+    }
+    p.set_flag(flag);
+    return command;
+}

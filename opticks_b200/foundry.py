@@ -1,0 +1,259 @@
+"""CSGFoundry-layout geometry arrays built from Python.
+
+The arrays have the byte layouts of the reference's persisted CSGFoundry
+(CSG/CSGFoundry.cc:2769-2800 save, :2978-3016 load):
+
+* ``node``  (Nn,4,4) float32  CSGNode   CSG/CSGNode.h:60-100 (q1.u.z boundary, q3.u.z typecode,
+  q3.u.w gtransformIdx | complement<<31, q2/q3 bbox, root q0.u.x = subNum)
+* ``prim``  (Np,4,4)          CSGPrim   CSG/CSGPrim.h:40-100 (q0.i numNode,nodeOffset,tranOffset,planOffset;
+  q2/q3 bbox; q3.w globalPrimIdx)
+* ``solid`` (Ns,3,4) int32    CSGSolid  CSG/CSGSolid.h:37-48 (label[16], numPrim, primOffset, type, intent, center_extent)
+* ``inst``  (Ni,4,4) float32  qat4      sysrap/sqat4.h:345-389 (row-vector transform, identity ints in .w)
+* ``itra``/``tran`` (Nt,4,4)  node transforms (inverse / forward)
+
+so a foundry saved by the reference can be fed to the engine unchanged, and the synthetic
+scenes here can be written out in the same format.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# typecodes sysrap/OpticksCSG.h
+CSG_ZERO = 0
+CSG_UNION = 1
+CSG_INTERSECTION = 2
+CSG_DIFFERENCE = 3
+CSG_SPHERE = 101
+CSG_ZSPHERE = 103
+CSG_CYLINDER = 105
+CSG_BOX3 = 110
+CSG_TORUS = 116
+
+OPS = {"union": CSG_UNION, "intersection": CSG_INTERSECTION, "difference": CSG_DIFFERENCE}
+
+
+@dataclass
+class Node:
+    """One CSG node before serialisation; ``left``/``right`` only for operators."""
+    typecode: int
+    param: tuple = (0.0,) * 6
+    left: "Node | None" = None
+    right: "Node | None" = None
+    transform: np.ndarray | None = None   # 4x4 row-vector (object -> parent frame)
+    complement: bool = False
+    bbox: tuple | None = None             # local (object frame) box of this leaf
+
+    @property
+    def is_leaf(self) -> bool:
+        return self.typecode >= 100
+
+
+def sphere(r, center=(0.0, 0.0, 0.0)):
+    cx, cy, cz = center
+    return Node(CSG_SPHERE, (cx, cy, cz, r, 0.0, 0.0), bbox=(cx - r, cy - r, cz - r, cx + r, cy + r, cz + r))
+
+
+def zsphere(r, z1, z2, center=(0.0, 0.0, 0.0)):
+    """sphere radius r cut to z in [center.z+z1, center.z+z2] (zdelta in q1.xy)"""
+    cx, cy, cz = center
+    return Node(CSG_ZSPHERE, (cx, cy, cz, r, z1, z2), bbox=(cx - r, cy - r, cz + z1, cx + r, cy + r, cz + z2))
+
+
+def cylinder(r, z1, z2):
+    return Node(CSG_CYLINDER, (0.0, 0.0, 0.0, r, z1, z2), bbox=(-r, -r, z1, r, r, z2))
+
+
+def box3(fx, fy, fz):
+    return Node(CSG_BOX3, (fx, fy, fz, 0.0, 0.0, 0.0), bbox=(-fx / 2, -fy / 2, -fz / 2, fx / 2, fy / 2, fz / 2))
+
+
+def torus(rmajor, rminor):
+    """full-phi torus about z: param (rmin=0, rmax=rminor, rtor=rmajor, startPhi=0, deltaPhi=360)
+    as sysrap/sn.h:3323-3337 sn::Torus stores it"""
+    R, r = rmajor, rminor
+    return Node(CSG_TORUS, (0.0, r, R, 0.0, 360.0, 0.0), bbox=(-(R + r), -(R + r), -r, R + r, R + r, r))
+
+
+def op(name, a: Node, b: Node) -> Node:
+    return Node(OPS[name], left=a, right=b)
+
+
+def translate(n: Node, tx, ty, tz) -> Node:
+    m = np.eye(4)
+    m[3, :3] = (tx, ty, tz)
+    n.transform = m if n.transform is None else n.transform @ m
+    return n
+
+
+def _height(n: Node) -> int:
+    return 0 if n.is_leaf else 1 + max(_height(n.left), _height(n.right))
+
+
+def _bbox_transformed(bb, m):
+    if m is None:
+        return bb
+    pts = np.array([[bb[0 + 3 * (i & 1)], bb[1 + 3 * ((i >> 1) & 1)], bb[2 + 3 * ((i >> 2) & 1)], 1.0] for i in range(8)])
+    w = pts @ m
+    return tuple(w[:, :3].min(0)) + tuple(w[:, :3].max(0))
+
+
+def _tree_bbox(n: Node):
+    if n.is_leaf:
+        return _bbox_transformed(n.bbox, n.transform)
+    a, b = _tree_bbox(n.left), _tree_bbox(n.right)
+    if n.typecode == CSG_UNION:
+        return tuple(min(a[k], b[k]) for k in range(3)) + tuple(max(a[k], b[k]) for k in range(3, 6))
+    if n.typecode == CSG_INTERSECTION:
+        return tuple(max(a[k], b[k]) for k in range(3)) + tuple(min(a[k], b[k]) for k in range(3, 6))
+    return a   # difference bounded by A
+
+
+@dataclass
+class Foundry:
+    node: list = field(default_factory=list)
+    prim: list = field(default_factory=list)
+    solid: list = field(default_factory=list)
+    inst: list = field(default_factory=list)
+    tran: list = field(default_factory=list)
+    itra: list = field(default_factory=list)
+
+    # -------------------------------------------------------------- building
+    def _add_transform(self, m) -> int:
+        self.tran.append(np.asarray(m, dtype=np.float64))
+        self.itra.append(np.linalg.inv(np.asarray(m, dtype=np.float64)))
+        return len(self.tran)   # 1-based gtransformIdx
+
+    def add_prim(self, root: Node, boundary: int, mesh_idx: int = 0) -> int:
+        """Serialise a tree as a complete binary tree (level order, CSG_ZERO padding)."""
+        h = _height(root)
+        num = (1 << (h + 1)) - 1
+        slots: list[Node | None] = [None] * num
+
+        def place(n, i):
+            slots[i] = n
+            if not n.is_leaf:
+                place(n.left, 2 * i + 1)
+                place(n.right, 2 * i + 2)
+        place(root, 0)
+        offset = len(self.node)
+        for i, n in enumerate(slots):
+            q = np.zeros((4, 4), dtype=np.float32)
+            qu = q.view(np.uint32)
+            if n is None:
+                qu[3, 2] = CSG_ZERO
+            else:
+                if n.is_leaf:
+                    q[0, :4] = n.param[:4]
+                    q[1, :2] = n.param[4:6]
+                    bb = n.bbox
+                else:
+                    bb = _tree_bbox(n)
+                q[2, 0:3] = bb[0:3]
+                q[2, 3] = bb[3]
+                q[3, 0:2] = bb[4:6]
+                qu[3, 2] = n.typecode
+                tidx = self._add_transform(n.transform) if (n.is_leaf and n.transform is not None) else 0
+                qu[3, 3] = (tidx & 0x7FFFFFFF) | (0x80000000 if n.complement else 0)
+            qu[1, 2] = boundary
+            qu[1, 3] = i
+            self.node.append(q)
+        if not root.is_leaf:
+            self.node[offset].view(np.uint32)[0, 0] = num      # subNum
+        bb = _tree_bbox(root)
+        p = np.zeros((4, 4), dtype=np.float32)
+        pi = p.view(np.int32)
+        pi[0, 0] = num
+        pi[0, 1] = offset
+        pi[1, 1] = mesh_idx
+        pi[1, 3] = len(self.prim)
+        p[2, 0:3] = bb[0:3]
+        p[2, 3] = bb[3]
+        p[3, 0:2] = bb[4:6]
+        pi[3, 3] = len(self.prim)       # globalPrimIdx
+        self.prim.append(p)
+        return len(self.prim) - 1
+
+    def add_solid(self, label: str, prims: list[int]) -> int:
+        assert prims == list(range(prims[0], prims[0] + len(prims))), "prims of a solid must be contiguous"
+        s = np.zeros((3, 4), dtype=np.int32)
+        lab = label.encode()[:16].ljust(16, b"\0")
+        s[0, :] = np.frombuffer(lab, dtype=np.int32)
+        s[1, 0] = len(prims)
+        s[1, 1] = prims[0]
+        self.solid.append(s)
+        return len(self.solid) - 1
+
+    def add_inst(self, m, gas_idx: int, sensor_identifier: int = -1, sensor_index: int = -1) -> int:
+        """m : 4x4 row-vector object->world; sensor_identifier -1 means not a sensor (stored +1)"""
+        q = np.asarray(m, dtype=np.float32).copy()
+        qi = q.view(np.int32)
+        ins = len(self.inst)
+        qi[0, 3] = ins
+        qi[1, 3] = gas_idx
+        qi[2, 3] = sensor_identifier + 1
+        qi[3, 3] = sensor_index
+        self.inst.append(q)
+        return ins
+
+    # -------------------------------------------------------------- arrays
+    def arrays(self) -> dict:
+        def stack(lst, shape, dt):
+            return np.ascontiguousarray(np.stack(lst).astype(dt)) if lst else np.zeros((0,) + shape, dtype=dt)
+        return {
+            "node": stack(self.node, (4, 4), np.float32),
+            "prim": stack(self.prim, (4, 4), np.float32),
+            "solid": stack(self.solid, (3, 4), np.int32),
+            "inst": stack(self.inst, (4, 4), np.float32),
+            "tran": stack([m.astype(np.float32) for m in self.tran], (4, 4), np.float32),
+            "itra": stack([m.astype(np.float32) for m in self.itra], (4, 4), np.float32),
+            "plan": np.zeros((0, 4), dtype=np.float32),
+        }
+
+    def save(self, fold: str) -> None:
+        """write the arrays as CSGFoundry/*.npy"""
+        import os
+        os.makedirs(fold, exist_ok=True)
+        for k, v in self.arrays().items():
+            np.save(os.path.join(fold, f"{k}.npy"), v)
+
+
+def load_arrays(fold: str) -> dict:
+    """read CSGFoundry/{node,prim,solid,inst,itra,plan}.npy as written by the reference"""
+    import os
+    out = {}
+    for k in ("node", "prim", "solid", "inst", "itra", "plan", "tran"):
+        p = os.path.join(fold, f"{k}.npy")
+        if os.path.exists(p):
+            out[k] = np.load(p)
+    out.setdefault("plan", np.zeros((0, 4), dtype=np.float32))
+    out.setdefault("itra", np.zeros((0, 4, 4), dtype=np.float32))
+    return out
+
+
+def look_at_z(pos, target) -> np.ndarray:
+    """row-vector transform placing local +z along (target - pos), origin at pos"""
+    pos = np.asarray(pos, dtype=np.float64)
+    z = np.asarray(target, dtype=np.float64) - pos
+    z /= np.linalg.norm(z)
+    a = np.array([1.0, 0.0, 0.0]) if abs(z[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+    x = np.cross(a, z)
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    m = np.eye(4)
+    m[0, :3] = x
+    m[1, :3] = y
+    m[2, :3] = z
+    m[3, :3] = pos
+    return m
+
+
+def fibonacci_sphere(n: int, radius: float) -> np.ndarray:
+    i = np.arange(n, dtype=np.float64)
+    z = 1.0 - 2.0 * (i + 0.5) / n
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    ga = math.pi * (3.0 - math.sqrt(5.0))
+    phi = ga * i
+    return radius * np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1)

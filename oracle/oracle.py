@@ -1,0 +1,256 @@
+"""ctypes access to the checkers under oracle/ — TEST INFRASTRUCTURE ONLY.
+
+* ``liboracle.so``        C restatement of the simulate path (oracle.c) : CPU, FP32 + FP64 CSG
+* ``_ref/libref_csg.so``  the reference's own CSG intersector compiled for the CPU
+* ``_ref/libref_sim.so``  the reference's own qsim/CSG device code driven on the GPU
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and
+only as the checker / the timed CPU baseline.  Nothing in opticks_b200/ imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_CSG = os.path.join(HERE, "_ref", "libref_csg.so")
+REF_SIM = os.path.join(HERE, "_ref", "libref_sim.so")
+
+
+def build(ref: bool = False) -> None:
+    """make liboracle.so (and the reference builds when the reference checkout is present)"""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    if ref and os.path.isdir(os.environ.get("REF", "/root/reference")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+class OracleScene(C.Structure):
+    _fields_ = [
+        ("node", C.c_void_p), ("itra", C.c_void_p), ("inst_inv", C.c_void_p),
+        ("pair_inst", C.c_void_p), ("pair_node", C.c_void_p), ("pair_gpbd", C.c_void_p), ("pair_iiid", C.c_void_p),
+        ("num_pair", C.c_int),
+        ("bnd", C.c_void_p), ("bnd_w", C.c_int), ("bnd_h", C.c_int), ("nm0", C.c_float), ("nms", C.c_float),
+        ("optical", C.c_void_p), ("icdf", C.c_void_p), ("icdf_w", C.c_int), ("icdf_h", C.c_int), ("hd_factor", C.c_int),
+        ("max_bounce", C.c_int), ("max_time", C.c_float), ("tmin", C.c_float), ("tmin0", C.c_float),
+        ("eps0_mask", C.c_uint), ("hit_mask", C.c_uint), ("polish", C.c_int),
+        ("pair_bbox", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.oracle_simulate.restype = C.c_int
+        L.oracle_simulate.argtypes = [C.POINTER(OracleScene), C.c_void_p, C.c_int, C.c_longlong, C.c_longlong,
+                                      C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.oracle_csg_scan.restype = C.c_int
+        L.oracle_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p,
+                                      C.c_int, C.c_int]
+        L.oracle_csg_scan_t64.restype = C.c_int
+        L.oracle_csg_scan_t64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p]
+        L.oracle_csg_action.restype = C.c_int
+        L.oracle_csg_action.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+        L.oracle_tex2d_f1.restype = C.c_float
+        L.oracle_tex2d_f1.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.oracle_tex2d_f4.restype = None
+        L.oracle_tex2d_f4.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]
+        L.oracle_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def instance_pairs(geom: dict):
+    """(instance, prim) pairs in instance order with the IS/CH identity words, and world->object
+    inverses of the instance transforms (computed in double, stored float32)"""
+    node, prim, solid, inst = geom["node"], geom["prim"], geom["solid"], geom["inst"]
+    nu = node.view(np.uint32)
+    pi = prim.view(np.int32)
+    ii = inst.view(np.int32)
+    inv = np.zeros((len(inst), 4, 4), np.float32)
+    pin, pnode, pgb, pid = [], [], [], []
+    for i in range(len(inst)):
+        m = inst[i].astype(np.float64).copy()
+        m[:3, 3] = 0.0
+        m[3, 3] = 1.0
+        inv[i] = np.linalg.inv(m).astype(np.float32)
+        inv[i][:3, 3] = 0.0
+        inv[i][3, 3] = 1.0
+        gas = ii[i, 1, 3]
+        sid1 = ii[i, 2, 3]
+        num, off = solid[gas, 1, 0], solid[gas, 1, 1]
+        for p in range(off, off + num):
+            no = pi[p, 0, 1]
+            gpi = pi[p, 3, 3]
+            bnd = nu[no, 1, 2]
+            pin.append(i)
+            pnode.append(no)
+            pgb.append(((gpi & 0xFFFF) << 16) | (bnd & 0xFFFF))
+            pid.append(((i & 0xFFFF) << 16) | (sid1 & 0xFFFF))
+    return (inv, np.array(pin, np.int32), np.array(pnode, np.int32), np.array(pgb, np.uint32), np.array(pid, np.uint32))
+
+
+def pair_world_boxes(geom: dict, pin, pnode) -> np.ndarray:
+    """padded world AABB of each (instance, prim) pair from the CSGPrim box (q2,q3) and the
+    instance transform, in double; only used to skip hopeless pairs in the brute-force loop"""
+    prim, inst = geom["prim"], geom["inst"]
+    pi = prim.view(np.int32)
+    root_to_prim = {int(pi[p, 0, 1]): p for p in range(len(prim))}
+    out = np.zeros((len(pin), 6), np.float32)
+    for k, (i, no) in enumerate(zip(pin, pnode)):
+        p = root_to_prim[int(no)]
+        bb = np.array([prim[p, 2, 0], prim[p, 2, 1], prim[p, 2, 2], prim[p, 2, 3], prim[p, 3, 0], prim[p, 3, 1]], np.float64)
+        m = inst[i].astype(np.float64).copy()
+        m[:3, 3] = 0.0
+        m[3, 3] = 1.0
+        c = np.array([[bb[0 + 3 * (j & 1)], bb[1 + 3 * ((j >> 1) & 1)], bb[2 + 3 * ((j >> 2) & 1)], 1.0] for j in range(8)])
+        w = (c @ m)[:, :3]
+        lo, hi = w.min(0), w.max(0)
+        pad = 1e-3 * (hi - lo).max() + 1e-5 * np.abs(w).max() + 1e-2
+        out[k, :3] = lo - pad
+        out[k, 3:] = hi + pad
+    return out
+
+
+class Scene:
+    """keeps the arrays alive behind an OracleScene"""
+
+    def __init__(self, geom: dict, phys: dict, max_bounce=31, max_time=1e27, tmin=0.05, tmin0=0.05,
+                 eps0_mask=0x4 | 0x1 | 0x2 | 0x20 | 0x10, hit_mask=0x40, polish=0, cull=True):
+        self.node = np.ascontiguousarray(geom["node"], np.float32)
+        itra = geom.get("itra")
+        self.itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+        self.inst_inv, self.pin, self.pnode, self.pgb, self.pid = instance_pairs(geom)
+        self.bnd = np.ascontiguousarray(phys["bnd"], np.float32)
+        self.optical = np.ascontiguousarray(phys["optical"], np.uint32)
+        icdf = phys.get("icdf")
+        self.icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
+        nb, nwl = self.bnd.shape[0], self.bnd.shape[3]
+        self.pair_bbox = pair_world_boxes(geom, self.pin, self.pnode) if cull else None
+        self.s = OracleScene(
+            _p(self.node), _p(self.itra), _p(self.inst_inv), _p(self.pin), _p(self.pnode), _p(self.pgb), _p(self.pid),
+            len(self.pin), _p(self.bnd), nwl, nb * 8, float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)),
+            _p(self.optical), _p(self.icdf), 0 if self.icdf is None else self.icdf.shape[1],
+            0 if self.icdf is None else self.icdf.shape[0], int(phys.get("hd_factor", 20)),
+            max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox))
+
+    def simulate(self, gs: np.ndarray, uniforms: np.ndarray, first: int = 0):
+        gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
+        u = np.ascontiguousarray(uniforms, np.float32)
+        n, K = u.shape
+        photon = np.zeros((n, 4, 4), np.float32)
+        seq = np.zeros((n, 2, 2), np.uint64)
+        err = lib().oracle_simulate(C.byref(self.s), _p(gs), len(gs), first, n, _p(u), K, _p(photon), _p(seq))
+        return photon, seq, err
+
+
+def csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, use_double: bool = False, polish: bool = False):
+    node = np.ascontiguousarray(node, np.float32)
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[1]
+    out = np.zeros((n, 4), np.float32)
+    err = lib().oracle_csg_scan(_p(node), _p(itra), root, tmin, _p(rays), n, _p(out), int(use_double), int(polish))
+    return out, err
+
+
+def csg_scan_t64(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0):
+    node = np.ascontiguousarray(node, np.float32)
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[1]
+    t = np.zeros((n,), np.float64)
+    err = lib().oracle_csg_scan_t64(_p(node), _p(itra), root, tmin, _p(rays), n, _p(t))
+    return t, err
+
+
+def tex2d_f1(data: np.ndarray, x: float, y: float) -> float:
+    d = np.ascontiguousarray(data, np.float32)
+    H, W = d.shape[:2]
+    return lib().oracle_tex2d_f1(_p(d), W, H, x, y)
+
+
+# ---------------------------------------------------------------- reference builds
+def have_ref_csg() -> bool:
+    return os.path.exists(REF_CSG)
+
+
+def have_ref_sim() -> bool:
+    return os.path.exists(REF_SIM)
+
+
+def ref_csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, nthread: int = 0):
+    L = C.CDLL(REF_CSG)
+    L.ref_csg_scan.restype = C.c_int
+    L.ref_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p, C.c_int]
+    node = np.ascontiguousarray(node, np.float32)
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[1]
+    out = np.zeros((n, 4), np.float32)
+    L.ref_csg_scan(_p(node), _p(itra), root, tmin, _p(rays), n, _p(out), nthread or (os.cpu_count() or 1))
+    return out
+
+
+def ref_scan_gpu(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0):
+    L = C.CDLL(REF_SIM)
+    L.ref_scan_run.restype = C.c_int
+    L.ref_scan_run.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p]
+    node = np.ascontiguousarray(node, np.float32)
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[1]
+    out = np.zeros((n, 4), np.float32)
+    rc = L.ref_scan_run(_p(node), len(node), _p(itra), len(itra), root, tmin, _p(rays), n, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_scan_run failed {rc}")
+    return out
+
+
+def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 0, seed: int = 0, skip: int = 100000,
+                     max_bounce: int = 31, max_time: float = 1e27, tmin: float = 0.05, tmin0: float = 0.05,
+                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10):
+    """run the reference's qsim on the GPU through ref_sim.cu; returns photon (N,4,4), seq (N,2,2)"""
+    L = C.CDLL(REF_SIM)
+    f = L.ref_sim_run
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                  C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                  C.c_void_p, C.c_int, C.c_int, C.c_int,
+                  C.c_ulonglong, C.c_ulonglong, C.c_int,
+                  C.c_void_p, C.c_int, C.c_longlong,
+                  C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint,
+                  C.c_void_p, C.c_void_p]
+    node = np.ascontiguousarray(geom["node"], np.float32)
+    itra = geom.get("itra")
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    inv, pin, pnode, pgb, pid = instance_pairs(geom)
+    bnd = np.ascontiguousarray(phys["bnd"], np.float32)
+    optical = np.ascontiguousarray(phys["optical"], np.uint32)
+    icdf = phys.get("icdf")
+    icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
+    gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
+    N = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
+    photon = np.zeros((N, 4, 4), np.float32)
+    seq = np.zeros((N, 2, 2), np.uint64)
+    rc = f(_p(node), len(node), _p(itra), len(itra), _p(inv), len(inv), _p(pin), _p(pnode), _p(pgb), _p(pid), len(pin),
+           _p(bnd), bnd.shape[0], bnd.shape[3], float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)), _p(optical),
+           _p(icdf), 0 if icdf is None else icdf.shape[1], 0 if icdf is None else icdf.shape[0], int(phys.get("hd_factor", 20)),
+           seed, skip, event_index, _p(gs), len(gs), N, max_bounce, max_time, tmin, tmin0, eps0_mask, _p(photon), _p(seq))
+    if rc != 0:
+        raise RuntimeError(f"ref_sim_run failed {rc}")
+    return photon, seq

@@ -1,0 +1,65 @@
+"""Generate the committed golden fixtures under tests/golden/ from the reference's own code.
+
+csg_scan_ref.npz : rays and the intersects computed by the reference's CSG intersector
+                   (CSG/csg_intersect_tree.h etc. compiled for the CPU by oracle/Makefile `ref`
+                   into oracle/_ref/libref_csg.so) for the benchmark tree without the torus
+                   (the reference intersector has no torus leaf) and for each leaf alone.
+
+Run from the repository root where the reference checkout is present:
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from opticks_b200 import foundry as F  # noqa: E402
+from opticks_b200 import scenes  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def leaf_foundry():
+    fd = F.Foundry()
+    prims = []
+    for n in (F.sphere(240.0), F.zsphere(254.0, 0.0, 190.0), F.cylinder(250.0, -200.0, 200.0), F.box3(500.0, 500.0, 300.0)):
+        prims.append(fd.add_prim(n, 0))
+    # a complemented leaf and a transformed leaf inside small trees
+    a = F.sphere(200.0)
+    b = F.translate(F.box3(150.0, 150.0, 150.0), 50.0, -30.0, 120.0)
+    prims.append(fd.add_prim(F.op("intersection", a, b), 0))
+    c = F.cylinder(100.0, -300.0, 300.0)
+    c.complement = True
+    prims.append(fd.add_prim(F.op("intersection", F.sphere(250.0), c), 0))
+    fd.add_solid("leaves", prims)
+    fd.add_inst(np.eye(4), 0)
+    return fd, prims
+
+
+def main():
+    out = {}
+    fd, p = scenes.csg_scan_tree(with_torus=False)
+    A = fd.arrays()
+    rays = scenes.scan_rays(3000, seed=7, half=450.0)
+    root = int(A["prim"].view(np.int32)[p, 0, 1])
+    out["tree_node"] = A["node"]
+    out["tree_itra"] = A["itra"] if len(A["itra"]) else np.zeros((1, 4, 4), np.float32)
+    out["tree_root"] = np.int32(root)
+    out["tree_rays"] = rays
+    out["tree_isect"] = O.ref_csg_scan(A["node"], A["itra"], root, rays, 0.0)
+    fd2, prims = leaf_foundry()
+    B = fd2.arrays()
+    out["leaf_node"] = B["node"]
+    out["leaf_itra"] = B["itra"]
+    out["leaf_roots"] = np.array([int(B["prim"].view(np.int32)[q, 0, 1]) for q in prims], np.int32)
+    lr = scenes.scan_rays(1500, seed=11, half=400.0)
+    out["leaf_rays"] = lr
+    out["leaf_isect"] = np.stack([O.ref_csg_scan(B["node"], B["itra"], int(r), lr, 0.0) for r in out["leaf_roots"]])
+    np.savez_compressed(os.path.join(ROOT, "tests", "golden", "csg_scan_ref.npz"), **out)
+    print({k: getattr(v, "shape", v) for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,62 @@
+"""Full synthetic detector (17,612 instanced PMTs, scintillation with reemission) on the GPU:
+the BVH traversal + CSG + physics against the reference's device code (brute-force closest hit
+over all instances) and the CPU oracle, plus per-sensor hit counts."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from opticks_b200 import scenes
+from tests._parity import frac_close, seq_match
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def det(cuda):
+    from opticks_b200 import engine as E
+    fd, lib, icdf = scenes.detector()
+    phys = lib.arrays()
+    phys["icdf"] = icdf
+    gs = scenes.detector_gensteps(4, 1000, seed=1, lib=lib)
+    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=4000, num_sensor=scenes.NUM_PMT))
+    res = eng.simulate(gs, 0, sensor_hits=True)
+    yield dict(fd=fd, lib=lib, phys=phys, gs=gs, eng=eng, res=res)
+    eng.close()
+
+
+def test_detector_runs_clean(det):
+    from opticks_b200 import engine as E
+    r = det["res"]
+    assert r["status"] == 0, E.status_names(r["status"])
+    assert r["num_hit"] > 100
+    sh = r["sensor_hits"]
+    assert sh.sum() == r["num_hit"]
+    ids = r["hit"].view(np.uint32)[:, 3, 1] & 0xFFFFFF
+    np.testing.assert_array_equal(np.bincount(ids - 1, minlength=scenes.NUM_PMT), sh)
+
+
+@pytest.mark.skipif(not O.have_ref_sim(), reason="reference GPU build absent")
+def test_detector_matches_reference_device_code(det):
+    ph, sq = O.ref_simulate_gpu(det["fd"].arrays(), det["phys"], det["gs"])
+    r = det["res"]
+    m = seq_match(r["seq"], sq)
+    same = np.all(r["seq"][:, 0, :] == sq[:, 0, :], axis=1)
+    fc = frac_close(r["photon"], ph, same, 1e-4)
+    print(f"detector vs reference: seqhis match {m:.6f} close {fc:.6f}")
+    assert m >= 0.999
+    assert fc >= 0.999
+
+
+def test_detector_matches_cpu_oracle(det):
+    n = 600
+    u = det["eng"].rng_sequence(0, 0, n, 1024)
+    S = O.Scene(det["fd"].arrays(), det["phys"])
+    ph, sq, err = S.simulate(det["gs"], u, 0)
+    assert err & 1 == 0
+    r = det["res"]
+    m = seq_match(r["seq"][:n], sq)
+    same = np.all(r["seq"][:n, 0, :] == sq[:, 0, :], axis=1)
+    fc = frac_close(r["photon"][:n], ph, same, 1e-4)
+    print(f"detector vs CPU oracle: seqhis match {m:.6f} close {fc:.6f}")
+    assert m >= 0.995
+    assert fc >= 0.995

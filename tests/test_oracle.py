@@ -1,0 +1,131 @@
+"""The oracle (oracle/) pinned against the reference: golden intersects produced by the
+reference's own CSG intersector, the Kensler decision table, texture-filter emulation and
+physics invariants of the CPU restatement."""
+import os
+
+import numpy as np
+import pytest
+
+from tests.conftest import ROOT
+from oracle import oracle as O
+from opticks_b200 import engine_module, foundry as F, scenes
+
+GOLD = os.path.join(ROOT, "tests", "golden", "csg_scan_ref.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def test_oracle_csg_tree_matches_reference_golden_bit_exact(gold):
+    out, err = O.csg_scan(gold["tree_node"], gold["tree_itra"], int(gold["tree_root"]), gold["tree_rays"], 0.0)
+    ref = gold["tree_isect"]
+    assert err == 0
+    assert (ref[:, 3] > 0).sum() > 200
+    np.testing.assert_array_equal(out, ref)
+
+
+def test_oracle_csg_leaves_match_reference_golden_bit_exact(gold):
+    for k, root in enumerate(gold["leaf_roots"]):
+        out, err = O.csg_scan(gold["leaf_node"], gold["leaf_itra"], int(root), gold["leaf_rays"], 0.0)
+        ref = gold["leaf_isect"][k]
+        assert err == 0
+        assert (ref[:, 3] > 0).sum() > 20, k
+        np.testing.assert_array_equal(out, ref, err_msg=f"leaf prim {k}")
+
+
+@pytest.mark.skipif(not O.have_ref_csg(), reason="reference CPU build absent")
+def test_oracle_matches_live_reference_on_fresh_rays():
+    fd, p = scenes.csg_scan_tree(with_torus=False)
+    A = fd.arrays()
+    root = int(A["prim"].view(np.int32)[p, 0, 1])
+    rays = scenes.scan_rays(100000, seed=3, half=600.0)
+    ref = O.ref_csg_scan(A["node"], A["itra"], root, rays, 0.0)
+    out, err = O.csg_scan(A["node"], A["itra"], root, rays, 0.0)
+    np.testing.assert_array_equal(out, ref)
+
+
+def test_kensler_table_rules():
+    # spot checks of the single-hit CSG rules (A closer / B closer)
+    E, X, M = 0, 1, 2
+    act = O.lib().oracle_csg_action
+    assert act(1, E, E, 1) == 1 and act(1, E, E, 0) == 2        # union enter/enter : closer
+    assert act(1, E, X, 1) == 4 and act(1, X, E, 0) == 5        # union loops
+    assert act(1, M, M, 1) == 0
+    assert act(2, E, M, 1) == 0 and act(2, X, X, 0) == 2        # intersection
+    assert act(3, X, E, 0) == 3 and act(3, E, M, 0) == 1        # difference flips B
+    # the packed words of the reference's table (decoded from its published layout)
+    words = {(1, 1): 0x22121141, (1, 0): 0x22115122, (2, 1): 0x00014014, (2, 0): 0x00022055,
+             (3, 1): 0x00141141, (3, 0): 0x00133155}
+    for (op, ac), w in words.items():
+        for off in range(8):
+            assert act(op, off // 3, off % 3, ac) == (w >> (4 * off)) & 0xF
+
+
+def test_torus_fp64_hits_analytic_points():
+    fd = F.Foundry()
+    p = fd.add_prim(F.torus(200.0, 20.0), 0)
+    fd.add_solid("t", [p])
+    A = fd.arrays()
+    # rays along x through the tube centre line at z=0: entry at x = -(R+r) from the far side
+    o = np.array([[-1000.0, 0.0, 0.0], [0.0, 0.0, 500.0], [200.0, 0.0, 500.0]], np.float32).T
+    d = np.array([[1.0, 0.0, 0.0], [0.0, 0.0, -1.0], [0.0, 0.0, -1.0]], np.float32).T
+    rays = np.ascontiguousarray(np.concatenate([o, d]))
+    out, err = O.csg_scan(A["node"], A["itra"], 0, rays, 0.0, use_double=True)
+    assert err == 0
+    assert abs(out[0, 3] - (1000.0 - 220.0)) < 1e-3       # outer equator
+    assert out[1, 3] == 0.0                               # down the hole: miss
+    assert abs(out[2, 3] - (500.0 - 20.0)) < 1e-3         # top of the tube
+    np.testing.assert_allclose(out[2, :3], [0, 0, 1], atol=1e-6)
+
+
+def test_texture_emulation_linear_and_wrap():
+    data = np.arange(8, dtype=np.float32).reshape(1, 8)
+    # texel centres reproduce the samples
+    for i in range(8):
+        assert O.tex2d_f1(data, (i + 0.5) / 8, 0.5) == float(i)
+    # halfway between texels 2 and 3
+    assert O.tex2d_f1(data, 3.0 / 8, 0.5) == 2.5
+    # wrap: below texel 0 blends with the last texel
+    assert O.tex2d_f1(data, 0.0, 0.5) == 3.5
+
+
+def _c1_oracle(n=4000, seed=5, K=256):
+    fd, lib, icdf, gs = scenes.sphere_in_box(n)
+    S = O.Scene(fd.arrays(), lib.arrays())
+    u = np.random.default_rng(seed).random((n, K), dtype=np.float32)
+    return S.simulate(gs, u)
+
+
+def test_oracle_physics_invariants_sphere_in_box():
+    ph, seq, err = _c1_oracle()
+    assert err == 0
+    mom, pol = ph[:, 1, :3], ph[:, 2, :3]
+    np.testing.assert_allclose(np.linalg.norm(mom, axis=1), 1.0, atol=2e-5)
+    np.testing.assert_allclose(np.linalg.norm(pol, axis=1), 1.0, atol=2e-5)
+    assert np.abs((mom * pol).sum(1)).max() < 2e-4
+    flags = ph.view(np.uint32)[:, 3, 3]
+    E = engine_module()
+    lab = [E.seqhis_label(int(s[0, 0]), int(s[0, 1])) for s in seq]
+    sd = (flags & 0x40) != 0
+    # every detected photon ends on the box wall (|coordinate| = 1500 mm on one axis)
+    assert np.allclose(np.abs(ph[sd, 0, :3]).max(1), 1500.0, atol=0.05)
+    assert all(l.endswith("SD") for l, s in zip(lab, sd) if s)
+    assert all(l.startswith("TO") for l in lab)
+    # bulk absorption in 1 m of water with a 10 m absorption length: ~9.5 %
+    ab = np.mean([l.endswith("AB") for l in lab])
+    assert 0.06 < ab < 0.14
+    # seqhis nibbles are consistent with the flagmask
+    for s, fm in zip(seq[:500], flags[:500]):
+        nib = [(int(s[0, 0]) >> (4 * k)) & 0xF for k in range(16)]
+        m = 0
+        for v in nib:
+            if v:
+                m |= 1 << (v - 1)
+        assert m == fm
+
+
+def test_oracle_reports_exhausted_uniform_stream():
+    ph, seq, err = _c1_oracle(n=200, K=3)
+    assert err & 2
