@@ -84,7 +84,6 @@ PHX_D int phx_csg_lookup(int op, int sa, int sb, bool aCloser)
 struct PhxCsgCtx {
     const float4* node;   // (Nn*4) float4 : CSGNode table
     const float4* itra;   // (Nt*4) float4 : inverse node transforms
-    int polish;           // 1: FP64 root polish in quadratic leaves
 };
 
 PHX_D unsigned nd_u(const float4& q, int k) { return __float_as_uint(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w); }
@@ -127,7 +126,8 @@ PHX_D void polish_roots(float& t1, float& t2, double d, double b, double c)
 }
 
 // ---------------------------------------------------------------- leaves
-PHX_D bool leaf_sphere(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir, int polish)
+template <bool POLISH>
+PHX_D bool leaf_sphere(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir)
 {
     float3 center = make_float3(q0.x, q0.y, q0.z);
     float radius = q0.w;
@@ -138,7 +138,7 @@ PHX_D bool leaf_sphere(float4& isect, const float4& q0, float t_min, const float
     float d = dot(D, D);
     float root1, root2, disc, sdisc;
     robust_roots(root1, root2, disc, sdisc, d, b, c);
-    if (polish && sdisc > 0.f) {
+    if (POLISH && sdisc > 0.f) {
         double ox = (double)o.x - center.x, oy = (double)o.y - center.y, oz = (double)o.z - center.z;
         double bb = ox * D.x + oy * D.y + oz * D.z;
         double cc = ox * ox + oy * oy + oz * oz - (double)radius * radius;
@@ -156,7 +156,8 @@ PHX_D bool leaf_sphere(float4& isect, const float4& q0, float t_min, const float
     return valid;
 }
 
-PHX_D bool leaf_zsphere(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir, int polish)
+template <bool POLISH>
+PHX_D bool leaf_zsphere(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir)
 {
     const float3 center = make_float3(q0.x, q0.y, q0.z);
     float3 O = o - center;
@@ -170,7 +171,7 @@ PHX_D bool leaf_zsphere(float4& isect, const float4& q0, const float4& q1, float
     float d = dot(D, D);
     float t1sph, t2sph, disc, sdisc;
     robust_roots(t1sph, t2sph, disc, sdisc, d, b, c);
-    if (polish && sdisc > 0.f) {
+    if (POLISH && sdisc > 0.f) {
         double ox = (double)o.x - center.x, oy = (double)o.y - center.y, oz = (double)o.z - center.z;
         double bb = ox * D.x + oy * D.y + oz * D.z;
         double cc = ox * ox + oy * oy + oz * oz - (double)radius * radius;
@@ -209,7 +210,8 @@ PHX_D bool leaf_zsphere(float4& isect, const float4& q0, const float4& q1, float
     return valid;
 }
 
-PHX_D bool leaf_cylinder(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir, int polish)
+template <bool POLISH>
+PHX_D bool leaf_cylinder(float4& isect, const float4& q0, const float4& q1, float t_min, const float3& o, const float3& dir)
 {
     const float r = q0.w;
     const float z1 = q1.x;
@@ -222,7 +224,7 @@ PHX_D bool leaf_cylinder(float4& isect, const float4& q0, const float4& q1, floa
     const float c = ox * ox + oy * oy - r2;
     float t_near, t_far, disc, sdisc;
     robust_roots_disq(t_min, t_near, t_far, disc, sdisc, a, b, c);
-    if (polish && sdisc > 0.f) {
+    if (POLISH && sdisc > 0.f) {
         double aa = (double)vx * vx + (double)vy * vy;
         double bb = (double)ox * vx + (double)oy * vy;
         double cc = (double)ox * ox + (double)oy * oy - (double)r * r;
@@ -409,6 +411,7 @@ PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3
 }
 
 // ---------------------------------------------------------------- leaf with transform
+template <bool POLISH>
 PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
 {
     isect = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -430,9 +433,9 @@ PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min
     float3 direction = q ? xform_row(q, ray_d, 0.f) : ray_d;
     bool valid = false;
     switch (typecode) {
-        case PHX_CSG_SPHERE:   valid = leaf_sphere(isect, q0, t_min, origin, direction, g.polish); break;
-        case PHX_CSG_ZSPHERE:  valid = leaf_zsphere(isect, q0, q1, t_min, origin, direction, g.polish); break;
-        case PHX_CSG_CYLINDER: valid = leaf_cylinder(isect, q0, q1, t_min, origin, direction, g.polish); break;
+        case PHX_CSG_SPHERE:   valid = leaf_sphere<POLISH>(isect, q0, t_min, origin, direction); break;
+        case PHX_CSG_ZSPHERE:  valid = leaf_zsphere<POLISH>(isect, q0, q1, t_min, origin, direction); break;
+        case PHX_CSG_CYLINDER: valid = leaf_cylinder<POLISH>(isect, q0, q1, t_min, origin, direction); break;
         case PHX_CSG_BOX3:     valid = leaf_box3(isect, q0, t_min, origin, direction); break;
         case PHX_CSG_TORUS:    valid = leaf_torus(isect, q0, t_min, origin, direction, err); break;
         default: break;
@@ -457,6 +460,7 @@ PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
 #define PHX_POSTORDER_NEXT(i, elev) (((i) & 1u) ? (i) >> 1 : ((i) << (elev)) + (1u << (elev)))
 
 // ---------------------------------------------------------------- tree
+template <bool POLISH>
 PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
 {
     const unsigned numNode = __float_as_uint(__ldg(g.node + 4 * root).x);   // subNum
@@ -484,7 +488,7 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
             if (typecode == PHX_CSG_ZERO) { nodeIdx = PHX_POSTORDER_NEXT(nodeIdx, elevation); continue; }
             if (typecode >= PHX_CSG_NODE) {
                 float4 nd_isect;
-                intersect_leaf(nd_isect, g, ni, tmin, o, d, err);
+                intersect_leaf<POLISH>(nd_isect, g, ni, tmin, o, d, err);
                 nd_isect.w = copysignf(nd_isect.w, nodeIdx % 2u == 0u ? -1.f : 1.f);
                 if (sp >= PHX_CSG_STACK - 1) { ierr |= PHX_CSG_ERR_OVERFLOW; break; }
                 stk[++sp] = nd_isect;
@@ -546,12 +550,14 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
     return isect.w > 0.f;
 }
 
-// one prim: leaf at the root, or a boolean tree
+// one prim: leaf at the root, or a boolean tree.  POLISH selects the FP64 root polish at
+// compile time so the default path keeps the reference's FP32 expression structure.
+template <bool POLISH>
 PHX_D bool intersect_prim(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
 {
     const unsigned typecode = __float_as_uint(__ldg(g.node + 4 * root + 3).z);
     isect = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (typecode >= PHX_CSG_LEAF) return intersect_leaf(isect, g, root, t_min, o, d, err);
-    if (typecode < PHX_CSG_NODE) return intersect_tree(isect, g, root, t_min, o, d, err);
+    if (typecode >= PHX_CSG_LEAF) return intersect_leaf<POLISH>(isect, g, root, t_min, o, d, err);
+    if (typecode < PHX_CSG_NODE) return intersect_tree<POLISH>(isect, g, root, t_min, o, d, err);
     return false;
 }

@@ -103,7 +103,7 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.inst_inv = e->inst_inv.p;
     S.csg.node = e->node.p;
     S.csg.itra = e->itra.p;
-    S.csg.polish = polish;
+    (void)polish;
     S.empty = e->num_leaf == 0;
     return S;
 }
@@ -215,6 +215,7 @@ struct SimArgs {
 };
 
 // one thread per photon : CSGOptiX/CSGOptiX7.cu:432-530 simulate()
+template <bool POLISH>
 __global__ void __launch_bounds__(128) k_simulate(SimArgs a)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(128) k_simulate(SimArgs a)
         memset(&p, 0, sizeof(p));
         generate_photon(p, rng, g, (unsigned long long)photon_idx, a.P, status);
         unsigned long long seqhis[2] = { 0ull, 0ull }, seqbnd[2] = { 0ull, 0ull };
-        phx_bounce_loop(p, rng, a.S, a.P, a.C, seqhis, seqbnd, status);
+        phx_bounce_loop<POLISH>(p, rng, a.S, a.P, a.C, seqhis, seqbnd, status);
         if (a.photon) phx_store_photon(a.photon + idx, p);
         if (a.seq) {
             ulonglong2* s = reinterpret_cast<ulonglong2*>(a.seq + idx);
@@ -331,6 +332,7 @@ __global__ void k_compact(const phx_photon* photon, long long N, const uint32_t*
 }
 
 // CSGScan : one thread per ray, SoA rays
+template <bool POLISH>
 __global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* rays, long long n, float4* out, unsigned* status)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -339,7 +341,7 @@ __global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* ra
     const float3 d = make_float3(__ldg(rays + 3 * n + i), __ldg(rays + 4 * n + i), __ldg(rays + 5 * n + i));
     unsigned st = 0;
     float4 is;
-    const bool valid = intersect_prim(is, csg, root, t_min, o, d, st);
+    const bool valid = intersect_prim<POLISH>(is, csg, root, t_min, o, d, st);
     out[i] = valid ? is : make_float4(0.f, 0.f, 0.f, 0.f);
     if (st) atomicOr(status, st);
 }
@@ -652,7 +654,8 @@ static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long lo
     a.status = e->status.p;
     if (N > 0) {
         const int B = 128;
-        k_simulate<<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
         PHX_CU(cudaGetLastError());
     }
     long long nh = 0;
@@ -736,10 +739,11 @@ int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d
     PhxCsgCtx csg;
     csg.node = e->node.p;
     csg.itra = e->itra.p;
-    csg.polish = polish;
     if (n > 0) {
         const int B = 128;
-        k_csg_scan<<<(unsigned)((n + B - 1) / B), B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
+        const unsigned grid = (unsigned)((n + B - 1) / B);
+        if (polish) k_csg_scan<true><<<grid, B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
+        else k_csg_scan<false><<<grid, B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
         PHX_CU(cudaGetLastError());
     }
     return 0;

@@ -20,6 +20,7 @@ struct PhxScene {
 // IS program CSGOptiX/CSGOptiX7.cu:896-967 (object-frame intersect_prim, lposcost) and the
 // CH program :776-874 (object->world normal, iindex<<16|identity, globalPrimIdx<<16|boundary).
 // Returns false for a miss (prd boundary 0xffff).
+template <bool POLISH>
 PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float tmin, float tmax, PhxPRD& prd, unsigned& status)
 {
     prd.gp_bd = 0xffffffffu;
@@ -92,7 +93,7 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                 const float3 lo = xform_row(m, o, 1.f);
                 const float3 ld = xform_row(m, d, 0.f);
                 float4 is;
-                const bool valid = intersect_prim(is, S.csg, L.y, tmin, lo, ld, status);
+                const bool valid = intersect_prim<POLISH>(is, S.csg, L.y, tmin, lo, ld, status);
                 if (valid && is.w < best_t) {
                     best_t = is.w;
                     best_leaf = li;
@@ -146,6 +147,7 @@ PHX_D void seq_add_nibble(unsigned long long* seqhis, unsigned long long* seqbnd
 
 // The bounce loop of CSGOptiX/CSGOptiX7.cu:432-530 with sctx::point/end seq recording
 // (sysrap/sctx.h:134-185, sysrap/sseq.h:174-184) always on.
+template <bool POLISH>
 PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene& S, const PhxProps& P, const PhxLoopCfg& C,
                            unsigned long long* seqhis, unsigned long long* seqbnd, unsigned& status)
 {
@@ -154,7 +156,7 @@ PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene&
     while (bounce < C.max_bounce && p.time < C.max_time) {
         const float tmin = (p.obf & C.eps0_mask) ? C.tmin0 : C.tmin;
         PhxPRD prd;
-        phx_trace(S, p.pos, p.mom, tmin, C.tmax, prd, status);
+        phx_trace<POLISH>(S, p.pos, p.mom, tmin, C.tmax, prd, status);
         if (prd.boundary() == 0xffffu) break;
         prd.normal = normalize(prd.normal);
         const int command = propagate(p, rng, prd, P, status);

@@ -7,27 +7,25 @@ def seq_match(a, b):
     return float(np.mean(np.all(a[:, 0, :] == b[:, 0, :], axis=1)))
 
 
-def photon_close(a, b, sel, rtol=1e-4, atol_mm=1e-2):
-    """max relative deviation of pos/time/mom/pol over the selected photons"""
-    if not sel.any():
-        return 0.0
-    pa, pb = a[sel], b[sel]
-    scale = np.maximum(np.abs(pb[:, 0, :3]).max(1, keepdims=True), 1.0)
-    dpos = (np.abs(pa[:, 0, :3] - pb[:, 0, :3]) / scale).max()
-    dt = (np.abs(pa[:, 0, 3] - pb[:, 0, 3]) / np.maximum(np.abs(pb[:, 0, 3]), 1e-3)).max()
-    dmom = np.abs(pa[:, 1, :3] - pb[:, 1, :3]).max()
-    dpol = np.abs(pa[:, 2, :3] - pb[:, 2, :3]).max()
-    return float(max(dpos, dt, dmom, dpol))
+def close_mask(a, b, rtol=1e-4):
+    """per-photon: position, time, direction and polarisation within rtol (relative to the
+    position scale, the time, and unit vectors respectively)"""
+    scale = np.maximum(np.abs(b[:, 0, :3]).max(1), 1.0)
+    pos = np.abs(a[:, 0, :3] - b[:, 0, :3]).max(1) <= rtol * scale
+    tim = np.abs(a[:, 0, 3] - b[:, 0, 3]) <= rtol * np.maximum(np.abs(b[:, 0, 3]), 1.0)
+    mom = np.abs(a[:, 1, :3] - b[:, 1, :3]).max(1) <= rtol
+    pol = np.abs(a[:, 2, :3] - b[:, 2, :3]).max(1) <= rtol
+    return pos, tim, mom, pol
 
 
 def frac_close(a, b, sel, rtol=1e-4):
-    """fraction of selected photons whose pos, time, mom, pol agree within rtol"""
-    pa, pb = a[sel], b[sel]
-    if len(pa) == 0:
+    """fraction of selected photons whose pos, time, mom, pol all agree within rtol"""
+    if not sel.any():
         return 1.0
-    scale = np.maximum(np.abs(pb[:, 0, :3]).max(1), 1.0)
-    ok = (np.abs(pa[:, 0, :3] - pb[:, 0, :3]).max(1) <= rtol * scale)
-    ok &= np.abs(pa[:, 0, 3] - pb[:, 0, 3]) <= rtol * np.maximum(np.abs(pb[:, 0, 3]), 1.0)
-    ok &= np.abs(pa[:, 1, :3] - pb[:, 1, :3]).max(1) <= 10 * rtol
-    ok &= np.abs(pa[:, 2, :3] - pb[:, 2, :3]).max(1) <= 10 * rtol
-    return float(ok.mean())
+    pos, tim, mom, pol = close_mask(a[sel], b[sel], rtol)
+    return float(np.mean(pos & tim & mom & pol))
+
+
+def describe(a, b, sel, rtol=1e-4):
+    pos, tim, mom, pol = close_mask(a[sel], b[sel], rtol)
+    return f"pos {pos.mean():.6f} time {tim.mean():.6f} mom {mom.mean():.6f} pol {pol.mean():.6f}"

@@ -17,8 +17,8 @@ def det(cuda):
     fd, lib, icdf = scenes.detector()
     phys = lib.arrays()
     phys["icdf"] = icdf
-    gs = scenes.detector_gensteps(4, 1000, seed=1, lib=lib)
-    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=4000, num_sensor=scenes.NUM_PMT))
+    gs = scenes.detector_gensteps(2, 1000, seed=1, lib=lib)
+    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=2000, num_sensor=scenes.NUM_PMT))
     res = eng.simulate(gs, 0, sensor_hits=True)
     yield dict(fd=fd, lib=lib, phys=phys, gs=gs, eng=eng, res=res)
     eng.close()
