@@ -102,6 +102,22 @@ int phx_simulate(phx_engine* e, const float* gensteps, int32_t num_genstep, int3
 int phx_simulate_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                         int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream);
 
+/* Allocation-free variant of phx_simulate_device.  No counterpart in the reference.
+ * For callers that cannot allocate device memory per call (a framework whose caching allocator owns
+ * all device memory, or a per-event loop that cannot take the device-wide synchronisation that
+ * cudaMalloc/cudaFree may imply): it calls no cudaMalloc, cudaFree or allocating library routine.
+ * Its scratch is one fixed device array in the library (about 2.6 MB, held on every GPU that loads
+ * the library until the process exits), sized for at most 8,388,608 photons and 65,536 gensteps per
+ * call; larger calls are rejected with an error.  Inputs and outputs are the caller's device
+ * buffers as for phx_simulate_device; when hits or sensor counts are requested the photon output
+ * must be given (hits are selected from it).  The photons must lie within the RNG slots prepared at
+ * phx_create (config max_photon); otherwise the call is rejected rather than growing them.
+ * The first call on a device looks up the device address of the scratch array (once per device);
+ * make that first call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (on any engine of the same device) race; serialise them. */
+int phx_simulate_device_noalloc(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                                int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream);
+
 /* many events in one persistent launch: gensteps (num_genstep,6,4) with genstep_event[g] the event index
  * of genstep g (non-decreasing).  Outputs are the concatenation of the events' photons in genstep order;
  * event_photon_offset (num_event+1) receives the photon offsets of the events (host array). */

@@ -61,6 +61,8 @@ SIGNATURES = {
     "phx_simulate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(PhxOutputs)]),
     "phx_simulate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int64, C.POINTER(PhxOutputs),
                                       C.c_void_p]),
+    "phx_simulate_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int64,
+                                              C.POINTER(PhxOutputs), C.c_void_p]),
     "phx_simulate_batched_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int32,
                                               C.c_int32, C.POINTER(PhxOutputs), C.c_void_p]),
     "phx_csg_scan": (C.c_int, [C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p]),

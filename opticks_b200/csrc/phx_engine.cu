@@ -811,3 +811,124 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free simulate
+// Some callers cannot allocate device memory per call: a framework whose caching allocator owns
+// every device byte, or a per-event loop that cannot afford the device-wide synchronisation that
+// cudaMalloc/cudaFree may imply.  phx_simulate_device_noalloc serves them: its scratch (genstep
+// offsets, hit bit words and their prefix sums, counters, status) lives in one fixed file-scope
+// device array instead of engine buffers that grow on demand.  The array below is sized for
+// PHX_NOALLOC_MAX_PHOTON photons and PHX_NOALLOC_MAX_GENSTEP gensteps per call (about 2.6 MB)
+// and is held on every GPU that loads this library until the process exits.
+#define PHX_NOALLOC_MAX_PHOTON (1ll << 23)
+#define PHX_NOALLOC_MAX_GENSTEP 65536
+#define PHX_NOALLOC_WORDS (PHX_NOALLOC_MAX_PHOTON / 32)
+#define PHX_NOALLOC_BLOCKS (PHX_NOALLOC_WORDS / 256)
+
+struct PhxNoAllocScratch {
+    long long gs_off[PHX_NOALLOC_MAX_GENSTEP + 1];
+    uint32_t hitword[PHX_NOALLOC_WORDS];
+    uint32_t wordoff[PHX_NOALLOC_WORDS];
+    uint32_t blocksum[PHX_NOALLOC_BLOCKS];
+    long long counters[8];
+    unsigned status[8];
+};
+
+static __device__ __align__(256) PhxNoAllocScratch g_phx_noalloc_scratch;
+
+// In host code the symbol above is only a host-side stand-in, never a device address.  The
+// device address is looked up once per device, with that device current, and cached.
+#include <mutex>
+static std::mutex g_phx_noalloc_mu;
+static PhxNoAllocScratch* g_phx_noalloc_ptr[128] = {};
+
+static int noalloc_scratch(int device, PhxNoAllocScratch** out)
+{
+    std::lock_guard<std::mutex> lock(g_phx_noalloc_mu);
+    if (device < 0 || device >= 128) return phx_fail(-1, "phx_simulate_device_noalloc: device %d out of range", device);
+    if (!g_phx_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress(&p, g_phx_noalloc_scratch);
+        if (rc != cudaSuccess || !p)
+            return phx_fail(-2, "phx_simulate_device_noalloc: cudaGetSymbolAddress of the scratch array failed on device %d: %s",
+                            device, cudaGetErrorString(rc));
+        g_phx_noalloc_ptr[device] = static_cast<PhxNoAllocScratch*>(p);
+    }
+    *out = g_phx_noalloc_ptr[device];
+    return 0;
+}
+
+extern "C" int phx_simulate_device_noalloc(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
+                                           int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream)
+{
+    if (!e || !d_out) return phx_fail(-1, "phx_simulate_device_noalloc: null argument");
+    if (num_genstep < 0 || num_photon < 0 || photon_offset < 0)
+        return phx_fail(-1, "phx_simulate_device_noalloc: negative size or offset");
+    if (num_genstep > PHX_NOALLOC_MAX_GENSTEP)
+        return phx_fail(-4, "phx_simulate_device_noalloc: %d gensteps exceed the fixed scratch limit of %d per call",
+                        num_genstep, PHX_NOALLOC_MAX_GENSTEP);
+    if (num_photon > PHX_NOALLOC_MAX_PHOTON)
+        return phx_fail(-4, "phx_simulate_device_noalloc: %lld photons exceed the fixed scratch limit of %lld per call",
+                        (long long)num_photon, (long long)PHX_NOALLOC_MAX_PHOTON);
+    if (photon_offset + num_photon > e->rng_slots)
+        return phx_fail(-4, "phx_simulate_device_noalloc: photons %lld..%lld need RNG slots the engine did not prepare (%lld); "
+                        "create the engine with a larger max_photon", (long long)photon_offset,
+                        (long long)(photon_offset + num_photon), e->rng_slots);
+    const bool want_hits = d_out->hit != nullptr || d_out->sensor_hits != nullptr;
+    if (want_hits && num_photon > 0 && !d_out->photon)
+        return phx_fail(-1, "phx_simulate_device_noalloc: hit selection reads the photon output, pass d_out->photon");
+    PHX_CU(cudaSetDevice(e->device));
+    PhxNoAllocScratch* scr = nullptr;
+    int rc = noalloc_scratch(e->device, &scr);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    const long long N = num_photon;
+    const int G = num_genstep;
+    PHX_CU(cudaMemsetAsync(scr->status, 0, sizeof(unsigned), st));
+    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gensteps), G, scr->gs_off);
+    PHX_CU(cudaGetLastError());
+    SimArgs a;
+    a.S = scene_of(e, e->cfg.root_polish);
+    a.P = props_of(e);
+    a.C = loop_of(e);
+    a.gs = reinterpret_cast<const float4*>(d_gensteps);
+    a.gs_off = scr->gs_off;
+    a.G = G;
+    a.N = N;
+    a.photon_offset = photon_offset;
+    a.event_index = (unsigned long long)event_index;
+    a.skip = e->cfg.skipahead_event_offset;
+    a.rng = e->rng.p;
+    a.rng_slots = e->rng_slots;
+    a.photon = reinterpret_cast<phx_photon*>(d_out->photon);
+    a.seq = reinterpret_cast<phx_seq*>(d_out->seq);
+    a.hitword = want_hits ? scr->hitword : nullptr;
+    a.hit_mask = e->cfg.hit_mask;
+    a.status = scr->status;
+    if (N > 0) {
+        const int B = 128;
+        if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        PHX_CU(cudaGetLastError());
+    }
+    if (d_out->sensor_hits) PHX_CU(cudaMemsetAsync(d_out->sensor_hits, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
+    if (want_hits && N > 0) {
+        const long long nword = (N + 31) / 32;
+        const long long nblock = (nword + 255) / 256;
+        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(scr->hitword, nword, scr->wordoff, scr->blocksum);
+        k_block_scan<<<1, 1024, 0, st>>>(scr->blocksum, (int)nblock, scr->counters);
+        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(a.photon, N, scr->hitword, scr->wordoff, scr->blocksum,
+                                                              reinterpret_cast<phx_photon*>(d_out->hit), d_out->hit_capacity,
+                                                              d_out->sensor_hits, e->cfg.num_sensor, scr->status);
+        PHX_CU(cudaGetLastError());
+        PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, scr->counters, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    }
+    PHX_CU(cudaMemcpyAsync(e->h_pinned, scr->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaStreamSynchronize(st));
+    long long nh = 0;
+    if (want_hits && N > 0) memcpy(&nh, e->h_pinned + 2, sizeof(long long));
+    d_out->num_photon = N;
+    d_out->num_hit = nh;
+    d_out->status = e->h_pinned[0];
+    return 0;
+}
