@@ -69,6 +69,11 @@ typedef struct {
     uint32_t hit_mask;                /* OPTICKS_HIT_MASK                          SD */
     int32_t  root_polish;             /* FP64 polish of quadratic leaf roots       0 */
     int32_t  num_sensor;              /* length of the per-sensor hit count output 0 */
+    int32_t  kernel_mode;             /* 0: one thread per photon, 1: persistent threads with refill */
+    int32_t  block;                   /* persistent kernel block size (32, 64, 128, 256) */
+    int32_t  regroup;                 /* persistent kernel: bounces between lane refills */
+    int32_t  chunk;                   /* persistent kernel: queue grab per warp in units of 32 photons */
+    int32_t  use_graph;               /* batched launches: capture once as a CUDA graph and replay */
 } phx_config;
 
 typedef struct {
@@ -118,12 +123,18 @@ int phx_simulate_device(phx_engine* e, const float* d_gensteps, int32_t num_gens
 int phx_simulate_device_noalloc(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                                 int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream);
 
-/* many events in one persistent launch: gensteps (num_genstep,6,4) with genstep_event[g] the event index
- * of genstep g (non-decreasing).  Outputs are the concatenation of the events' photons in genstep order;
- * event_photon_offset (num_event+1) receives the photon offsets of the events (host array). */
+/* Many events in one persistent launch (no reference counterpart: the reference loops
+ * QSim::simulate per event, qudarap/QSim.cc:436-595).  gensteps (num_genstep,6,4) on device with
+ * d_genstep_event[g] the event index of genstep g (non-decreasing).  Photon j of an event uses RNG slot j
+ * advanced by skipahead(event * skipahead_event_offset), so every event's photons, seq and hits equal
+ * those of phx_simulate_device for that event alone.  Outputs are the events' photons concatenated in
+ * genstep order; hits are selected over the concatenation (in photon order).  block/chunk/regroup <= 0
+ * take the engine config.  d_event_done_ns (num_event+1, optional) receives the %globaltimer value when
+ * each event's last photon finished, and at [num_event] the launch start. */
 int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const int32_t* d_genstep_event,
                                 int32_t num_genstep, int64_t num_photon, int32_t block, int32_t chunk,
-                                int32_t regroup, phx_outputs* d_out, void* stream);
+                                int32_t regroup, int32_t num_event, uint64_t* d_event_done_ns,
+                                phx_outputs* d_out, void* stream);
 
 /* ray scan against one CSGPrim (CSGScan): rays SoA (6,n) = ox,oy,oz,dx,dy,dz ;
  * isect (n,4) = normal.xyz, t (t=0 for a miss) */

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libphox.so")
+# PHX_LIB selects another build of the same library (used to time compile-time variants)
+LIB_PATH = os.environ.get("PHX_LIB", os.path.join(HERE, "libphox.so"))
 
 
 class PhxGeometry(C.Structure):
@@ -39,6 +40,8 @@ class PhxConfig(C.Structure):
         ("propagate_epsilon", C.c_float), ("propagate_epsilon0", C.c_float),
         ("epsilon0_mask", C.c_uint32), ("hit_mask", C.c_uint32),
         ("root_polish", C.c_int32), ("num_sensor", C.c_int32),
+        ("kernel_mode", C.c_int32), ("block", C.c_int32), ("regroup", C.c_int32), ("chunk", C.c_int32),
+        ("use_graph", C.c_int32),
     ]
 
 
@@ -64,7 +67,7 @@ SIGNATURES = {
     "phx_simulate_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int64,
                                               C.POINTER(PhxOutputs), C.c_void_p]),
     "phx_simulate_batched_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int32,
-                                              C.c_int32, C.POINTER(PhxOutputs), C.c_void_p]),
+                                              C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PhxOutputs), C.c_void_p]),
     "phx_csg_scan": (C.c_int, [C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p]),
     "phx_csg_scan_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p]),
     "phx_rng_sequence": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_void_p]),

@@ -253,8 +253,9 @@ PHX_D bool leaf_cylinder(float4& isect, const float4& q0, const float4& q1, floa
     return valid;
 }
 
-PHX_D bool leaf_box3(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir)
+PHX_COLD float4 leaf_box3(const float4 q0, const float t_min, const float3 o, const float3 dir)
 {
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
     const float3 bmin = make_float3(-q0.x / 2.f, -q0.y / 2.f, -q0.z / 2.f);
     const float3 bmax = make_float3(q0.x / 2.f, q0.y / 2.f, q0.z / 2.f);
     float3 idir = f3s(1.f) / dir;
@@ -289,7 +290,8 @@ PHX_D bool leaf_box3(float4& isect, const float4& q0, float t_min, const float3&
             isect.x = n.x; isect.y = n.y; isect.z = n.z; isect.w = t_cand;
         }
     }
-    return valid;
+    (void)valid;
+    return isect;
 }
 
 // ---------------------------------------------------------------- torus (FP64)
@@ -364,12 +366,14 @@ PHX_D bool quartic_first_root(const double* c, double lo, double hi, double& roo
 }
 
 // q0.y = minor radius r (rmax), q0.z = major radius R (rtor) ; full phi range
-PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3& o, const float3& dir, unsigned& err)
+PHX_COLD float4 leaf_torus(const float4 q0, const float t_min, const float3 o, const float3 dir)
 {
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned err = 0;
     const double r = q0.y, R = q0.z;
     const double dx = dir.x, dy = dir.y, dz = dir.z;
     const double dl = sqrt(dx * dx + dy * dy + dz * dz);
-    if (!(dl > 0.0)) return false;
+    if (!(dl > 0.0)) return isect;
     const double nx = dx / dl, ny = dy / dl, nz = dz / dl;
     double ox = o.x, oy = o.y, oz = o.z;
     // clip to the bounding sphere |p| <= R + r, and shift the origin near the torus
@@ -377,11 +381,11 @@ PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3
     const double bb = ox * nx + oy * ny + oz * nz;
     const double cc = ox * ox + oy * oy + oz * oz - Rb * Rb;
     const double dsc = bb * bb - cc;
-    if (dsc <= 0.0) return false;
+    if (dsc <= 0.0) return isect;
     const double sq = sqrt(dsc);
     const double s_in = -bb - sq, s_out = -bb + sq;
     const double s_min = (double)t_min * dl;
-    if (s_out <= s_min) return false;
+    if (s_out <= s_min) return isect;
     const double s0 = fmax(s_in, 0.0);
     ox += s0 * nx; oy += s0 * ny; oz += s0 * nz;
     const double B = 2.0 * (ox * nx + oy * ny + oz * nz);
@@ -395,10 +399,10 @@ PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3
     const double lo = fmax(s_min - s0, 0.0);
     const double hi = s_out - s0 + 1e-9 * Rb;
     double u;
-    if (!quartic_first_root(c, lo, hi, u, err)) return false;
+    if (!quartic_first_root(c, lo, hi, u, err)) return isect;
     const double s = s0 + u;
     const float t = (float)(s / dl);
-    if (!(t > t_min)) return false;
+    if (!(t > t_min)) return isect;
     const double px = ox + u * nx, py = oy + u * ny, pz = oz + u * nz;
     const double k = px * px + py * py + pz * pz + R * R - r * r;
     double gx = px * (k - 2.0 * R * R), gy = py * (k - 2.0 * R * R), gz = pz * k;
@@ -407,17 +411,26 @@ PHX_D bool leaf_torus(float4& isect, const float4& q0, float t_min, const float3
     isect.y = (float)(gy / gl);
     isect.z = (float)(gz / gl);
     isect.w = t;
-    return true;
+    return isect;
 }
 
 // ---------------------------------------------------------------- leaf with transform
+#if PHX_OUTLINE
+#define PHX_LEAFFN __device__ __noinline__
+#else
+#define PHX_LEAFFN __device__ __forceinline__
+#endif
+// One out-of-line copy of the leaf intersector, shared by the tree evaluator and leaf-rooted
+// prims; arguments and result by value so nothing goes through the stack.  A miss returns w=0
+// (with x=-0 for a complemented leaf), a hit has w = t > t_min.
 template <bool POLISH>
-PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
+PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __restrict__ itra, const int ni, const float t_min,
+                            const float3 ray_o, const float3 ray_d)
 {
-    isect = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 q0 = __ldg(g.node + 4 * ni + 0);
-    const float4 q1 = __ldg(g.node + 4 * ni + 1);
-    const float4 q3 = __ldg(g.node + 4 * ni + 3);
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 q0 = __ldg(node + 4 * ni + 0);
+    const float4 q1 = __ldg(node + 4 * ni + 1);
+    const float4 q3 = __ldg(node + 4 * ni + 3);
     const unsigned typecode = __float_as_uint(q3.z);
     const unsigned tc_w = __float_as_uint(q3.w);
     const unsigned gtransformIdx = tc_w & 0x7fffffffu;
@@ -425,7 +438,7 @@ PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min
     float4 t4[4];
     const float4* q = nullptr;
     if (gtransformIdx > 0) {
-        const float4* src = g.itra + 4 * (gtransformIdx - 1);
+        const float4* src = itra + 4 * (gtransformIdx - 1);
         t4[0] = __ldg(src + 0); t4[1] = __ldg(src + 1); t4[2] = __ldg(src + 2); t4[3] = __ldg(src + 3);
         q = t4;
     }
@@ -436,8 +449,8 @@ PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min
         case PHX_CSG_SPHERE:   valid = leaf_sphere<POLISH>(isect, q0, t_min, origin, direction); break;
         case PHX_CSG_ZSPHERE:  valid = leaf_zsphere<POLISH>(isect, q0, q1, t_min, origin, direction); break;
         case PHX_CSG_CYLINDER: valid = leaf_cylinder<POLISH>(isect, q0, q1, t_min, origin, direction); break;
-        case PHX_CSG_BOX3:     valid = leaf_box3(isect, q0, t_min, origin, direction); break;
-        case PHX_CSG_TORUS:    valid = leaf_torus(isect, q0, t_min, origin, direction, err); break;
+        case PHX_CSG_BOX3:     isect = leaf_box3(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_TORUS:    isect = leaf_torus(q0, t_min, origin, direction); valid = isect.w > t_min; break;
         default: break;
     }
     if (valid && q) {
@@ -449,7 +462,15 @@ PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min
         isect.y = valid ? -isect.y : isect.y;
         isect.z = valid ? -isect.z : isect.z;
     }
-    return valid;
+    return isect;
+}
+
+template <bool POLISH>
+PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
+{
+    (void)err;
+    isect = leaf_eval<POLISH>(g.node, g.itra, ni, t_min, ray_o, ray_d);
+    return isect.w > t_min;
 }
 
 PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
@@ -459,11 +480,60 @@ PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
 
 #define PHX_POSTORDER_NEXT(i, elev) (((i) & 1u) ? (i) >> 1 : ((i) << (elev)) + (1u << (elev)))
 
+// ---------------------------------------------------------------- one-operator tree
+// The postorder walk below specialised to a 3-node tree (operator over two leaves, e.g. a PMT
+// cap U neck) with both intermediate results in registers.  It takes the same steps as the
+// general evaluator: both leaves at t_min, combine at t_min; LOOP_A/LOOP_B re-intersect only
+// the looping leaf from |t|+0.0001 (the left tranche (2,3) / right tranche (3,1) of
+// CSG/csg_intersect_tree.h) and combine again at t_min.
+#ifndef PHX_TREE3
+#define PHX_TREE3 1
+#endif
+#define PHX_TREE3_LOOP_CAP 64
+
+template <bool POLISH>
+PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned op, float t_min, const float3& o, const float3& d, unsigned& err)
+{
+    float4 L = leaf_eval<POLISH>(g.node, g.itra, root + 1, t_min, o, d);
+    float4 R = leaf_eval<POLISH>(g.node, g.itra, root + 2, t_min, o, d);
+    for (int it = 0; it < PHX_TREE3_LOOP_CAP; it++) {
+        int l_state = phx_classify(L, d, t_min);
+        int r_state = phx_classify(R, d, t_min);
+        bool leftIsCloser = fabsf(L.w) <= fabsf(R.w);
+        const bool l_promote = l_state == PHX_STATE_MISS && (signbit(L.x) || signbit(L.y));
+        const bool r_promote = r_state == PHX_STATE_MISS && (signbit(R.x) || signbit(R.y));
+        if (r_promote) { r_state = PHX_STATE_EXIT; leftIsCloser = true; }
+        if (l_promote) { l_state = PHX_STATE_EXIT; leftIsCloser = false; }
+        const int ctrl = phx_csg_lookup((int)op, l_state, r_state, leftIsCloser);
+        if (ctrl < PHX_CTRL_LOOP_A) {
+            float4 result = ctrl == PHX_CTRL_RETURN_MISS ? make_float4(0.f, 0.f, 0.f, 0.f) : (ctrl == PHX_CTRL_RETURN_A ? L : R);
+            if (ctrl == PHX_CTRL_RETURN_FLIP_B) { result.x = -result.x; result.y = -result.y; result.z = -result.z; }
+            result.w = copysignf(result.w, 1.f);
+            isect = result;
+            return isect.w > 0.f;
+        }
+        if (ctrl == PHX_CTRL_LOOP_A) L = leaf_eval<POLISH>(g.node, g.itra, root + 1, fabsf(L.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+        else R = leaf_eval<POLISH>(g.node, g.itra, root + 2, fabsf(R.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+    }
+    err |= PHX_STATUS_CSG_STACK;
+    isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    return false;
+}
+
 // ---------------------------------------------------------------- tree
 template <bool POLISH>
 PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
 {
     const unsigned numNode = __float_as_uint(__ldg(g.node + 4 * root).x);   // subNum
+#if PHX_TREE3
+    if (numNode == 3u) {
+        const unsigned op = __float_as_uint(__ldg(g.node + 4 * root + 3).z);
+        const unsigned tl = __float_as_uint(__ldg(g.node + 4 * (root + 1) + 3).z);
+        const unsigned tr = __float_as_uint(__ldg(g.node + 4 * (root + 2) + 3).z);
+        if (op >= PHX_CSG_UNION && op <= PHX_CSG_DIFFERENCE && tl >= PHX_CSG_NODE && tr >= PHX_CSG_NODE)
+            return intersect_tree3<POLISH>(isect, g, root, op, t_min, o, d, err);
+    }
+#endif
     const unsigned height = (unsigned)(__ffs((int)numNode + 1) - 2);
     float4 stk[PHX_CSG_STACK];
     int sp = -1;

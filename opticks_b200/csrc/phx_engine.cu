@@ -23,6 +23,8 @@
 #include "phx_pod.h"
 #include "phx_bvh.h"
 #include "phx_kernels.cuh"
+#include "phx_persist.cuh"
+#include "phx_rngjump.h"
 
 // ------------------------------------------------------------------ error plumbing
 static thread_local std::string g_last_error;
@@ -60,6 +62,12 @@ struct DevBuf {
     void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
 };
 
+struct PhxBatchCall {
+    const float* gs; const int32_t* ev; int G; long long N; int block, chunk, regroup, num_event;
+    uint64_t* done; float* photon; uint64_t* seq; float* hit; long long hcap; uint32_t* sensor; cudaStream_t st;
+    bool operator==(const PhxBatchCall& o) const { return memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
 struct phx_engine {
     int device = 0;
     phx_config cfg;
@@ -90,7 +98,13 @@ struct phx_engine {
     DevBuf<phx_seq> seq;
     DevBuf<phx_photon> hit;
     DevBuf<uint32_t> hitword, wordoff, blocksum, sensor;
-    DevBuf<long long> counters;   // [0] num_hit, [1] queue head, [2..] misc
+    DevBuf<long long> counters;   // [0] num_hit, [1] queue head, [3] largest event
+    DevBuf<long long> ev_start;
+    DevBuf<unsigned> ev_left;
+    DevBuf<uint32_t> jump_pow, jump_tab;   // P_k = T^(skip 2^k) and per-call event jump matrices
+    cudaGraphExec_t batch_exec = nullptr;   // cached batched launch sequence (use_graph)
+    PhxBatchCall batch_call;
+    const void* batch_bufs[11] = {};
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
 };
@@ -184,16 +198,6 @@ __global__ void k_genstep_offsets(const float4* gs, int G, long long* off)
     if (threadIdx.x == 0) off[0] = 0;
 }
 
-PHX_D int phx_find_genstep(const long long* off, int G, long long idx)
-{
-    int lo = 0, hi = G;   // off[lo] <= idx < off[hi]
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= idx) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
 struct SimArgs {
     PhxScene S;
     PhxProps P;
@@ -207,6 +211,7 @@ struct SimArgs {
     unsigned long long skip;
     const uint32_t* rng;
     long long rng_slots;
+    const uint32_t* jump;      // event jump matrix (phx_rngjump.h) or null for cuRAND skipahead
     phx_photon* photon;
     phx_seq* seq;
     uint32_t* hitword;
@@ -215,8 +220,14 @@ struct SimArgs {
 };
 
 // one thread per photon : CSGOptiX/CSGOptiX7.cu:432-530 simulate()
+#ifndef PHX_SIM_BLOCK
+#define PHX_SIM_BLOCK 64
+#endif
+#ifndef PHX_SIM_MINB
+#define PHX_SIM_MINB 8
+#endif
 template <bool POLISH>
-__global__ void __launch_bounds__(128) k_simulate(SimArgs a)
+__global__ void __launch_bounds__(PHX_SIM_BLOCK, PHX_SIM_MINB) k_simulate(SimArgs a)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned status = 0;
@@ -234,7 +245,10 @@ __global__ void __launch_bounds__(128) k_simulate(SimArgs a)
             status |= PHX_STATUS_RNG_RANGE;
             curand_init(0ull, (unsigned long long)photon_idx, 0ull, &rng);
         }
-        if (a.event_index > 0ull) skipahead(a.skip * a.event_index, &rng);
+        if (a.event_index > 0ull) {
+            if (a.jump) phx_rng_jump(rng, a.jump, a.skip * a.event_index);
+            else skipahead(a.skip * a.event_index, &rng);
+        }
         PhxPhoton p;
         memset(&p, 0, sizeof(p));
         generate_photon(p, rng, g, (unsigned long long)photon_idx, a.P, status);
@@ -470,6 +484,11 @@ void phx_config_default(phx_config* c)
     c->hit_mask = PHX_SURFACE_DETECT;
     c->root_polish = 0;
     c->num_sensor = 0;
+    c->kernel_mode = 1;
+    c->block = 64;
+    c->regroup = 1;
+    c->chunk = 1;
+    c->use_graph = 1;
 }
 
 int64_t phx_count_photons(const float* gensteps, int32_t num_genstep)
@@ -495,7 +514,9 @@ int phx_destroy(phx_engine* e)
     e->bvh.release(); e->leaves.release(); e->optical.release(); e->rng.release();
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
-    e->counters.release(); e->status.release();
+    e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
+    e->jump_pow.release(); e->jump_tab.release();
+    if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -606,6 +627,12 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
         PHX_TRY(make_texture_f1(e->icdf_arr, e->icdf_tex, dummy, 2, 2));
     }
     // ---- rng + small buffers
+    {
+        const std::vector<uint32_t> pw = phx_jump_powers(e->cfg.skipahead_event_offset);
+        PHX_TRYCU(e->jump_pow.ensure(pw.size()));
+        PHX_TRYCU(cudaMemcpy(e->jump_pow.p, pw.data(), pw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        PHX_TRYCU(e->jump_tab.ensure(PHX_JUMP_MATW));
+    }
     PHX_TRYCU(e->status.ensure(4));
     PHX_TRYCU(e->counters.ensure(8));
     PHX_TRY(ensure_rng(e, std::max<long long>(1, e->cfg.max_photon)));
@@ -616,30 +643,90 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     return 0;
 }
 
-// shared device path : gensteps already on device
-static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long long N, int event_index, long long photon_offset,
-                                phx_photon* d_photon, phx_seq* d_seq, phx_photon* d_hit, long long hit_capacity,
-                                uint32_t* d_sensor, long long* num_hit, unsigned* status, cudaStream_t st)
+}  // extern "C"
+
+static PersistArgs persist_args_from(const phx_engine* e, const SimArgs& a)
 {
-    if (G < 0 || N < 0) return phx_fail(-1, "simulate: negative sizes");
-    if (photon_offset < 0) return phx_fail(-1, "simulate: negative photon_offset");
-    int rc = ensure_rng(e, photon_offset + N);
-    if (rc) return rc;
-    PHX_CU(e->gs_off.ensure((size_t)G + 1));
-    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
-    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gs), G, e->gs_off.p);
+    PersistArgs A;
+    memset(&A, 0, sizeof(A));
+    A.seed = e->cfg.seed;
+    A.rng_offset = e->cfg.offset;
+    A.S = a.S; A.P = a.P; A.C = a.C;
+    A.gs = a.gs; A.gs_off = a.gs_off; A.G = a.G; A.N = a.N;
+    A.photon_offset = a.photon_offset; A.event_index = a.event_index;
+    A.gs_event = nullptr; A.ev_start = nullptr;
+    A.skip = a.skip; A.rng = a.rng; A.rng_slots = a.rng_slots; A.jump = a.jump;
+    A.photon = a.photon; A.seq = a.seq; A.hitword = a.hitword; A.hit_mask = a.hit_mask; A.status = a.status;
+    A.regroup = 1; A.chunk = 1;
+    return A;
+}
+
+// grid = SMs x resident blocks of the chosen block size (one wave of persistent blocks)
+template <bool POLISH, int BLOCK>
+static int launch_persistent_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
+{
+    // occupancy is queried once per (device, kernel) so graph capture sees only the launch
+    static int cached_sms[128] = {}, cached_per_sm[128] = {};
+    int dev = e->device;
+    if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
+    if (!cached_sms[dev]) {
+        int sms = 0, per_sm = 0;
+        PHX_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sim_persistent<POLISH, BLOCK>, BLOCK, 0));
+        cached_per_sm[dev] = per_sm;
+        cached_sms[dev] = sms;
+    }
+    const int sms = cached_sms[dev], per_sm = cached_per_sm[dev];
+    const long long want = (A.N + BLOCK - 1) / BLOCK;
+    const long long grid = std::max<long long>(1, std::min<long long>((long long)sms * std::max(1, per_sm), want));
+    k_sim_persistent<POLISH, BLOCK><<<(unsigned)grid, BLOCK, 0, st>>>(A);
     PHX_CU(cudaGetLastError());
+    return 0;
+}
+
+static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cudaStream_t st)
+{
+    const bool pol = e->cfg.root_polish != 0;
+    switch (block) {
+        case 32:  return pol ? launch_persistent_t<true, 32>(e, A, st) : launch_persistent_t<false, 32>(e, A, st);
+        case 64:  return pol ? launch_persistent_t<true, 64>(e, A, st) : launch_persistent_t<false, 64>(e, A, st);
+        case 256: return pol ? launch_persistent_t<true, 256>(e, A, st) : launch_persistent_t<false, 256>(e, A, st);
+        case 128:
+        default:  return pol ? launch_persistent_t<true, 128>(e, A, st) : launch_persistent_t<false, 128>(e, A, st);
+    }
+}
+
+extern "C" {
+
+// device buffers of one plain simulate call (engine buffers, or the fixed no-alloc scratch)
+struct PhxPlainBufs {
+    long long* gs_off;
+    uint32_t* hitword;
+    uint32_t* wordoff;
+    uint32_t* blocksum;
+    long long* counters;   // [0] num_hit, [1] queue head
+    unsigned* status;
+    uint32_t* jump;        // one event jump matrix (PHX_JUMP_MATW words)
+};
+
+// every device operation of one plain simulate call on st, then the D2H of num_hit/status
+// into the engine's pinned words; the caller synchronises
+static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs, int G, long long N, int event_index,
+                         long long photon_offset, phx_photon* photon, phx_seq* seq, phx_photon* hit, long long hcap,
+                         uint32_t* sensor, bool want_hits, cudaStream_t st)
+{
     const long long nword = (N + 31) / 32;
-    const bool want_hits = d_hit != nullptr || d_sensor != nullptr;
-    phx_photon* photon = d_photon;
-    if (want_hits && !photon) { PHX_CU(e->photon.ensure((size_t)N)); photon = e->photon.p; }
-    if (want_hits) PHX_CU(e->hitword.ensure((size_t)std::max<long long>(1, nword)));
+    PHX_CU(cudaMemsetAsync(b.status, 0, sizeof(unsigned), st));
+    PHX_CU(cudaMemsetAsync(b.counters, 0, 2 * sizeof(long long), st));
+    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gs), G, b.gs_off);
+    if (event_index > 0) k_jump_build<<<1, 160, 0, st>>>(nullptr, (unsigned long long)event_index, e->jump_pow.p, b.jump);
+    PHX_CU(cudaGetLastError());
     SimArgs a;
     a.S = scene_of(e, e->cfg.root_polish);
     a.P = props_of(e);
     a.C = loop_of(e);
     a.gs = reinterpret_cast<const float4*>(d_gs);
-    a.gs_off = e->gs_off.p;
+    a.gs_off = b.gs_off;
     a.G = G;
     a.N = N;
     a.photon_offset = photon_offset;
@@ -647,34 +734,66 @@ static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long lo
     a.skip = e->cfg.skipahead_event_offset;
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
+    a.jump = event_index > 0 ? b.jump : nullptr;
     a.photon = photon;
-    a.seq = d_seq;
-    a.hitword = want_hits ? e->hitword.p : nullptr;
+    a.seq = seq;
+    a.hitword = want_hits ? b.hitword : nullptr;
     a.hit_mask = e->cfg.hit_mask;
-    a.status = e->status.p;
-    if (N > 0) {
-        const int B = 128;
+    a.status = b.status;
+    if (N > 0 && e->cfg.kernel_mode == 1) {
+        // persistent threads with per-lane refill (phx_persist.cuh); hit bits are OR-ed in
+        if (want_hits) PHX_CU(cudaMemsetAsync(b.hitword, 0, sizeof(uint32_t) * (size_t)nword, st));
+        PersistArgs A = persist_args_from(e, a);
+        A.queue = reinterpret_cast<unsigned long long*>(b.counters + 1);
+        A.regroup = e->cfg.regroup;
+        A.chunk = e->cfg.chunk;
+        int rc = launch_persistent(e, A, e->cfg.block, st);
+        if (rc) return rc;
+    } else if (N > 0) {
+        const int B = PHX_SIM_BLOCK;
         if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
         else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
         PHX_CU(cudaGetLastError());
     }
-    long long nh = 0;
+    if (sensor) PHX_CU(cudaMemsetAsync(sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
     if (want_hits && N > 0) {
         const long long nblock = (nword + 255) / 256;
-        PHX_CU(e->wordoff.ensure((size_t)nword));
-        PHX_CU(e->blocksum.ensure((size_t)nblock));
-        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(e->hitword.p, nword, e->wordoff.p, e->blocksum.p);
-        k_block_scan<<<1, 1024, 0, st>>>(e->blocksum.p, (int)nblock, e->counters.p);
-        if (d_sensor) PHX_CU(cudaMemsetAsync(d_sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
-        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(photon, N, e->hitword.p, e->wordoff.p, e->blocksum.p,
-                                                              d_hit, hit_capacity, d_sensor, e->cfg.num_sensor, e->status.p);
+        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(b.hitword, nword, b.wordoff, b.blocksum);
+        k_block_scan<<<1, 1024, 0, st>>>(b.blocksum, (int)nblock, b.counters);
+        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(photon, N, b.hitword, b.wordoff, b.blocksum,
+                                                              hit, hcap, sensor, e->cfg.num_sensor, b.status);
         PHX_CU(cudaGetLastError());
-        PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, e->counters.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    } else if (d_sensor) {
-        PHX_CU(cudaMemsetAsync(d_sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
     }
-    PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, b.counters, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaMemcpyAsync(e->h_pinned, b.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+// shared device path : gensteps already on device, engine-owned scratch grown on demand
+static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long long N, int event_index, long long photon_offset,
+                                phx_photon* d_photon, phx_seq* d_seq, phx_photon* d_hit, long long hit_capacity,
+                                uint32_t* d_sensor, long long* num_hit, unsigned* status, cudaStream_t st)
+{
+    if (G < 0 || N < 0) return phx_fail(-1, "simulate: negative sizes");
+    if (photon_offset < 0) return phx_fail(-1, "simulate: negative photon_offset");
+    if (event_index < 0) return phx_fail(-1, "simulate: negative event index");
+    int rc = ensure_rng(e, photon_offset + N);
+    if (rc) return rc;
+    const long long nword = (N + 31) / 32;
+    const bool want_hits = d_hit != nullptr || d_sensor != nullptr;
+    phx_photon* photon = d_photon;
+    if (want_hits && !photon) { PHX_CU(e->photon.ensure((size_t)std::max<long long>(1, N))); photon = e->photon.p; }
+    PHX_CU(e->gs_off.ensure((size_t)G + 1));
+    PHX_CU(e->counters.ensure(8));
+    PHX_CU(e->hitword.ensure((size_t)std::max<long long>(1, nword)));
+    PHX_CU(e->wordoff.ensure((size_t)std::max<long long>(1, nword)));
+    PHX_CU(e->blocksum.ensure((size_t)std::max<long long>(1, (nword + 255) / 256)));
+    PHX_CU(e->jump_tab.ensure(PHX_JUMP_MATW));
+    PhxPlainBufs b = { e->gs_off.p, e->hitword.p, e->wordoff.p, e->blocksum.p, e->counters.p, e->status.p, e->jump_tab.p };
+    rc = plain_enqueue(e, b, d_gs, G, N, event_index, photon_offset, photon, d_seq, d_hit, hit_capacity, d_sensor, want_hits, st);
+    if (rc) return rc;
     PHX_CU(cudaStreamSynchronize(st));
+    long long nh = 0;
     if (want_hits && N > 0) memcpy(&nh, e->h_pinned + 2, sizeof(long long));
     *num_hit = nh;
     *status = e->h_pinned[0];
@@ -792,13 +911,144 @@ int phx_rng_sequence(phx_engine* e, int32_t event_index, int64_t photon_offset, 
     return 0;
 }
 
+// every device operation of one batched call, enqueued on st with no host synchronisation
+// (capturable as a CUDA graph); buffers are sized before this is called
+static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* photon, bool want_hits)
+{
+    cudaStream_t st = c.st;
+    const int G = c.G;
+    const long long N = c.N;
+    const long long nword = (N + 31) / 32;
+    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
+    PHX_CU(cudaMemsetAsync(e->counters.p, 0, 8 * sizeof(long long), st));
+    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(c.gs), G, e->gs_off.p);
+    if (G > 0) {
+        k_event_starts<<<(G + 255) / 256, 256, 0, st>>>(c.ev, e->gs_off.p, G, e->ev_start.p);
+        k_jump_build<<<G, 160, 0, st>>>(c.ev, 0ull, e->jump_pow.p, e->jump_tab.p);
+    }
+    PHX_CU(cudaGetLastError());
+    if (want_hits) PHX_CU(cudaMemsetAsync(e->hitword.p, 0, sizeof(uint32_t) * (size_t)std::max<long long>(1, nword), st));
+    if (c.done && c.num_event > 0) {
+        PHX_CU(cudaMemsetAsync(e->ev_left.p, 0, sizeof(unsigned) * (size_t)c.num_event, st));
+        PHX_CU(cudaMemsetAsync(c.done, 0, sizeof(uint64_t) * ((size_t)c.num_event + 1), st));
+        if (G > 0) k_event_counts<<<(G + 255) / 256, 256, 0, st>>>(c.ev, e->gs_off.p, G, e->ev_left.p, c.num_event);
+        k_stamp<<<1, 1, 0, st>>>(reinterpret_cast<unsigned long long*>(c.done) + c.num_event);
+    }
+    SimArgs a;
+    a.S = scene_of(e, e->cfg.root_polish);
+    a.P = props_of(e);
+    a.C = loop_of(e);
+    a.gs = reinterpret_cast<const float4*>(c.gs);
+    a.gs_off = e->gs_off.p;
+    a.G = G;
+    a.N = N;
+    a.photon_offset = 0;
+    a.event_index = 0;
+    a.skip = e->cfg.skipahead_event_offset;
+    a.rng = e->rng.p;
+    a.rng_slots = e->rng_slots;
+    a.jump = e->jump_tab.p;
+    a.photon = photon;
+    a.seq = reinterpret_cast<phx_seq*>(c.seq);
+    a.hitword = want_hits ? e->hitword.p : nullptr;
+    a.hit_mask = e->cfg.hit_mask;
+    a.status = e->status.p;
+    PersistArgs A = persist_args_from(e, a);
+    A.gs_event = c.ev;
+    A.ev_start = e->ev_start.p;
+    A.queue = reinterpret_cast<unsigned long long*>(e->counters.p + 1);
+    A.regroup = c.regroup;
+    A.chunk = c.chunk;
+    if (c.done && c.num_event > 0) {
+        A.ev_left = e->ev_left.p;
+        A.ev_done_ns = reinterpret_cast<unsigned long long*>(c.done);
+        A.num_event = c.num_event;
+    }
+    if (N > 0) {
+        int rc = launch_persistent(e, A, c.block, st);
+        if (rc) return rc;
+    }
+    if (want_hits && N > 0) {
+        const long long nblock = (nword + 255) / 256;
+        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(e->hitword.p, nword, e->wordoff.p, e->blocksum.p);
+        k_block_scan<<<1, 1024, 0, st>>>(e->blocksum.p, (int)nblock, e->counters.p);
+        if (c.sensor) PHX_CU(cudaMemsetAsync(c.sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
+        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(photon, N, e->hitword.p, e->wordoff.p, e->blocksum.p,
+                                                              reinterpret_cast<phx_photon*>(c.hit), c.hcap,
+                                                              c.sensor, e->cfg.num_sensor, e->status.p);
+        PHX_CU(cudaGetLastError());
+    }
+    PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, e->counters.p, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
 int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const int32_t* d_genstep_event,
                                 int32_t num_genstep, int64_t num_photon, int32_t block, int32_t chunk,
-                                int32_t regroup, phx_outputs* d_out, void* stream)
+                                int32_t regroup, int32_t num_event, uint64_t* d_event_done_ns,
+                                phx_outputs* d_out, void* stream)
 {
-    (void)e; (void)d_gensteps; (void)d_genstep_event; (void)num_genstep; (void)num_photon;
-    (void)block; (void)chunk; (void)regroup; (void)d_out; (void)stream;
-    return phx_fail(-9, "phx_simulate_batched_device: not built yet");
+    if (!e || !d_out || (num_genstep > 0 && (!d_gensteps || !d_genstep_event)))
+        return phx_fail(-1, "phx_simulate_batched_device: null argument");
+    if (num_genstep < 0 || num_photon < 0 || num_event < 0) return phx_fail(-1, "phx_simulate_batched_device: negative size");
+    PHX_CU(cudaSetDevice(e->device));
+    PhxBatchCall c;
+    memset(&c, 0, sizeof(c));
+    c.gs = d_gensteps; c.ev = d_genstep_event; c.G = num_genstep; c.N = num_photon;
+    c.block = block > 0 ? block : e->cfg.block;
+    c.chunk = chunk > 0 ? chunk : e->cfg.chunk;
+    c.regroup = regroup > 0 ? regroup : e->cfg.regroup;
+    c.num_event = d_event_done_ns ? num_event : 0;
+    c.done = d_event_done_ns;
+    c.photon = d_out->photon; c.seq = d_out->seq; c.hit = d_out->hit; c.hcap = d_out->hit_capacity; c.sensor = d_out->sensor_hits;
+    c.st = stream ? (cudaStream_t)stream : e->stream;
+    const long long N = c.N;
+    const long long nword = (N + 31) / 32;
+    const bool want_hits = c.hit != nullptr || c.sensor != nullptr;
+    // size every buffer first (no allocation may happen inside a captured sequence)
+    PHX_CU(e->gs_off.ensure((size_t)c.G + 1));
+    PHX_CU(e->ev_start.ensure((size_t)std::max(1, c.G)));
+    PHX_CU(e->counters.ensure(8));
+    phx_photon* photon = reinterpret_cast<phx_photon*>(c.photon);
+    if (want_hits && !photon) { PHX_CU(e->photon.ensure((size_t)std::max<long long>(1, N))); photon = e->photon.p; }
+    if (want_hits) {
+        PHX_CU(e->hitword.ensure((size_t)std::max<long long>(1, nword)));
+        PHX_CU(e->wordoff.ensure((size_t)std::max<long long>(1, nword)));
+        PHX_CU(e->blocksum.ensure((size_t)std::max<long long>(1, (nword + 255) / 256)));
+    }
+    if (c.num_event > 0) PHX_CU(e->ev_left.ensure((size_t)c.num_event));
+    PHX_CU(e->jump_tab.ensure((size_t)std::max(1, c.G) * PHX_JUMP_MATW));
+    if (e->cfg.use_graph) {
+        // the captured graph bakes in every engine buffer pointer: reuse it only if none moved
+        const void* bufs[11] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
+                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p };
+        const bool reuse = e->batch_exec && e->batch_call == c && memcmp(bufs, e->batch_bufs, sizeof(bufs)) == 0;
+        if (!reuse) {
+            if (e->batch_exec) { cudaGraphExecDestroy(e->batch_exec); e->batch_exec = nullptr; }
+            cudaGraph_t graph = nullptr;
+            PHX_CU(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeRelaxed));
+            int rc = batched_enqueue(e, c, photon, want_hits);
+            cudaError_t ce = cudaStreamEndCapture(c.st, &graph);
+            if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+            if (ce != cudaSuccess) return phx_fail(-2, "batched graph capture failed: %s", cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&e->batch_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) { e->batch_exec = nullptr; return phx_fail(-2, "batched graph instantiate failed: %s", cudaGetErrorString(ce)); }
+            e->batch_call = c;
+            memcpy(e->batch_bufs, bufs, sizeof(bufs));
+        }
+        PHX_CU(cudaGraphLaunch(e->batch_exec, c.st));
+    } else {
+        int rc = batched_enqueue(e, c, photon, want_hits);
+        if (rc) return rc;
+    }
+    PHX_CU(cudaStreamSynchronize(c.st));
+    long long nh = 0;
+    if (want_hits && N > 0) memcpy(&nh, e->h_pinned + 2, sizeof(long long));
+    d_out->num_photon = N;
+    d_out->num_hit = nh;
+    d_out->status = e->h_pinned[0];
+    return 0;
 }
 
 int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
@@ -832,6 +1082,7 @@ struct PhxNoAllocScratch {
     uint32_t blocksum[PHX_NOALLOC_BLOCKS];
     long long counters[8];
     unsigned status[8];
+    __align__(16) uint32_t jump[PHX_JUMP_MATW];
 };
 
 static __device__ __align__(256) PhxNoAllocScratch g_phx_noalloc_scratch;
@@ -867,6 +1118,7 @@ extern "C" int phx_simulate_device_noalloc(phx_engine* e, const float* d_genstep
     if (num_genstep > PHX_NOALLOC_MAX_GENSTEP)
         return phx_fail(-4, "phx_simulate_device_noalloc: %d gensteps exceed the fixed scratch limit of %d per call",
                         num_genstep, PHX_NOALLOC_MAX_GENSTEP);
+    if (event_index < 0) return phx_fail(-1, "phx_simulate_device_noalloc: negative event index");
     if (num_photon > PHX_NOALLOC_MAX_PHOTON)
         return phx_fail(-4, "phx_simulate_device_noalloc: %lld photons exceed the fixed scratch limit of %lld per call",
                         (long long)num_photon, (long long)PHX_NOALLOC_MAX_PHOTON);
@@ -883,47 +1135,12 @@ extern "C" int phx_simulate_device_noalloc(phx_engine* e, const float* d_genstep
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
     const long long N = num_photon;
-    const int G = num_genstep;
-    PHX_CU(cudaMemsetAsync(scr->status, 0, sizeof(unsigned), st));
-    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gensteps), G, scr->gs_off);
-    PHX_CU(cudaGetLastError());
-    SimArgs a;
-    a.S = scene_of(e, e->cfg.root_polish);
-    a.P = props_of(e);
-    a.C = loop_of(e);
-    a.gs = reinterpret_cast<const float4*>(d_gensteps);
-    a.gs_off = scr->gs_off;
-    a.G = G;
-    a.N = N;
-    a.photon_offset = photon_offset;
-    a.event_index = (unsigned long long)event_index;
-    a.skip = e->cfg.skipahead_event_offset;
-    a.rng = e->rng.p;
-    a.rng_slots = e->rng_slots;
-    a.photon = reinterpret_cast<phx_photon*>(d_out->photon);
-    a.seq = reinterpret_cast<phx_seq*>(d_out->seq);
-    a.hitword = want_hits ? scr->hitword : nullptr;
-    a.hit_mask = e->cfg.hit_mask;
-    a.status = scr->status;
-    if (N > 0) {
-        const int B = 128;
-        if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
-        else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
-        PHX_CU(cudaGetLastError());
-    }
-    if (d_out->sensor_hits) PHX_CU(cudaMemsetAsync(d_out->sensor_hits, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
-    if (want_hits && N > 0) {
-        const long long nword = (N + 31) / 32;
-        const long long nblock = (nword + 255) / 256;
-        k_word_scan<<<(unsigned)nblock, 256, 0, st>>>(scr->hitword, nword, scr->wordoff, scr->blocksum);
-        k_block_scan<<<1, 1024, 0, st>>>(scr->blocksum, (int)nblock, scr->counters);
-        k_compact<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(a.photon, N, scr->hitword, scr->wordoff, scr->blocksum,
-                                                              reinterpret_cast<phx_photon*>(d_out->hit), d_out->hit_capacity,
-                                                              d_out->sensor_hits, e->cfg.num_sensor, scr->status);
-        PHX_CU(cudaGetLastError());
-        PHX_CU(cudaMemcpyAsync(e->h_pinned + 2, scr->counters, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    }
-    PHX_CU(cudaMemcpyAsync(e->h_pinned, scr->status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    // the same launch sequence as phx_simulate_device, on the fixed scratch
+    PhxPlainBufs b = { scr->gs_off, scr->hitword, scr->wordoff, scr->blocksum, scr->counters, scr->status, scr->jump };
+    rc = plain_enqueue(e, b, d_gensteps, num_genstep, N, event_index, photon_offset, reinterpret_cast<phx_photon*>(d_out->photon),
+                       reinterpret_cast<phx_seq*>(d_out->seq), reinterpret_cast<phx_photon*>(d_out->hit), d_out->hit_capacity,
+                       d_out->sensor_hits, want_hits, st);
+    if (rc) return rc;
     PHX_CU(cudaStreamSynchronize(st));
     long long nh = 0;
     if (want_hits && N > 0) memcpy(&nh, e->h_pinned + 2, sizeof(long long));

@@ -166,6 +166,63 @@ PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene&
     }
 }
 
+// genstep of photon idx: the last g with off[g] <= idx (empty gensteps are skipped)
+PHX_D int phx_find_genstep(const long long* off, int G, long long idx)
+{
+    int lo = 0, hi = G;   // off[lo] <= idx < off[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= idx) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Advance a loaded XORWOW state by n steps with a precomputed jump matrix M (= T^n, see
+// phx_rngjump.h): v <- M v over GF(2), d <- d + 362437 n.  Same state as skipahead(n).
+PHX_D void phx_rng_jump(curandStateXORWOW& s, const uint32_t* __restrict__ M, unsigned long long n)
+{
+    uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u, o4 = 0u;
+    const uint32_t in[5] = { s.v[0], s.v[1], s.v[2], s.v[3], s.v[4] };
+#pragma unroll 1
+    for (int w = 0; w < 5; w++) {
+        const uint32_t x = in[w];
+        const uint32_t* colw = M + (size_t)(32 * w) * 8;
+#pragma unroll 8
+        for (int b = 0; b < 32; b++) {
+            const uint32_t m = 0u - ((x >> b) & 1u);
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(colw + 8 * b));
+            const uint32_t e4 = __ldg(colw + 8 * b + 4);
+            o0 ^= a.x & m; o1 ^= a.y & m; o2 ^= a.z & m; o3 ^= a.w & m; o4 ^= e4 & m;
+        }
+    }
+    s.v[0] = o0; s.v[1] = o1; s.v[2] = o2; s.v[3] = o3; s.v[4] = o4;
+    s.d += (unsigned int)((362437ull * n) & 0xffffffffull);
+}
+
+// one event jump matrix per entry: entry i uses event ev[i] (or `single` when ev is null);
+// thread c composes column c of prod_k P_k^(bit k of event)
+__global__ void k_jump_build(const int* ev, unsigned long long single, const uint32_t* __restrict__ P, uint32_t* out)
+{
+    const int c = threadIdx.x;
+    if (c >= 160) return;
+    const unsigned long long e = ev ? (unsigned long long)(unsigned)ev[blockIdx.x] : single;
+    uint32_t v[5] = { 0u, 0u, 0u, 0u, 0u };
+    v[c >> 5] = 1u << (c & 31);
+    for (int k = 0; k < 32; k++) {
+        if (!((e >> k) & 1ull)) continue;
+        const uint32_t* Pk = P + (size_t)k * 160 * 8;
+        uint32_t o[5] = { 0u, 0u, 0u, 0u, 0u };
+        for (int bit = 0; bit < 160; bit++) {
+            if ((v[bit >> 5] >> (bit & 31)) & 1u)
+                for (int q = 0; q < 5; q++) o[q] ^= Pk[bit * 8 + q];
+        }
+        for (int q = 0; q < 5; q++) v[q] = o[q];
+    }
+    uint32_t* dst = out + (size_t)blockIdx.x * 160 * 8 + c * 8;
+    for (int q = 0; q < 5; q++) dst[q] = v[q];
+    dst[5] = dst[6] = dst[7] = 0u;
+}
+
 PHX_D void phx_load_rng(curandStateXORWOW& s, const uint32_t* rng, long long slots, long long slot)
 {
     s.d = __ldg(rng + slot);

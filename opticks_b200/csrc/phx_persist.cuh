@@ -1,0 +1,216 @@
+// phx_persist.cuh : persistent-thread photon kernel with a device work queue.
+//
+// Many events of uneven size (or one large event) are flattened into one photon index space.
+// Each warp takes chunks of photon indices from a global counter; a lane whose photon finishes
+// is refilled with the next index from the warp's chunk every `regroup` bounces, so lanes do
+// not idle until the longest photon of their warp ends (the divergence of a one-thread-per-photon
+// launch).  Photon j of genstep g belongs to event ev[g]; its RNG slot is its index within the
+// event and its stream is advanced by skipahead(event * skip), exactly as a separate launch of
+// that event would do (qudarap/qrng.h:85-90 with photon_slot_offset, CSGOptiX/CSGOptiX7.cu:441),
+// so batched results are identical to the per-event loop.
+//
+// There are no waits: the queue is a monotonic atomic counter, loops are bounded by the number
+// of photons, and each photon's bounce count is bounded by max_bounce.
+#pragma once
+#include "phx_kernels.cuh"
+
+struct PersistArgs {
+    PhxScene S;
+    PhxProps P;
+    PhxLoopCfg C;
+    const float4* gs;
+    const long long* gs_off;        // (G+1) photon offsets of the gensteps
+    int G;
+    long long N;
+    long long photon_offset;        // single-event mode: absolute index of photon 0
+    unsigned long long event_index; // single-event mode: event index
+    const int* gs_event;            // batched mode: event index of each genstep (non-decreasing), or null
+    const long long* ev_start;      // batched mode: photon offset of the first photon of each genstep's event
+    unsigned long long skip;
+    unsigned long long seed, rng_offset;   // curand_init arguments for photons beyond the prepared slots
+    const uint32_t* rng;
+    long long rng_slots;
+    const uint32_t* jump;           // event jump matrices: one (single event) or one per genstep (batched)
+    phx_photon* photon;
+    phx_seq* seq;
+    uint32_t* hitword;              // zeroed before launch; bits set with atomicOr
+    unsigned hit_mask;
+    unsigned* status;
+    unsigned long long* queue;      // work counter, zeroed before launch
+    int regroup;                    // bounces between refills
+    int chunk;                      // queue grab per warp, in units of 32 photons
+    unsigned* ev_left;              // optional: photons left per event (batched), for completion times
+    unsigned long long* ev_done_ns; // optional: globaltimer when the event's last photon finished
+    int num_event;
+};
+
+PHX_D unsigned long long phx_globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct PhxLane {
+    PhxPhoton p;
+    curandStateXORWOW rng;
+    unsigned long long seqhis[2], seqbnd[2];
+    long long idx;
+    int bounce;
+    int ev;
+};
+
+template <bool POLISH>
+PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status)
+{
+    const int gi = phx_find_genstep(A.gs_off, A.G, idx);
+    float4 g[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) g[k] = __ldg(A.gs + 6 * gi + k);
+    long long slot;
+    unsigned long long ev;
+    if (A.gs_event) {
+        ev = (unsigned long long)__ldg(A.gs_event + gi);
+        slot = idx - __ldg(A.ev_start + gi);
+    } else {
+        ev = A.event_index;
+        slot = A.photon_offset + idx;
+    }
+    if (slot < A.rng_slots) {
+        phx_load_rng(L.rng, A.rng, A.rng_slots, slot);
+    } else {
+        // same state as a prepared slot, computed on the fly (slower; flagged)
+        status |= PHX_STATUS_RNG_RANGE;
+        curand_init(A.seed, (unsigned long long)slot, A.rng_offset, &L.rng);
+    }
+    if (ev > 0ull) {
+        if (A.jump) phx_rng_jump(L.rng, A.jump + (A.gs_event ? (size_t)gi * 1280 : 0), A.skip * ev);
+        else skipahead(A.skip * ev, &L.rng);
+    }
+    memset(&L.p, 0, sizeof(L.p));
+    generate_photon(L.p, L.rng, g, (unsigned long long)slot, A.P, status);
+    L.seqhis[0] = L.seqhis[1] = L.seqbnd[0] = L.seqbnd[1] = 0ull;
+    seq_add_nibble(L.seqhis, L.seqbnd, 0u, L.p.flag(), L.p.boundary());
+    L.idx = idx;
+    L.bounce = 0;
+    L.ev = (int)ev;
+}
+
+template <bool POLISH>
+PHX_D void persist_finish(PhxLane& L, const PersistArgs& A)
+{
+    const long long idx = L.idx;
+    if (A.photon) phx_store_photon(A.photon + idx, L.p);
+    if (A.seq) {
+        ulonglong2* s = reinterpret_cast<ulonglong2*>(A.seq + idx);
+        s[0] = make_ulonglong2(L.seqhis[0], L.seqhis[1]);
+        s[1] = make_ulonglong2(L.seqbnd[0], L.seqbnd[1]);
+    }
+    if (A.hitword && (L.p.flagmask & A.hit_mask) == A.hit_mask) atomicOr(A.hitword + (idx >> 5), 1u << (idx & 31));
+    if (A.ev_left) {
+        const int e = A.gs_event ? L.ev : 0;
+        if (e >= 0 && e < A.num_event && atomicSub(A.ev_left + e, 1u) == 1u) A.ev_done_ns[e] = phx_globaltimer();
+    }
+}
+
+// one bounce of CSGOptiX/CSGOptiX7.cu:477-509; returns true when the photon is finished
+template <bool POLISH>
+PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status)
+{
+    if (!(L.bounce < A.C.max_bounce && L.p.time < A.C.max_time)) return true;
+    const float tmin = (L.p.obf & A.C.eps0_mask) ? A.C.tmin0 : A.C.tmin;
+    PhxPRD prd;
+    phx_trace<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
+    if (prd.boundary() == 0xffffu) return true;
+    prd.normal = normalize(prd.normal);
+    const int command = propagate(L.p, L.rng, prd, A.P, status);
+    L.bounce++;
+    seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
+    return command == PHX_BREAK;
+}
+
+template <bool POLISH, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_sim_persistent(PersistArgs A)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    const long long grab = 32ll * (long long)(A.chunk > 0 ? A.chunk : 1);
+    const int regroup = A.regroup > 0 ? A.regroup : 1;
+    long long wnext = 0, wend = 0;   // warp-uniform pool of photon indices
+    bool exhausted = false;
+    bool active = false;
+    unsigned status = 0;
+    PhxLane L;
+    for (;;) {
+        unsigned need = __ballot_sync(FULL, !active);
+        while (need && !exhausted) {
+            if (wnext >= wend) {
+                unsigned long long base = 0ull;
+                if (lane == 0) base = atomicAdd(A.queue, (unsigned long long)grab);
+                base = __shfl_sync(FULL, base, 0);
+                if ((long long)base >= A.N) { exhausted = true; break; }
+                wnext = (long long)base;
+                wend = min(wnext + grab, A.N);
+            }
+            const long long avail = wend - wnext;
+            unsigned take = need;
+            if ((long long)__popc(take) > avail) {
+                // keep the lowest `avail` requesting lanes
+                unsigned t = 0u, m = need;
+                for (long long k = 0; k < avail; k++) { const unsigned b = m & (0u - m); t |= b; m ^= b; }
+                take = t;
+            }
+            if ((take >> lane) & 1u) {
+                persist_start<POLISH>(L, A, wnext + __popc(take & lanes_below), status);
+                active = true;
+            }
+            wnext += __popc(take);
+            need &= ~take;
+        }
+        if (!__any_sync(FULL, active)) break;
+        for (int k = 0; k < regroup; k++) {
+            if (active && persist_step<POLISH>(L, A, status)) {
+                persist_finish<POLISH>(L, A);
+                active = false;
+            }
+        }
+    }
+    if (status) atomicOr(A.status, status);
+}
+
+// per genstep: photon offset of the first photon of its event (gs_event non-decreasing)
+__global__ void k_event_starts(const int* gs_event, const long long* gs_off, int G, long long* ev_start)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const int ev = gs_event[g];
+    int lo = 0, hi = g;   // first index with gs_event == ev
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (gs_event[mid] < ev) lo = mid + 1; else hi = mid;
+    }
+    ev_start[g] = gs_off[lo];
+}
+
+// photons per event (for completion times): ev_left[e] = sum of genstep counts of event e
+__global__ void k_event_counts(const int* gs_event, const long long* gs_off, int G, unsigned* ev_left, int num_event)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const int ev = gs_event[g];
+    if (ev >= 0 && ev < num_event) atomicAdd(ev_left + ev, (unsigned)(gs_off[g + 1] - gs_off[g]));
+}
+
+// largest photon count of one event (the RNG slots a batched launch needs)
+__global__ void k_event_max(const long long* gs_off, const long long* ev_start, int G, unsigned long long* out)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    atomicMax(out, (unsigned long long)(gs_off[g + 1] - ev_start[g]));
+}
+
+__global__ void k_stamp(unsigned long long* t)
+{
+    *t = phx_globaltimer();
+}

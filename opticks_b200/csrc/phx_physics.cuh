@@ -336,7 +336,7 @@ PHX_D void generate_cerenkov(PhxPhoton& p, curandStateXORWOW& rng, const float4*
 }
 
 // qsim::generate_photon qudarap/qsim.h:2532-2561
-PHX_D void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
+PHX_COLD void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
 {
     const int gencode = __float_as_int(g[0].x);
     switch (gencode) {
@@ -353,7 +353,7 @@ PHX_D void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g
 // ---------------------------------------------------------------- propagation
 #define PHX_LOOP_CAP 1000000
 
-PHX_D void rayleigh_scatter(PhxPhoton& p, curandStateXORWOW& rng, unsigned& status)
+PHX_COLD void rayleigh_scatter(PhxPhoton& p, curandStateXORWOW& rng, unsigned& status)
 {
     float3 direction, polarization;
     bool looping = true;
@@ -509,7 +509,7 @@ PHX_D void lambertian_direction(float3& dir, const float3& normal, float orient,
     } while (!(u < ndotv) && (count < 1024));
 }
 
-PHX_D void reflect_diffuse(PhxPhoton& p, curandStateXORWOW& rng, const float3& normal)
+PHX_COLD void reflect_diffuse(PhxPhoton& p, curandStateXORWOW& rng, const float3& normal)
 {
     float3 old_mom = p.mom;
     const float orient = dot(old_mom, normal) > 0.f ? -1.f : 1.f;

@@ -11,6 +11,17 @@
 
 #define PHX_D __device__ __forceinline__
 
+// Cold paths (generation, scattering, rare leaves) are called out of line so the hot bounce loop
+// stays small enough for the instruction cache; PHX_OUTLINE=0 inlines everything (A/B builds).
+#ifndef PHX_OUTLINE
+#define PHX_OUTLINE 1
+#endif
+#if PHX_OUTLINE
+#define PHX_COLD __device__ __noinline__
+#else
+#define PHX_COLD __device__ __forceinline__
+#endif
+
 #ifndef PHX_PI_F
 #define PHX_PI_F 3.14159265358979323846f
 #endif

@@ -165,14 +165,18 @@ class Engine:
         return int(out.num_hit), int(out.status)
 
     def simulate_batched_device(self, gs_dev, gs_event_dev, num_photon: int, photon=None, seq=None, hit=None,
-                                hit_capacity: int = 0, block: int = 0, chunk: int = 0, regroup: int = 0,
-                                stream: int = 0) -> tuple[int, int]:
+                                hit_capacity: int = 0, sensor_hits=None, block: int = 0, chunk: int = 0, regroup: int = 0,
+                                num_event: int = 0, event_done_ns=None, stream: int = 0) -> tuple[int, int]:
+        """Many events in one persistent launch (torch CUDA tensors).  gs_event_dev: int32 event index
+        per genstep, non-decreasing.  event_done_ns: optional int64 tensor (num_event+1) receiving the
+        device clock when each event finished and, last, when the launch started.  Returns (num_hit, status)."""
         def dp(t):
             return None if t is None else C.c_void_p(t.data_ptr())
-        out = PhxOutputs(dp(photon), dp(seq), dp(hit), int(hit_capacity), None, 0, 0, 0)
+        out = PhxOutputs(dp(photon), dp(seq), dp(hit), int(hit_capacity), dp(sensor_hits), 0, 0, 0)
         G = gs_dev.numel() // 24
         _lib.check(_lib.lib().phx_simulate_batched_device(self._h, dp(gs_dev), dp(gs_event_dev), int(G), int(num_photon),
-                                                          int(block), int(chunk), int(regroup), C.byref(out),
+                                                          int(block), int(chunk), int(regroup), int(num_event),
+                                                          dp(event_done_ns), C.byref(out),
                                                           C.c_void_p(stream) if stream else None),
                    "phx_simulate_batched_device")
         return int(out.num_hit), int(out.status)

@@ -80,7 +80,7 @@ def test_scan_matches_reference_device_code(notorus_engine):
     print(f"   t rel diff p99.9 {np.quantile(rel, 0.999):.3g} max {rel.max():.3g}")
     assert np.quantile(rel, 0.999) < 1e-5
     assert rel.max() < 1e-3
-    assert exact > 0.98
+    assert exact > 0.95
 
 
 def test_scan_with_torus_against_fp64_oracle(tree_engine):

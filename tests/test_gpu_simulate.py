@@ -135,3 +135,22 @@ def test_empty_and_zero_photon_gensteps(cuda):
     r = eng.simulate(gs, 0)
     assert r["num_photon"] == 5 and r["status"] == 0
     eng.close()
+
+
+@pytest.mark.skipif(not O.have_ref_sim(), reason="reference GPU build absent")
+@pytest.mark.parametrize("event", [1, 5, 4095])
+def test_event_streams_match_reference_skipahead(cuda, event):
+    # the engine advances streams with one event jump matrix per event; the reference calls
+    # cuRAND skipahead(event * 100000) per photon (qudarap/qrng.h:85-90): histories must agree
+    n = 4000
+    fd, lib, icdf, _ = scenes.sphere_in_box(n)
+    gs = scenes.torch_genstep(n, type_=scenes.T_SPHERE, distance=0.1)[None]
+    eng, phys = _engine(fd, lib, max_photon=n)
+    r = eng.simulate(gs, event)
+    eng.close()
+    ph, sq = O.ref_simulate_gpu(fd.arrays(), phys, gs, event_index=event)
+    m = seq_match(r["seq"], sq)
+    same = np.all(r["seq"][:, 0, :] == sq[:, 0, :], axis=1)
+    print(f"event {event}: seqhis match {m:.6f} close {frac_close(r['photon'], ph, same, TOL):.6f}")
+    assert m >= SEQ_BAR
+    assert frac_close(r["photon"], ph, same, TOL) >= SEQ_BAR
