@@ -1,21 +1,23 @@
-"""Benchmark of the photon engine: photons/s on one B200 for the full synthetic detector.
+"""Benchmark of the photon engine on one B200 (one process per GPU under torchrun).
 
-Workload (one step = one event): 10,000,000 scintillation photons from 1,000 gensteps with
-vertices uniform in r < 17 m, in the 17,612-PMT detector (LS sphere 17.7 m, acrylic shell,
-water sphere 20.5 m), seqhis recorded, hits (SD) compacted in photon order.
+Headline (`value`): photons/s of the plain form on the full synthetic detector — one event of
+10,000,000 scintillation photons from 1,000 gensteps (vertices uniform in r < 17 m, 430/20 nm),
+17,612 PMT instances, seqhis recorded, SD hits compacted in photon order — gensteps resident
+in HBM, device time from CUDA events on the launch stream.
 
-  value : photons/s with gensteps resident in HBM (device path, CUDA events on the launch stream)
-  e2e   : photons/s through the host API phx_simulate (H2D gensteps, D2H photons+seq+hits into
-          pinned buffers) timed per step
-  roofline : k_simulate algorithmic bytes / its duration vs the measured HBM copy bandwidth
-  cpu_baseline : the CPU oracle (port of the reference's path) on a bounded sample, all threads
+Also on the line:
+  e2e          photons/s through the host API phx_simulate (H2D gensteps, D2H photon+seq+hits
+               into pinned buffers), timed per step
+  roofline     k_sim_persistent: 120.1 algorithmic bytes/photon / its duration vs measured HBM
+  cpu_baseline the CPU oracle (port of the reference's path) on a bounded sample, all threads
+  forms        batched (4,096 lognormal events in one persistent launch, CUDA graph, autotuned)
+               vs the per-event launch loop with per-event latency p50/p99; the CSG scan
+               (16,777,216 rays vs the 15-node tree with torus, rays/s, FP64 distance error)
 
---impl reference : the reference's CPU implementation of this path on the host cores.  Its qsim
-headers need glm/plog to compile for the CPU (absent), so the oracle port stands in
-(``kind: port``), run with every host thread on a bounded sample per step.
-
-Multi-GPU (torchrun): each rank simulates its own events (independent photons, no collective on
-the data path); value = photons of all ranks / max over ranks of the device time.
+--impl reference: the reference's CPU implementation of the path on the host cores.  Its qsim
+headers need glm/plog (absent) to build for the CPU, so the oracle port stands in (kind: port).
+Multi-GPU: each rank simulates its own events (no data-path collective); value = photons of all
+ranks / max over ranks of the device time.
 """
 from __future__ import annotations
 
@@ -34,6 +36,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "photons/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+BYTES_PER_PHOTON_FIXED = 24 + 64 + 32 + 4.0 / 32   # RNG state + sphoton + sseq + hit bit
 
 
 def load_peaks():
@@ -45,7 +48,7 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def workload(num_genstep, per_genstep, seed=0):
+def detector_workload(num_genstep, per_genstep, seed=0):
     from opticks_b200 import scenes
     fd, lib, icdf = scenes.detector()
     phys = lib.arrays()
@@ -55,7 +58,7 @@ def workload(num_genstep, per_genstep, seed=0):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region"""
+    """nvidia-smi sampling during a timed region"""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -100,7 +103,7 @@ class Clocks:
 
 
 def cpu_baseline(fd, phys, gs, target_s=12.0):
-    """oracle port on the host cores over a bounded sample of the same event"""
+    """oracle port on all host threads over a bounded sample of the same event"""
     from oracle import oracle as O
     S = O.Scene(fd.arrays(), phys)
     K = 1024
@@ -110,8 +113,7 @@ def cpu_baseline(fd, phys, gs, target_s=12.0):
     u = rng.random((n, K), dtype=np.float32)
     t0 = time.perf_counter()
     S.simulate(gs, u, 0)
-    dt = time.perf_counter() - t0
-    rate = n / dt
+    rate = n / (time.perf_counter() - t0)
     n2 = int(min(2_000_000, max(n, rate * target_s)))
     u = rng.random((n2, K), dtype=np.float32)
     t0 = time.perf_counter()
@@ -122,11 +124,10 @@ def cpu_baseline(fd, phys, gs, target_s=12.0):
 
 
 def run_reference(args):
-    """--impl reference : CPU implementation of the path on the host cores"""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    """--impl reference : CPU implementation of the path on the host cores (rank 0 only)"""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
-    fd, lib, phys, gs = workload(args.gensteps, args.per_genstep)
+    fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
     from oracle import oracle as O
     S = O.Scene(fd.arrays(), phys)
     K = 1024
@@ -148,9 +149,113 @@ def run_reference(args):
             "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": args.gensteps,
                        "photons_per_genstep": args.per_genstep, "sample_photons_per_step": n},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": f"first {n} photons of the event per step (oracle port; the reference's qsim needs glm/plog to build for the CPU)"},
+                             "sample": f"first {n} photons of the event per step (oracle port; the reference's qsim "
+                                       f"needs glm/plog to build for the CPU)"},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=None):
+    """C4: uneven events in one persistent launch (autotuned, CUDA graph) vs the per-event loop"""
+    from opticks_b200 import autotune, scenes
+    gs = scenes.batched_events(num_event, lib=lib)
+    ev = np.arange(len(gs), dtype=np.int32)
+    counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
+    N = int(counts.sum())
+    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=int(counts.max()), num_sensor=scenes.NUM_PMT), device=dev.index)
+    best = autotune.tune_batched(eng, gs, ev, torch, cache=tune_cache)
+    g = torch.from_numpy(gs).to(dev)
+    e = torch.from_numpy(ev).to(dev)
+    photon = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
+    seq = torch.empty((N, 2, 2), dtype=torch.int64, device=dev)
+    hit = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
+    done = torch.zeros((num_event + 1,), dtype=torch.int64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    assert st.cuda_stream != 0, "run on a non-default stream so the library launches where the events are recorded"
+
+    def batch():
+        return eng.simulate_batched_device(g, e, N, photon=photon, seq=seq, hit=hit, hit_capacity=N, block=best["block"],
+                                           regroup=best["regroup"], chunk=best["chunk"], num_event=num_event,
+                                           event_done_ns=done, stream=st.cuda_stream)
+    batch()                      # warm-up + graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    nh_b, st_b = batch()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    d = done.cpu().numpy()
+    lat_b = (d[:num_event] - d[num_event]) / 1e6    # ms from launch start to each event's last photon
+    off = np.concatenate([[0], np.cumsum(counts)])
+
+    def loop(record=None):
+        for k in range(num_event):
+            t0 = time.perf_counter()
+            eng.simulate_device(g[k:k + 1], int(counts[k]), k, photon=photon[off[k]:off[k + 1]], seq=seq[off[k]:off[k + 1]],
+                                hit=hit[off[k]:off[k + 1]], hit_capacity=int(counts[k]), stream=st.cuda_stream)
+            if record is not None:
+                record.append(time.perf_counter() - t0)
+    loop()                       # warm-up
+    torch.cuda.synchronize()
+    per = []
+    t0 = time.perf_counter()
+    e0.record(st)
+    loop(per)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_l = e0.elapsed_time(e1)
+    per = np.array(per) * 1e3
+    lat_l = np.cumsum(per)
+    eng.close()
+    return {"workload": f"{num_event} events, one scintillation genstep each, lognormal(median 50k, sigma_ln 1) "
+                        f"clipped [1e3,5e6], {N} photons",
+            "batched_photons_per_s": N / (ms_b / 1e3), "batched_ms": ms_b,
+            "loop_photons_per_s": N / (ms_l / 1e3), "loop_ms": ms_l,
+            "speedup_batched_over_loop": ms_l / ms_b,
+            "batched_event_done_ms_p50_p99": [float(np.percentile(lat_b, 50)), float(np.percentile(lat_b, 99))],
+            "loop_event_ms_p50_p99": [float(np.percentile(per, 50)), float(np.percentile(per, 99))],
+            "loop_event_done_ms_p50_p99": [float(np.percentile(lat_l, 50)), float(np.percentile(lat_l, 99))],
+            "autotuned": {k: best[k] for k in ("block", "regroup", "chunk", "photons_per_s", "sample_photons")},
+            "cuda_graph": True, "hits": nh_b, "status": st_b}
+
+
+def measure_scan(torch, E, dev, n_rays=1 << 24):
+    """C2: rays/s of the CSG scan over the 15-node tree with torus, and FP64 distance error"""
+    from opticks_b200 import scenes
+    from oracle import oracle as O
+    fd, p = scenes.csg_scan_tree(with_torus=True)
+    A = fd.arrays()
+    _, lib, _, _ = scenes.sphere_in_box(1)
+    eng = E.Engine(A, lib.arrays(), E.default_config(max_photon=64), device=dev.index)
+    rays = scenes.scan_rays(n_rays, seed=0)
+    r = torch.from_numpy(rays).to(dev)
+    out = torch.empty((n_rays, 4), dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    assert st.cuda_stream != 0, "run on a non-default stream so the library launches where the events are recorded"
+    res = {}
+    for pol in (0, 1):
+        eng.scan_device(p, r, n_rays, out, 0.0, pol, st.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(3):
+            eng.scan_device(p, r, n_rays, out, 0.0, pol, st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        o = out.cpu().numpy()
+        sub = slice(0, 1 << 21)
+        t64, _ = O.csg_scan_t64(A["node"], A["itra"], int(A["prim"].view(np.int32)[p, 0, 1]), rays[:, sub], 0.0)
+        hg, h64 = o[sub, 3] > 0, t64 > 0
+        both = hg & h64
+        rel = np.abs(o[sub, 3][both] - t64[both]) / np.maximum(t64[both], 1.0)
+        res["polish" if pol else "fp32"] = {"rays_per_s": n_rays / (ms / 1e3), "ms": ms,
+                                            "bytes_per_ray": 40, "achieved_gbs": 40 * n_rays / (ms / 1e3) / 1e9,
+                                            "fp64_check_rays": int(1 << 21), "hit_miss_mismatch": int((hg != h64).sum()),
+                                            "rel_t_err_p999": float(np.quantile(rel, 0.999)), "rel_t_err_max": float(rel.max())}
+    eng.close()
+    return dict(workload=f"{n_rays} rays, origins uniform in a 2 m cube, isotropic; 15-node CSG tree with torus", **res)
 
 
 def main():
@@ -163,10 +268,11 @@ def main():
     ap.add_argument("--per-genstep", type=int, default=10000)
     ap.add_argument("--ref-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -179,14 +285,17 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    # a dedicated stream: the library launches on it, and the CUDA events are recorded on it
+    work_stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(work_stream)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    fd, lib, phys, gs = workload(args.gensteps, args.per_genstep)
+    fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
     N = int(gs.view(np.int32)[:, 0, 3].sum())
     eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=N, num_sensor=scenes.NUM_PMT), device=local)
-    dev = torch.device("cuda", local)
     g_dev = torch.from_numpy(gs).to(dev)
     photon = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
     seq = torch.empty((N, 2, 2), dtype=torch.int64, device=dev)
@@ -197,24 +306,20 @@ def main():
 
     def step(ev, with_hits=True):
         return eng.simulate_device(g_dev, N, ev, photon=photon, seq=seq, hit=hit if with_hits else None,
-                                   hit_capacity=N if with_hits else 0, sensor_hits=sensor if with_hits else None,
-                                   stream=sp)
+                                   hit_capacity=N if with_hits else 0, sensor_hits=sensor if with_hits else None, stream=sp)
 
-    base_event = rank * 1000
+    base_event = rank * 1000 + 1          # every rank simulates its own events (event > 0: jumped streams)
     for w in range(args.warmup):
-        nh, st = step(base_event + w)
+        step(base_event + w)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    # ---- timed region (device path, events on the launch stream)
-    launches_per_step = 5
     hits_total = 0
     with Clocks(local) as clk:
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for s in range(args.steps):
             nh, st = step(base_event + 100 + s)
@@ -231,10 +336,9 @@ def main():
         ms_max = float(t.item())
     value = world * N * args.steps / (ms_max / 1e3)
 
-    # ---- dominant kernel alone (k_simulate + the genstep scan, no hit compaction)
-    k0 = torch.cuda.Event(enable_timing=True)
-    k1 = torch.cuda.Event(enable_timing=True)
-    ksteps = max(2, min(args.steps, 3))
+    # dominant kernel alone: the simulate launch without hit selection (genstep scan + jump + kernel)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ksteps = 3
     k0.record(stream)
     for s in range(ksteps):
         step(base_event + 200 + s, with_hits=False)
@@ -243,31 +347,36 @@ def main():
     k_ms = k0.elapsed_time(k1) / ksteps
     f_hit = hits_total / (N * args.steps)
     ppg = N / len(gs)
-    bytes_per_photon = 24 + 64 + 32 + 96.0 / ppg + 4.0 / 32
+    bytes_per_photon = BYTES_PER_PHOTON_FIXED + 96.0 / ppg
     peak, peak_kind = load_peaks()
     achieved = N * bytes_per_photon / (k_ms / 1e3) / 1e9
 
-    # ---- end to end through the host API with pinned buffers
-    e2e = None
-    if rank == 0 or world > 1:
-        ph_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
-        sq_h = torch.empty((N, 2, 2), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
-        ht_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
-        gs_h = torch.from_numpy(gs).pin_memory().numpy()
-        times, d2h = [], []
-        for s in range(args.e2e_steps + 1):
-            t0 = time.perf_counter()
-            out = eng.simulate_into(gs_h, base_event + 300 + s, ph_h, sq_h, ht_h)
-            dt = time.perf_counter() - t0
-            if s > 0:
-                times.append(dt)
-                d2h.append(N * 64 + N * 32 + out["num_hit"] * 64)
-        e2e = {"value": N / statistics.mean(times), "unit": METRIC, "h2d_bytes_per_step": int(gs.nbytes),
-               "d2h_bytes_per_step": int(statistics.mean(d2h)), "ms_per_step": 1e3 * statistics.mean(times)}
+    # end to end through the host API with pinned buffers
+    ph_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
+    sq_h = torch.empty((N, 2, 2), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    ht_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
+    gs_h = torch.from_numpy(gs).pin_memory().numpy()
+    times, d2h = [], []
+    for s in range(args.e2e_steps + 1):
+        t0 = time.perf_counter()
+        out = eng.simulate_into(gs_h, base_event + 300 + s, ph_h, sq_h, ht_h)
+        dt = time.perf_counter() - t0
+        if s > 0:
+            times.append(dt)
+            d2h.append(N * 64 + N * 32 + out["num_hit"] * 64)
+    e2e = {"value": N / statistics.mean(times), "unit": METRIC, "h2d_bytes_per_step": int(gs.nbytes),
+           "d2h_bytes_per_step": int(statistics.mean(d2h)), "ms_per_step": 1e3 * statistics.mean(times)}
+    eng.close()
+    del photon, seq, hit
+    torch.cuda.empty_cache()
 
     clocks = clk.summary()
-    line = None
     if rank == 0:
+        forms = None
+        if not args.no_forms and world == 1:
+            forms = {"batched": measure_batched(torch, E, fd, lib, phys, dev, args.events,
+                                                tune_cache=os.path.join(ROOT, "gpurun_out", "autotune.json")),
+                     "scan": measure_scan(torch, E, dev)}
         cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(fd, phys, gs)
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -275,16 +384,16 @@ def main():
                 "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": len(gs), "photons_per_genstep": int(ppg),
                            "photons_per_step": N, "outputs": "photon+seq+hits(SD)+sensor counts",
                            "l2": "inputs larger than L2 (RNG states 240 MB read + 960 MB written per step)",
+                           "kernel": "persistent work queue, block 64, refill every bounce",
                            "parallelism": f"{world} independent event streams" if world > 1 else "1 GPU"},
-                "gpu_launches": launches_per_step * args.steps,
+                "gpu_launches": 7 * args.steps,
                 "hit_fraction": f_hit,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": None, "kernel": "k_simulate", "kernel_ms": k_ms,
+                             "traffic": None, "kernel": "k_sim_persistent", "kernel_ms": k_ms,
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
-                             "note": "issue-bound divergent ray/physics kernel; HBM roof far from binding"},
-                "e2e": e2e, "clocks": clocks, "cpu_baseline": cpu}
+                             "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},
+                "e2e": e2e, "clocks": clocks, "cpu_baseline": cpu, "forms": forms}
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
