@@ -147,14 +147,19 @@ int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d
 int phx_rng_sequence(phx_engine* e, int32_t event_index, int64_t photon_offset, int64_t num_photon,
                      int32_t num_per_photon, float* out);
 
-/* score-function adjoint of the expected hits per sensor.  theta (32) = absorption length,
- * Rayleigh length, reemission probability, refractive index in 8 wavelength bins of the
- * material line mat_line over [wl_lo, wl_hi).  Runs the forward pass with those properties
- * and accumulates grad (num_sensor,32) = sum over hits of d log p(path)/d theta, and
- * hits (num_sensor).  All pointers are device pointers. */
+/* Score-function adjoint of the expected hits per sensor (no counterpart in the reference).
+ * theta (HOST, 32 floats) = absorption length [0:8], Rayleigh length [8:16], reemission probability
+ * [16:24] and refractive index [24:32] of the material of texture line mat_line (4*boundary+0 or +3),
+ * piecewise constant in 8 bins of width (wl_hi-wl_lo)/8 over [wl_lo, wl_hi).  Every texture line of
+ * that material is re-tabulated with theta for this call (the engine's own tables stay unchanged; the
+ * group velocity in the bins is c/n).  One forward pass over the device gensteps accumulates
+ * d_hits[s] = hits on sensor s and d_grad[s*32+k] = sum over those hits of d log p(path)/d theta_k
+ * (absorption/scattering/sail densities, reemission and Fresnel branch probabilities; the change of
+ * the refracted direction with n is not included).  d_hits, d_grad: device doubles, (num_sensor)
+ * and (num_sensor*32); the engine must have config num_sensor > 0. */
 int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                        int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
-                       float* d_hits, float* d_grad, void* stream);
+                       double* d_hits, double* d_grad, void* stream);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,9 @@ struct phx_engine {
     unsigned nx = 0, ny = 0, hd_factor = 20;
     int num_bnd = 0;
     std::vector<float> bnd_host;   // kept for the adjoint (property re-tabulation)
+    std::vector<uint32_t> optical_host;
+    cudaArray_t adj_arr = nullptr;
+    cudaTextureObject_t adj_tex = 0;
     int num_wl = 0;
     // rng
     DevBuf<uint32_t> rng;
@@ -507,6 +510,8 @@ int phx_destroy(phx_engine* e)
     if (!e) return 0;
     cudaSetDevice(e->device);
     if (e->bnd_tex) cudaDestroyTextureObject(e->bnd_tex);
+    if (e->adj_tex) cudaDestroyTextureObject(e->adj_tex);
+    if (e->adj_arr) cudaFreeArray(e->adj_arr);
     if (e->icdf_tex) cudaDestroyTextureObject(e->icdf_tex);
     if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
@@ -618,6 +623,7 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     PHX_TRY(make_texture_f4(e->bnd_arr, e->bnd_tex, phys->bnd, (int)e->nx, (int)e->ny));
     PHX_TRYCU(e->optical.ensure((size_t)phys->num_bnd * 4));
     PHX_TRYCU(cudaMemcpy(e->optical.p, phys->optical, (size_t)phys->num_bnd * 4 * 16, cudaMemcpyHostToDevice));
+    e->optical_host.assign(phys->optical, phys->optical + (size_t)phys->num_bnd * 16);
     if (phys->icdf && phys->icdf_width > 1 && phys->icdf_layers > 0) {
         e->hd_factor = (unsigned)phys->hd_factor;
         PHX_TRY(make_texture_f1(e->icdf_arr, e->icdf_tex, phys->icdf, phys->icdf_width, phys->icdf_layers));
@@ -662,7 +668,7 @@ static PersistArgs persist_args_from(const phx_engine* e, const SimArgs& a)
 }
 
 // grid = SMs x resident blocks of the chosen block size (one wave of persistent blocks)
-template <bool POLISH, int BLOCK>
+template <bool POLISH, int BLOCK, bool ADJ = false>
 static int launch_persistent_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
     // occupancy is queried once per (device, kernel) so graph capture sees only the launch
@@ -672,14 +678,14 @@ static int launch_persistent_t(phx_engine* e, const PersistArgs& A, cudaStream_t
     if (!cached_sms[dev]) {
         int sms = 0, per_sm = 0;
         PHX_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sim_persistent<POLISH, BLOCK>, BLOCK, 0));
+        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sim_persistent<POLISH, BLOCK, ADJ>, BLOCK, 0));
         cached_per_sm[dev] = per_sm;
         cached_sms[dev] = sms;
     }
     const int sms = cached_sms[dev], per_sm = cached_per_sm[dev];
     const long long want = (A.N + BLOCK - 1) / BLOCK;
     const long long grid = std::max<long long>(1, std::min<long long>((long long)sms * std::max(1, per_sm), want));
-    k_sim_persistent<POLISH, BLOCK><<<(unsigned)grid, BLOCK, 0, st>>>(A);
+    k_sim_persistent<POLISH, BLOCK, ADJ><<<(unsigned)grid, BLOCK, 0, st>>>(A);
     PHX_CU(cudaGetLastError());
     return 0;
 }
@@ -1053,11 +1059,99 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
 
 int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                        int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
-                       float* d_hits, float* d_grad, void* stream)
+                       double* d_hits, double* d_grad, void* stream)
 {
-    (void)e; (void)d_gensteps; (void)num_genstep; (void)num_photon; (void)event_index; (void)theta;
-    (void)mat_line; (void)wl_lo; (void)wl_hi; (void)d_hits; (void)d_grad; (void)stream;
-    return phx_fail(-9, "phx_adjoint_device: not built yet");
+    if (!e || !theta || !d_hits || !d_grad || (num_genstep > 0 && !d_gensteps)) return phx_fail(-1, "phx_adjoint_device: null argument");
+    if (num_genstep < 0 || num_photon < 0 || event_index < 0) return phx_fail(-1, "phx_adjoint_device: negative size");
+    if (mat_line < 0 || mat_line >= e->num_bnd * 4 || !(wl_hi > wl_lo)) return phx_fail(-1, "phx_adjoint_device: bad material line or bins");
+    if (e->cfg.num_sensor <= 0) return phx_fail(-1, "phx_adjoint_device: the engine needs num_sensor > 0");
+    for (int k = 0; k < 32; k++)
+        if (!(theta[k] == theta[k])) return phx_fail(-1, "phx_adjoint_device: theta[%d] is NaN", k);
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    const uint32_t mat = e->optical_host[(size_t)mat_line * 4];
+    if (mat == 0) return phx_fail(-1, "phx_adjoint_device: line %d is not a material line", mat_line);
+    // re-tabulate every material line (omat/imat) of this material with theta, in 8 bins
+    const float binw = (wl_hi - wl_lo) / 8.f;
+    std::vector<float> tab(e->bnd_host);
+    const int nwl = e->num_wl;
+    for (int b = 0; b < e->num_bnd; b++)
+        for (int j = 0; j < 4; j += 3) {
+            if (e->optical_host[(size_t)(4 * b + j) * 4] != mat) continue;
+            float* g0 = tab.data() + (size_t)((b * 4 + j) * 2 + 0) * nwl * 4;
+            float* g1 = tab.data() + (size_t)((b * 4 + j) * 2 + 1) * nwl * 4;
+            for (int i = 0; i < nwl; i++) {
+                const float lam = e->nm0 + i * e->nms;
+                if (!(lam >= wl_lo && lam < wl_hi)) continue;
+                const int bin = std::min(7, (int)std::floor((lam - wl_lo) / binw));
+                g0[4 * i + 0] = theta[24 + bin];
+                g0[4 * i + 1] = theta[bin];
+                g0[4 * i + 2] = theta[8 + bin];
+                g0[4 * i + 3] = theta[16 + bin];
+                g1[4 * i + 0] = 299.792458f / theta[24 + bin];
+            }
+        }
+    if (!e->adj_arr) {
+        int rc = make_texture_f4(e->adj_arr, e->adj_tex, tab.data(), (int)e->nx, (int)e->ny);
+        if (rc) return rc;
+    } else {
+        PHX_CU(cudaMemcpy2DToArray(e->adj_arr, 0, 0, tab.data(), e->nx * sizeof(float4), e->nx * sizeof(float4), e->ny, cudaMemcpyHostToDevice));
+    }
+    int rc = ensure_rng(e, num_photon);
+    if (rc) return rc;
+    const int G = num_genstep;
+    const long long N = num_photon;
+    PHX_CU(e->gs_off.ensure((size_t)G + 1));
+    PHX_CU(e->counters.ensure(8));
+    PHX_CU(e->jump_tab.ensure(PHX_JUMP_MATW));
+    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
+    PHX_CU(cudaMemsetAsync(e->counters.p, 0, 2 * sizeof(long long), st));
+    PHX_CU(cudaMemsetAsync(d_hits, 0, sizeof(double) * (size_t)e->cfg.num_sensor, st));
+    PHX_CU(cudaMemsetAsync(d_grad, 0, sizeof(double) * (size_t)e->cfg.num_sensor * 32, st));
+    k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gensteps), G, e->gs_off.p);
+    if (event_index > 0) k_jump_build<<<1, 160, 0, st>>>(nullptr, (unsigned long long)event_index, e->jump_pow.p, e->jump_tab.p);
+    PHX_CU(cudaGetLastError());
+    SimArgs a;
+    a.S = scene_of(e, 0);
+    a.P = props_of(e);
+    a.P.bnd_tex = e->adj_tex;
+    a.C = loop_of(e);
+    a.gs = reinterpret_cast<const float4*>(d_gensteps);
+    a.gs_off = e->gs_off.p;
+    a.G = G;
+    a.N = N;
+    a.photon_offset = 0;
+    a.event_index = (unsigned long long)event_index;
+    a.skip = e->cfg.skipahead_event_offset;
+    a.rng = e->rng.p;
+    a.rng_slots = e->rng_slots;
+    a.jump = event_index > 0 ? e->jump_tab.p : nullptr;
+    a.photon = nullptr;
+    a.seq = nullptr;
+    a.hitword = nullptr;
+    a.hit_mask = e->cfg.hit_mask;
+    a.status = e->status.p;
+    PersistArgs A = persist_args_from(e, a);
+    A.queue = reinterpret_cast<unsigned long long*>(e->counters.p + 1);
+    A.regroup = e->cfg.regroup;
+    A.chunk = e->cfg.chunk;
+    A.adj_hits = d_hits;
+    A.adj_grad = d_grad;
+    A.num_sensor = e->cfg.num_sensor;
+    A.adj_mat = mat;
+    A.adj_nm0 = e->nm0;
+    A.adj_nms = e->nms;
+    A.adj_wl_lo = wl_lo;
+    A.adj_binw = binw;
+    if (N > 0) {
+        rc = launch_persistent_t<false, 64, true>(e, A, st);
+        if (rc) return rc;
+    }
+    PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaStreamSynchronize(st));
+    if (e->h_pinned[0] & ~(unsigned)PHX_STATUS_RNG_RANGE)
+        return phx_fail(-5, "phx_adjoint_device: device status 0x%x", e->h_pinned[0]);
+    return 0;
 }
 
 }  // extern "C"

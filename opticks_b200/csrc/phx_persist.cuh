@@ -42,6 +42,12 @@ struct PersistArgs {
     unsigned* ev_left;              // optional: photons left per event (batched), for completion times
     unsigned long long* ev_done_ns; // optional: globaltimer when the event's last photon finished
     int num_event;
+    // adjoint (ADJ kernels): per-sensor hit counts and score sums, (num_sensor) and (num_sensor, 32)
+    double* adj_hits;
+    double* adj_grad;
+    int num_sensor;
+    unsigned adj_mat;
+    float adj_nm0, adj_nms, adj_wl_lo, adj_binw;
 };
 
 PHX_D unsigned long long phx_globaltimer()
@@ -60,9 +66,13 @@ struct PhxLane {
     int ev;
 };
 
-template <bool POLISH>
-PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status)
+template <bool POLISH, bool ADJ>
+PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status, PhxScore* sc)
 {
+    if (ADJ) {
+#pragma unroll
+        for (int k = 0; k < 32; k++) sc->g[k] = 0.f;
+    }
     const int gi = phx_find_genstep(A.gs_off, A.G, idx);
     float4 g[6];
 #pragma unroll
@@ -96,10 +106,20 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
     L.ev = (int)ev;
 }
 
-template <bool POLISH>
-PHX_D void persist_finish(PhxLane& L, const PersistArgs& A)
+template <bool POLISH, bool ADJ>
+PHX_D void persist_finish(PhxLane& L, const PersistArgs& A, const PhxScore* sc)
 {
     const long long idx = L.idx;
+    if (ADJ && (L.p.flagmask & A.hit_mask) == A.hit_mask) {
+        // estimator of d E[hits_s] / d theta : sum over hits on s of the path score
+        const unsigned id = L.p.identity & 0xffffffu;
+        if (id > 0u && (int)(id - 1u) < A.num_sensor) {
+            const unsigned s = id - 1u;
+            atomicAdd(A.adj_hits + s, 1.0);
+            for (int k = 0; k < 32; k++)
+                if (sc->g[k] != 0.f) atomicAdd(A.adj_grad + (size_t)s * 32 + k, (double)sc->g[k]);
+        }
+    }
     if (A.photon) phx_store_photon(A.photon + idx, L.p);
     if (A.seq) {
         ulonglong2* s = reinterpret_cast<ulonglong2*>(A.seq + idx);
@@ -114,8 +134,8 @@ PHX_D void persist_finish(PhxLane& L, const PersistArgs& A)
 }
 
 // one bounce of CSGOptiX/CSGOptiX7.cu:477-509; returns true when the photon is finished
-template <bool POLISH>
-PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status)
+template <bool POLISH, bool ADJ>
+PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status, PhxScore* sc)
 {
     if (!(L.bounce < A.C.max_bounce && L.p.time < A.C.max_time)) return true;
     const float tmin = (L.p.obf & A.C.eps0_mask) ? A.C.tmin0 : A.C.tmin;
@@ -123,15 +143,21 @@ PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status)
     phx_trace<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
     if (prd.boundary() == 0xffffu) return true;
     prd.normal = normalize(prd.normal);
-    const int command = propagate(L.p, L.rng, prd, A.P, status);
+    const int command = propagate<ADJ>(L.p, L.rng, prd, A.P, status, sc);
     L.bounce++;
     seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
     return command == PHX_BREAK;
 }
 
-template <bool POLISH, int BLOCK>
+template <bool POLISH, int BLOCK, bool ADJ = false>
 __global__ void __launch_bounds__(BLOCK) k_sim_persistent(PersistArgs A)
 {
+    PhxScore score;
+    if (ADJ) {
+        score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
+        score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
+    }
+    PhxScore* sc = ADJ ? &score : nullptr;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
@@ -162,7 +188,7 @@ __global__ void __launch_bounds__(BLOCK) k_sim_persistent(PersistArgs A)
                 take = t;
             }
             if ((take >> lane) & 1u) {
-                persist_start<POLISH>(L, A, wnext + __popc(take & lanes_below), status);
+                persist_start<POLISH, ADJ>(L, A, wnext + __popc(take & lanes_below), status, sc);
                 active = true;
             }
             wnext += __popc(take);
@@ -170,8 +196,8 @@ __global__ void __launch_bounds__(BLOCK) k_sim_persistent(PersistArgs A)
         }
         if (!__any_sync(FULL, active)) break;
         for (int k = 0; k < regroup; k++) {
-            if (active && persist_step<POLISH>(L, A, status)) {
-                persist_finish<POLISH>(L, A);
+            if (active && persist_step<POLISH, ADJ>(L, A, status, sc)) {
+                persist_finish<POLISH, ADJ>(L, A, sc);
                 active = false;
             }
         }

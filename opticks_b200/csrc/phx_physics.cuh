@@ -63,7 +63,53 @@ struct PhxState {
     float4 material2;
     float4 surface;     // detect, absorb, reflect specular, reflect diffuse
     uint4 optical;      // x: 1-based surface index (0: none) ; y: ems
+    unsigned m1idx, m2idx;   // 1-based material indices of m1/m2 (qbnd s.index.x/y; adjoint only)
 };
+
+// Score-function accumulator of the adjoint: d log p(path) / d theta for the properties of one
+// material tabulated in 8 wavelength bins (kind 0 absorption length, 1 Rayleigh length,
+// 2 reemission probability, 3 refractive index).  A property at wavelength wl is the texture's
+// linear interpolation of its 1 nm samples, so d prop / d theta_b is the filter weight of the
+// samples that lie in bin b.
+struct PhxScore {
+    float g[32];
+    unsigned mat;              // 1-based material index of the parametrised material
+    float nm0, nms;            // texture wavelength domain
+    float wl_lo, binw;         // bins [wl_lo + b binw, wl_lo + (b+1) binw), b < 8
+};
+
+PHX_D void score_add(PhxScore& S, int kind, float wl, float v)
+{
+    const float fx = (wl - S.nm0) / S.nms;
+    const float f = floorf(fx);
+    const float a = fx - f;
+    const float l0 = S.nm0 + f * S.nms, l1 = l0 + S.nms;
+    const int b0 = (int)floorf((l0 - S.wl_lo) / S.binw);
+    const int b1 = (int)floorf((l1 - S.wl_lo) / S.binw);
+    if (b0 >= 0 && b0 < 8) S.g[kind * 8 + b0] += (1.f - a) * v;
+    if (b1 >= 0 && b1 < 8) S.g[kind * 8 + b1] += a * v;
+}
+
+// forward-mode dual numbers for d TransCoeff / d n
+struct PhxDual { float v, d; };
+PHX_D PhxDual dd(float v, float d) { PhxDual r; r.v = v; r.d = d; return r; }
+PHX_D PhxDual operator+(PhxDual a, PhxDual b) { return dd(a.v + b.v, a.d + b.d); }
+PHX_D PhxDual operator-(PhxDual a, PhxDual b) { return dd(a.v - b.v, a.d - b.d); }
+PHX_D PhxDual operator*(PhxDual a, PhxDual b) { return dd(a.v * b.v, a.d * b.v + a.v * b.d); }
+PHX_D PhxDual operator/(PhxDual a, PhxDual b) { return dd(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
+PHX_D PhxDual dsqrt(PhxDual a) { const float r = sqrtf(a.v); return dd(r, r > 0.f ? 0.5f * a.d / r : 0.f); }
+
+// TransCoeff of propagate_at_boundary as a function of (n1, n2) at fixed c1 and E1 amplitudes
+PHX_D PhxDual trans_coeff_dual(PhxDual n1, PhxDual n2, float c1, float E1x, float E1y)
+{
+    const PhxDual one = dd(1.f, 0.f), two = dd(2.f, 0.f), C1 = dd(c1, 0.f);
+    const PhxDual eta = n1 / n2;
+    const PhxDual c2 = dsqrt(one - eta * eta * (one - C1 * C1));
+    const PhxDual n1c1 = n1 * C1, n2c2 = n2 * c2, n2c1 = n2 * C1, n1c2 = n1 * c2;
+    const PhxDual tx = two * n1c1 * dd(E1x, 0.f) / (n1c1 + n2c2);
+    const PhxDual ty = two * n1c1 * dd(E1y, 0.f) / (n2c1 + n1c2);
+    return n2c2 * (tx * tx + ty * ty) / n1c1;
+}
 
 struct PhxProps {
     cudaTextureObject_t bnd_tex;    // (num_wl) x (num_bnd*4*2) float4, linear, normalized, wrap
@@ -85,6 +131,7 @@ PHX_D float4 boundary_lookup(const PhxProps& P, float nm, unsigned line, unsigne
     return tex2D<float4>(P.bnd_tex, x, y);
 }
 
+template <bool ADJ = false>
 PHX_D void fill_state(PhxState& s, const PhxProps& P, unsigned boundary, float wavelength, float cosTheta)
 {
     const int line = boundary * 4;
@@ -96,6 +143,10 @@ PHX_D void fill_state(PhxState& s, const PhxProps& P, unsigned boundary, float w
     s.material2 = boundary_lookup(P, wavelength, m2_line, 0);
     s.surface = boundary_lookup(P, wavelength, su_line, 0);
     s.optical = __ldg(P.optical + su_line);
+    if (ADJ) {
+        s.m1idx = __ldg(&P.optical[m1_line].x);
+        s.m2idx = __ldg(&P.optical[m2_line].x);
+    }
 }
 
 // hd20 inverse-CDF lookup qudarap/qscint.h:251-258 (hd10/hd0 for other tables)
@@ -392,8 +443,10 @@ PHX_COLD void rayleigh_scatter(PhxPhoton& p, curandStateXORWOW& rng, unsigned& s
     p.pol = polarization;
 }
 
-PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, float distance_to_boundary, const PhxProps& P, unsigned& status)
+template <bool ADJ = false>
+PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, float distance_to_boundary, const PhxProps& P, unsigned& status, PhxScore* sc = nullptr)
 {
+    const bool scored = ADJ && s.m1idx == sc->mat;
     const float absorption_length = s.material1.y;
     const float scattering_length = s.material1.z;
     const float reemission_prob = s.material1.w;
@@ -407,6 +460,13 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
             p.time += absorption_distance / group_velocity;
             p.pos += absorption_distance * (p.mom);
             float u_reemit = reemission_prob == 0.f ? 2.f : phx_uniform(rng);
+            if (scored) {
+                // absorbed at d (scattering later): log p = -log La - d/La - d/Ls ; then the reemission draw
+                const float d = absorption_distance;
+                score_add(*sc, 0, p.wavelength, -1.f / absorption_length + d / (absorption_length * absorption_length));
+                score_add(*sc, 1, p.wavelength, d / (scattering_length * scattering_length));
+                score_add(*sc, 2, p.wavelength, u_reemit < reemission_prob ? 1.f / reemission_prob : -1.f / (1.f - reemission_prob));
+            }
             if (u_reemit < reemission_prob) {
                 float u_re_wavelength = phx_uniform(rng);
                 float u_re_mom_ph = phx_uniform(rng);
@@ -425,6 +485,11 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
         }
     } else {
         if (scattering_distance <= distance_to_boundary) {
+            if (scored) {
+                const float d = scattering_distance;
+                score_add(*sc, 1, p.wavelength, -1.f / scattering_length + d / (scattering_length * scattering_length));
+                score_add(*sc, 0, p.wavelength, d / (absorption_length * absorption_length));
+            }
             p.time += scattering_distance / group_velocity;
             p.pos += scattering_distance * (p.mom);
             rayleigh_scatter(p, rng, status);
@@ -432,12 +497,19 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
             return PHX_CONTINUE;
         }
     }
+    if (scored) {
+        // reached the boundary unabsorbed and unscattered: log p = -D/La - D/Ls
+        const float D = distance_to_boundary;
+        score_add(*sc, 0, p.wavelength, D / (absorption_length * absorption_length));
+        score_add(*sc, 1, p.wavelength, D / (scattering_length * scattering_length));
+    }
     p.pos += distance_to_boundary * (p.mom);
     p.time += distance_to_boundary / group_velocity;
     return PHX_BOUNDARY;
 }
 
-PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal)
+template <bool ADJ = false>
+PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal, PhxScore* sc = nullptr)
 {
     const float n1 = s.material1.x;
     const float n2 = s.material2.x;
@@ -466,6 +538,12 @@ PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
     const float TransCoeff = (tir || n1c1 == 0.f ? 0.f : n2c2 * dot2(E2_t, E2_t) / n1c1);
     const float u_reflect = phx_uniform(rng);
     bool reflect = u_reflect > TransCoeff;
+    if (ADJ && !tir && n1c1 != 0.f && TransCoeff > 0.f && TransCoeff < 1.f && (s.m1idx == sc->mat || s.m2idx == sc->mat)) {
+        // Fresnel branch probability: log T (transmit) or log(1-T) (reflect), T = T(n1, n2)
+        const float k = reflect ? -1.f / (1.f - TransCoeff) : 1.f / TransCoeff;
+        if (s.m1idx == sc->mat) score_add(*sc, 3, p.wavelength, k * trans_coeff_dual(dd(n1, 1.f), dd(n2, 0.f), c1, E1.x, E1.y).d);
+        if (s.m2idx == sc->mat) score_add(*sc, 3, p.wavelength, k * trans_coeff_dual(dd(n1, 0.f), dd(n2, 1.f), c1, E1.x, E1.y).d);
+    }
     p.mom = reflect ? p.mom + 2.0f * c1 * oriented_normal : eta * (p.mom) + (eta * c1 - c2) * oriented_normal;
     const float3 A_paral = normalize(cross(p.mom, A_trans));
     p.pol = normal_incidence ? (reflect ? p.pol * (n2 > n1 ? -1.f : 1.f) : p.pol)
@@ -544,8 +622,9 @@ PHX_D int propagate_at_surface(unsigned& flag, PhxPhoton& p, curandStateXORWOW& 
     return action;
 }
 
-// qsim::propagate : returns CONTINUE/BREAK, sets the flag
-PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, const PhxProps& P, unsigned& status)
+// qsim::propagate : returns CONTINUE/BREAK, sets the flag.  ADJ adds the score terms.
+template <bool ADJ = false>
+PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, const PhxProps& P, unsigned& status, PhxScore* sc = nullptr)
 {
     const unsigned boundary = prd.boundary();
     const unsigned identity = prd.identity();
@@ -555,13 +634,13 @@ PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, con
     float cosTheta = dot(p.mom, normal);
     p.set_prd(boundary, identity, cosTheta, iindex);
     PhxState s;
-    fill_state(s, P, boundary, p.wavelength, cosTheta);
+    fill_state<ADJ>(s, P, boundary, p.wavelength, cosTheta);
     unsigned flag = 0;
-    int command = propagate_to_boundary(flag, p, rng, s, prd.distance, P, status);
+    int command = propagate_to_boundary<ADJ>(flag, p, rng, s, prd.distance, P, status, sc);
     if (command == PHX_BOUNDARY) {
         const int ems = (int)s.optical.y;
         if (ems == PHX_EMS_NOSURFACE) {
-            command = propagate_at_boundary(flag, p, rng, s, normal);
+            command = propagate_at_boundary<ADJ>(flag, p, rng, s, normal, sc);
         } else if (ems == PHX_EMS_SURFACE) {
             command = propagate_at_surface(flag, p, rng, s, normal);
         } else if (lposcost < 0.f) {

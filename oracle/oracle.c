@@ -425,7 +425,31 @@ static int trace(const oracle_scene* S, v3 o, v3 d, float tmin, prd_t* prd, int*
 /* ------------------------------------------------------------------ propagation */
 enum { CONTINUE = 0, BREAK = 1, BOUNDARY = 2 };
 
-typedef struct { f4 m1, m1g, m2, su; unsigned opt[4]; } state_t;
+typedef struct { f4 m1, m1g, m2, su; unsigned opt[4]; unsigned m1idx, m2idx; } state_t;
+
+/* FP64 score accumulator of the adjoint estimator (same terms as the engine's, in double):
+ * d log p / d theta for 8 wavelength bins x (absorption length, Rayleigh length, reemission
+ * probability, refractive index) of material `mat` (1-based index), weights = the linear texture
+ * interpolation weights of the 1 nm samples falling in each bin. */
+typedef struct { double g[32]; unsigned mat; double nm0, nms, wl_lo, binw; } oscore;
+
+static void oscore_add(oscore* S, int kind, float wl, double v)
+{
+    double fx = ((double)wl - S->nm0) / S->nms, f = floor(fx), a = fx - f;
+    double l0 = S->nm0 + f * S->nms, l1 = l0 + S->nms;
+    int b0 = (int)floor((l0 - S->wl_lo) / S->binw), b1 = (int)floor((l1 - S->wl_lo) / S->binw);
+    if (b0 >= 0 && b0 < 8) S->g[kind * 8 + b0] += (1.0 - a) * v;
+    if (b1 >= 0 && b1 < 8) S->g[kind * 8 + b1] += a * v;
+}
+
+/* TransCoeff and its derivatives in n1, n2 (analytic, double) */
+static double trans_T(double n1, double n2, double c1, double ex, double ey)
+{
+    double eta = n1 / n2, c2 = sqrt(1.0 - eta * eta * (1.0 - c1 * c1));
+    double n1c1 = n1 * c1, n2c2 = n2 * c2, n2c1 = n2 * c1, n1c2 = n1 * c2;
+    double tx = 2.0 * n1c1 * ex / (n1c1 + n2c2), ty = 2.0 * n1c1 * ey / (n2c1 + n1c2);
+    return n2c2 * (tx * tx + ty * ty) / n1c1;
+}
 
 static void rayleigh(photon_t* p, ustream* r)
 {
@@ -453,16 +477,23 @@ static void rayleigh(photon_t* p, ustream* r)
     p->pol = pol;
 }
 
-static int to_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s, float dist, const oracle_scene* S)
+static int to_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s, float dist, const oracle_scene* S, oscore* sc)
 {
     float ul = s->m1.y, sl = s->m1.z, rp = s->m1.w, gv = s->m1g.x;
     float us = U(r), ua = U(r);
     float sd = -sl * logf(us), ad = -ul * logf(ua);
+    int scored = sc && s->m1idx == sc->mat;
+    double La = ul, Ls = sl;
     if (ad <= sd) {
         if (ad <= dist) {
             p->time += ad / gv;
             p->pos = add(p->pos, mul(ad, p->mom));
             float ur = rp == 0.f ? 2.f : U(r);
+            if (scored) {
+                oscore_add(sc, 0, p->wavelength, -1.0 / La + (double)ad / (La * La));
+                oscore_add(sc, 1, p->wavelength, (double)ad / (Ls * Ls));
+                oscore_add(sc, 2, p->wavelength, ur < rp ? 1.0 / rp : -1.0 / (1.0 - rp));
+            }
             if (ur < rp) {
                 float uw = U(r), a = U(r), b = U(r), c = U(r), d = U(r);
                 p->wavelength = scint_wl(S, uw);
@@ -475,18 +506,26 @@ static int to_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s
             return BREAK;
         }
     } else if (sd <= dist) {
+        if (scored) {
+            oscore_add(sc, 1, p->wavelength, -1.0 / Ls + (double)sd / (Ls * Ls));
+            oscore_add(sc, 0, p->wavelength, (double)sd / (La * La));
+        }
         p->time += sd / gv;
         p->pos = add(p->pos, mul(sd, p->mom));
         rayleigh(p, r);
         *flag = 0x20;
         return CONTINUE;
     }
+    if (scored) {
+        oscore_add(sc, 0, p->wavelength, (double)dist / (La * La));
+        oscore_add(sc, 1, p->wavelength, (double)dist / (Ls * Ls));
+    }
     p->pos = add(p->pos, mul(dist, p->mom));
     p->time += dist / gv;
     return BOUNDARY;
 }
 
-static int at_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s, v3 nrm)
+static int at_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s, v3 nrm, oscore* sc)
 {
     float n1 = s->m1.x, n2 = s->m2.x, eta = n1 / n2;
     float _c1 = -dot3(p->mom, nrm);
@@ -510,6 +549,15 @@ static int at_boundary(unsigned* flag, photon_t* p, ustream* r, const state_t* s
     float T = (tir || n1c1 == 0.f) ? 0.f : n2c2 * (Etx * Etx + Ety * Ety) / n1c1;
     float u = U(r);
     int refl = u > T;
+    if (sc && !tir && n1c1 != 0.f && T > 0.f && T < 1.f && (s->m1idx == sc->mat || s->m2idx == sc->mat)) {
+        double k = refl ? -1.0 / (1.0 - (double)T) : 1.0 / (double)T;
+        double h1 = 1e-6 * n1, h2 = 1e-6 * n2;
+        /* central differences of the analytic T in double (step 1e-6 relative) */
+        if (s->m1idx == sc->mat)
+            oscore_add(sc, 3, p->wavelength, k * (trans_T(n1 + h1, n2, c1, E1x, E1y) - trans_T(n1 - h1, n2, c1, E1x, E1y)) / (2 * h1));
+        if (s->m2idx == sc->mat)
+            oscore_add(sc, 3, p->wavelength, k * (trans_T(n1, n2 + h2, c1, E1x, E1y) - trans_T(n1, n2 - h2, c1, E1x, E1y)) / (2 * h2));
+    }
     p->mom = refl ? add(p->mom, mul(2.0f * c1, on)) : add(mul(eta, p->mom), mul(eta * c1 - c2, on));
     v3 Ap = norm3(cross3(p->mom, At));
     if (ni) p->pol = refl ? mul(n2 > n1 ? -1.f : 1.f, p->pol) : p->pol;
@@ -558,7 +606,7 @@ static int at_surface(unsigned* flag, photon_t* p, ustream* r, const state_t* s,
     return CONTINUE;
 }
 
-static int propagate(photon_t* p, ustream* r, const prd_t* prd, const oracle_scene* S)
+static int propagate(photon_t* p, ustream* r, const prd_t* prd, const oracle_scene* S, oscore* sc)
 {
     unsigned bnd = prd->gpbd & 0xffffu, id = prd->iiid & 0xffffu, ii = prd->iiid >> 16;
     v3 n = prd->n;
@@ -575,11 +623,13 @@ static int propagate(photon_t* p, ustream* r, const prd_t* prd, const oracle_sce
     s.m2 = bnd_lookup(S, p->wavelength, m2, 0);
     s.su = bnd_lookup(S, p->wavelength, su, 0);
     memcpy(s.opt, S->optical + 4 * su, 16);
+    s.m1idx = S->optical[4 * m1];
+    s.m2idx = S->optical[4 * m2];
     unsigned flag = 0;
-    int cmd = to_boundary(&flag, p, r, &s, prd->t, S);
+    int cmd = to_boundary(&flag, p, r, &s, prd->t, S, sc);
     if (cmd == BOUNDARY) {
         int ems = (int)s.opt[1];
-        if (ems == 1) cmd = at_boundary(&flag, p, r, &s, n);
+        if (ems == 1) cmd = at_boundary(&flag, p, r, &s, n, sc);
         else if (ems == 2) cmd = at_surface(&flag, p, r, &s, n);
         else if (prd->lposcost < 0.f) cmd = at_surface(&flag, p, r, &s, n);
         else if (ems == 3) { (void)U(r); flag = 0x40; cmd = BREAK; }
@@ -602,8 +652,30 @@ static void add_nibble(uint64_t* his, uint64_t* bnd, unsigned slot, unsigned fla
 /* photon loop.  gs (G,6,4); uniforms (n,K) for photons first..first+n-1 of the event;
  * photon out (n,4,4) float; seq out (n,4) u64 ; returns OR of error bits:
  *   1 CSG evaluator error, 2 uniform stream exhausted */
+static int run_photons(const oracle_scene* S, const float* gs, int G, long long first, long long n,
+                       const float* uniforms, int K, float* photon, uint64_t* seq,
+                       const oscore* proto, int num_sensor, double* hits, double* grad);
+
 int oracle_simulate(const oracle_scene* S, const float* gs, int G, long long first, long long n,
                     const float* uniforms, int K, float* photon, uint64_t* seq)
+{
+    return run_photons(S, gs, G, first, n, uniforms, K, photon, seq, NULL, 0, NULL, NULL);
+}
+
+/* FP64 reference of the adjoint estimator: hits[s] and grad[s*32+k] = sum over hits on sensor s
+ * of the path score, with the same photons as oracle_simulate (scene tables already re-tabulated) */
+int oracle_adjoint(const oracle_scene* S, const float* gs, int G, long long first, long long n, const float* uniforms, int K,
+                   unsigned mat, double nm0, double nms, double wl_lo, double binw, int num_sensor, double* hits, double* grad)
+{
+    oscore proto;
+    memset(&proto, 0, sizeof(proto));
+    proto.mat = mat; proto.nm0 = nm0; proto.nms = nms; proto.wl_lo = wl_lo; proto.binw = binw;
+    return run_photons(S, gs, G, first, n, uniforms, K, NULL, NULL, &proto, num_sensor, hits, grad);
+}
+
+static int run_photons(const oracle_scene* S, const float* gs, int G, long long first, long long n,
+                       const float* uniforms, int K, float* photon, uint64_t* seq,
+                       const oscore* proto, int num_sensor, double* hits, double* grad)
 {
     long long* off = (long long*)malloc(sizeof(long long) * (G + 1));
     off[0] = 0;
@@ -627,6 +699,8 @@ int oracle_simulate(const oracle_scene* S, const float* gs, int G, long long fir
         p.identity = ((unsigned)((idx >> 32) & 0xff) << 24) | (p.identity & 0xffffffu);
         uint64_t his[2] = { 0, 0 }, bn[2] = { 0, 0 };
         int err = 0;
+        oscore score, *sc = NULL;
+        if (proto) { score = *proto; memset(score.g, 0, sizeof(score.g)); sc = &score; }
         add_nibble(his, bn, 0, p.obf & 0xffffu, (p.obf >> 16) & 0x7fffu);
         int bounce = 0;
         while (bounce < S->max_bounce && p.time < S->max_time) {
@@ -636,11 +710,22 @@ int oracle_simulate(const oracle_scene* S, const float* gs, int G, long long fir
             trace(S, p.pos, p.mom, tmin, &prd, &err);
             if ((prd.gpbd & 0xffffu) == 0xffffu) break;
             prd.n = norm3(prd.n);
-            int cmd = propagate(&p, &r, &prd, S);
+            int cmd = propagate(&p, &r, &prd, S, sc);
             bounce++;
             add_nibble(his, bn, (unsigned)bounce, p.obf & 0xffffu, (p.obf >> 16) & 0x7fffu);
             if (cmd == BREAK) break;
         }
+        if (sc && (p.flagmask & S->hit_mask) == S->hit_mask) {
+            unsigned id = p.identity & 0xffffffu;
+            if (id > 0 && (int)(id - 1) < num_sensor) {
+#pragma omp critical
+                {
+                    hits[id - 1] += 1.0;
+                    for (int k = 0; k < 32; k++) grad[(size_t)(id - 1) * 32 + k] += sc->g[k];
+                }
+            }
+        }
+        if (!photon) { err_all |= (err ? 1 : 0) | (r.over ? 2 : 0); continue; }
         float* o = photon + 16 * j;
         o[0] = p.pos.x; o[1] = p.pos.y; o[2] = p.pos.z; o[3] = p.time;
         o[4] = p.mom.x; o[5] = p.mom.y; o[6] = p.mom.z; memcpy(o + 7, &p.hitcount_iindex, 4);

@@ -65,6 +65,9 @@ def lib() -> C.CDLL:
         L.oracle_tex2d_f4.restype = None
         L.oracle_tex2d_f4.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p]
         L.oracle_threads.restype = C.c_int
+        L.oracle_adjoint.restype = C.c_int
+        L.oracle_adjoint.argtypes = [C.POINTER(OracleScene), C.c_void_p, C.c_int, C.c_longlong, C.c_longlong, C.c_void_p, C.c_int,
+                                     C.c_uint, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -155,6 +158,19 @@ class Scene:
         seq = np.zeros((n, 2, 2), np.uint64)
         err = lib().oracle_simulate(C.byref(self.s), _p(gs), len(gs), first, n, _p(u), K, _p(photon), _p(seq))
         return photon, seq, err
+
+    def adjoint(self, gs: np.ndarray, uniforms: np.ndarray, mat_line: int, wl_lo: float, wl_hi: float, num_sensor: int,
+                first: int = 0, wl_low: float = 60.0, wl_step: float = 1.0):
+        """FP64 reference of the score-function estimator (the scene's tables must already hold theta)"""
+        gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
+        u = np.ascontiguousarray(uniforms, np.float32)
+        n, K = u.shape
+        mat = int(self.optical[mat_line, 0])
+        hits = np.zeros((num_sensor,), np.float64)
+        grad = np.zeros((num_sensor, 32), np.float64)
+        err = lib().oracle_adjoint(C.byref(self.s), _p(gs), len(gs), first, n, _p(u), K, mat, wl_low, wl_step, wl_lo,
+                                   (wl_hi - wl_lo) / 8.0, num_sensor, _p(hits), _p(grad))
+        return hits, grad, err
 
 
 def csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, use_double: bool = False, polish: bool = False):
