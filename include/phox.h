@@ -161,6 +161,24 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
                        int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
                        double* d_hits, double* d_grad, void* stream);
 
+/* Hit merging: SPM::merge_partial_select (sysrap/SPM.cu:110-200, called per launch from
+ * QEvt::PerLaunchMerge qudarap/QEvt.cc:1172 and on concatenated results from QEvt::FinalMerge).
+ * Records are sphoton (lite 0, 64 B) or sphotonlite (lite 1, 16 B).  Selects records with
+ * (flagmask & select_flagmask) != 0 (0xffffffff: all records, already selected), groups them by the
+ * key (identity << 48) | unsigned(time / time_window) and reduces each group to one record
+ * (sphoton: the earliest record, flagmask OR, hitcount sum; sphotonlite: the first record, min time,
+ * flagmask OR, hitcount sum: sysrap/sphoton.h:292-320, sysrap/sphotonlite.h:68-97).  Output is in
+ * ascending key order.  time_window 0 returns the selected records in input order, unmerged.
+ * *num_out receives the number of output records; when it exceeds out_capacity nothing is written
+ * and the call fails (-3), so a caller can retry with *num_out (num_in rows are always enough).
+ * The call synchronises the stream (the output count is read back), as the reference does.
+ * num_in < 2^31.  Times are expected finite: a group whose times are all NaN keeps its first record. */
+int phx_merge_hits_device(phx_engine* e, const void* d_in, int64_t num_in, int32_t lite, uint32_t select_flagmask,
+                          float time_window, void* d_out, int64_t out_capacity, int64_t* num_out, void* stream);
+/* host arrays in and out; same semantics */
+int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, uint32_t select_flagmask, float time_window,
+                   void* out, int64_t out_capacity, int64_t* num_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,10 @@ SIGNATURES = {
     "phx_rng_sequence": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_void_p]),
     "phx_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_int32,
                                      C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "phx_merge_hits_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint32, C.c_float, C.c_void_p,
+                                        C.c_int64, C.POINTER(C.c_int64), C.c_void_p]),
+    "phx_merge_hits": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint32, C.c_float, C.c_void_p, C.c_int64,
+                                 C.POINTER(C.c_int64)]),
 }
 
 

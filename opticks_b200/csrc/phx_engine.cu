@@ -62,6 +62,21 @@ struct DevBuf {
     void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
 };
 
+#include "phx_merge.cuh"
+
+// scratch of the hit merge (grow-only, per engine)
+struct PhxMergeWs {
+    DevBuf<uint32_t> sel, tcount, val0, val1, head, tsum, hist, pmin, gor, gsum, hin, hout;
+    DevBuf<unsigned long long> key0, key1, amin, key_or;
+    DevBuf<long long> total;
+    void release()
+    {
+        sel.release(); tcount.release(); val0.release(); val1.release(); head.release(); tsum.release(); hist.release();
+        pmin.release(); gor.release(); gsum.release(); hin.release(); hout.release();
+        key0.release(); key1.release(); amin.release(); key_or.release(); total.release();
+    }
+};
+
 struct PhxBatchCall {
     const float* gs; const int32_t* ev; int G; long long N; int block, chunk, regroup, num_event;
     uint64_t* done; float* photon; uint64_t* seq; float* hit; long long hcap; uint32_t* sensor; cudaStream_t st;
@@ -110,6 +125,7 @@ struct phx_engine {
     const void* batch_bufs[11] = {};
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
+    PhxMergeWs merge;
 };
 
 static PhxScene scene_of(const phx_engine* e, int polish)
@@ -521,6 +537,7 @@ int phx_destroy(phx_engine* e)
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
     e->jump_pow.release(); e->jump_tab.release();
+    e->merge.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -1241,5 +1258,155 @@ extern "C" int phx_simulate_device_noalloc(phx_engine* e, const float* d_genstep
     d_out->num_photon = N;
     d_out->num_hit = nh;
     d_out->status = e->h_pinned[0];
+    return 0;
+}
+
+// ------------------------------------------------------------------ hit merging
+// exclusive scan of n u32 in place; the total goes to *d_total when given
+static int merge_scan(PhxMergeWs& w, uint32_t* x, long long n, long long* d_total, cudaStream_t st)
+{
+    const long long nt = (n + PHX_MERGE_SCAN_TILE - 1) / PHX_MERGE_SCAN_TILE;
+    PHX_CU(w.tsum.ensure((size_t)std::max(1LL, nt)));
+    PHX_CU(w.total.ensure(2));
+    k_scan_tile<<<(unsigned)nt, 256, 0, st>>>(x, n, w.tsum.p);
+    k_block_scan<<<1, 1024, 0, st>>>(w.tsum.p, (int)nt, d_total ? d_total : w.total.p + 1);
+    k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, w.tsum.p);
+    PHX_CU(cudaGetLastError());
+    return 0;
+}
+
+// read back a few bytes through the engine's pinned words (synchronises the stream)
+static int merge_read(phx_engine* e, const void* d, size_t bytes, void* h, cudaStream_t st)
+{
+    PHX_CU(cudaMemcpyAsync(e->h_pinned + 48, d, bytes, cudaMemcpyDeviceToHost, st));
+    PHX_CU(cudaStreamSynchronize(st));
+    memcpy(h, e->h_pinned + 48, bytes);
+    return 0;
+}
+
+template <int LITE>
+static int merge_impl(phx_engine* e, const uint32_t* in, long long n, uint32_t mask, float tw, uint32_t* out, long long cap,
+                      long long* num_out, cudaStream_t st)
+{
+    PhxMergeWs& w = e->merge;
+    *num_out = 0;
+    if (n == 0) return 0;
+    long long m = n;
+    const uint32_t* sel = nullptr;
+    int rc;
+    PHX_CU(w.total.ensure(2));
+    if (mask != 0xffffffffu) {
+        const long long nt = (n + PHX_MERGE_TILE - 1) / PHX_MERGE_TILE;
+        PHX_CU(w.tcount.ensure((size_t)nt));
+        PHX_CU(w.sel.ensure((size_t)n));
+        k_merge_sel_count<LITE><<<(unsigned)nt, 256, 0, st>>>(in, n, mask, w.tcount.p);
+        k_block_scan<<<1, 1024, 0, st>>>(w.tcount.p, (int)nt, w.total.p);
+        k_merge_sel_write<LITE><<<(unsigned)nt, 256, 0, st>>>(in, n, mask, w.tcount.p, w.sel.p);
+        PHX_CU(cudaGetLastError());
+        if ((rc = merge_read(e, w.total.p, sizeof(long long), &m, st))) return rc;
+        sel = w.sel.p;
+    }
+    if (m == 0) return 0;
+    const int W = PhxRec<LITE>::W;
+    const unsigned grid = (unsigned)std::min<long long>((m + 255) / 256, 148LL * 16);
+    if (tw == 0.f) {                 // selection only, input order
+        *num_out = m;
+        if (m > cap) return phx_fail(-3, "phx_merge_hits: %lld records selected, out_capacity %lld", m, cap);
+        k_merge_gather<LITE><<<(unsigned)std::min<long long>((m * W + 255) / 256, 148LL * 32), 256, 0, st>>>(in, sel, m, out);
+        PHX_CU(cudaGetLastError());
+        return 0;
+    }
+    PHX_CU(w.key0.ensure((size_t)m)); PHX_CU(w.key1.ensure((size_t)m));
+    PHX_CU(w.val0.ensure((size_t)m)); PHX_CU(w.val1.ensure((size_t)m));
+    PHX_CU(w.key_or.ensure(1));
+    PHX_CU(cudaMemsetAsync(w.key_or.p, 0, sizeof(unsigned long long), st));
+    k_merge_keys<LITE><<<grid, 256, 0, st>>>(in, sel, m, tw, w.key0.p, w.val0.p, w.key_or.p);
+    PHX_CU(cudaGetLastError());
+    unsigned long long kor = 0;
+    if ((rc = merge_read(e, w.key_or.p, sizeof(kor), &kor, st))) return rc;
+    // stable LSD radix passes over the key bytes that are non-zero somewhere
+    const long long nt = (m + PHX_MERGE_TILE - 1) / PHX_MERGE_TILE;
+    PHX_CU(w.hist.ensure((size_t)(256 * nt)));
+    unsigned long long* kin = w.key0.p;
+    unsigned long long* kout = w.key1.p;
+    uint32_t* vin = w.val0.p;
+    uint32_t* vout = w.val1.p;
+    for (int b = 0; b < 8; b++) {
+        if (((kor >> (8 * b)) & 0xffull) == 0ull) continue;
+        k_radix_hist<<<(unsigned)nt, 256, 0, st>>>(kin, m, 8 * b, w.hist.p, (int)nt);
+        if ((rc = merge_scan(w, w.hist.p, 256 * nt, nullptr, st))) return rc;
+        k_radix_scatter<<<(unsigned)nt, 256, 0, st>>>(kin, vin, kout, vout, m, 8 * b, w.hist.p, (int)nt);
+        PHX_CU(cudaGetLastError());
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    // groups
+    PHX_CU(w.head.ensure((size_t)m));
+    k_merge_heads<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(kin, m, w.head.p);
+    if ((rc = merge_scan(w, w.head.p, m, w.total.p, st))) return rc;
+    long long ng = 0;
+    if ((rc = merge_read(e, w.total.p, sizeof(long long), &ng, st))) return rc;
+    *num_out = ng;
+    if (ng > cap) return phx_fail(-3, "phx_merge_hits: %lld merged records, out_capacity %lld", ng, cap);
+    PHX_CU(w.amin.ensure((size_t)ng)); PHX_CU(w.pmin.ensure((size_t)ng));
+    PHX_CU(w.gor.ensure((size_t)ng)); PHX_CU(w.gsum.ensure((size_t)ng));
+    PHX_CU(cudaMemsetAsync(w.amin.p, 0xff, sizeof(unsigned long long) * ng, st));
+    PHX_CU(cudaMemsetAsync(w.pmin.p, 0xff, sizeof(uint32_t) * ng, st));
+    PHX_CU(cudaMemsetAsync(w.gor.p, 0, sizeof(uint32_t) * ng, st));
+    PHX_CU(cudaMemsetAsync(w.gsum.p, 0, sizeof(uint32_t) * ng, st));
+    k_merge_reduce<LITE><<<grid, 256, 0, st>>>(in, sel, kin, vin, w.head.p, m, w.amin.p, w.pmin.p, w.gor.p, w.gsum.p);
+    k_merge_write<LITE><<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(in, sel, ng, w.amin.p, w.pmin.p, w.gor.p, w.gsum.p, out);
+    PHX_CU(cudaGetLastError());
+    return 0;
+}
+
+static int merge_check(const char* fn, phx_engine* e, const void* in, int64_t n, int32_t lite, float tw)
+{
+    if (!e) return phx_fail(-1, "%s: null engine", fn);
+    if (n < 0 || n > 0x7fffffffLL) return phx_fail(-1, "%s: num_in %lld outside [0, 2^31)", fn, (long long)n);
+    if (n > 0 && !in) return phx_fail(-1, "%s: null input", fn);
+    if (lite != 0 && lite != 1) return phx_fail(-1, "%s: record kind %d (0 sphoton, 1 sphotonlite)", fn, lite);
+    if (!(tw >= 0.f)) return phx_fail(-1, "%s: time_window must be >= 0", fn);
+    return 0;
+}
+
+int phx_merge_hits_device(phx_engine* e, const void* d_in, int64_t num_in, int32_t lite, uint32_t select_flagmask,
+                          float time_window, void* d_out, int64_t out_capacity, int64_t* num_out, void* stream)
+{
+    int rc = merge_check("phx_merge_hits_device", e, d_in, num_in, lite, time_window);
+    if (rc) return rc;
+    if (out_capacity > 0 && !d_out) return phx_fail(-1, "phx_merge_hits_device: null output with out_capacity > 0");
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    long long no = 0;
+    rc = lite ? merge_impl<1>(e, (const uint32_t*)d_in, num_in, select_flagmask, time_window, (uint32_t*)d_out, out_capacity, &no, st)
+              : merge_impl<0>(e, (const uint32_t*)d_in, num_in, select_flagmask, time_window, (uint32_t*)d_out, out_capacity, &no, st);
+    if (num_out) *num_out = no;
+    return rc;
+}
+
+int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, uint32_t select_flagmask, float time_window,
+                   void* out, int64_t out_capacity, int64_t* num_out)
+{
+    int rc = merge_check("phx_merge_hits", e, in, num_in, lite, time_window);
+    if (rc) return rc;
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    const size_t rb = lite ? 16 : 64;
+    PhxMergeWs& w = e->merge;
+    PHX_CU(w.hin.ensure((size_t)std::max<int64_t>(1, num_in) * rb / 4));
+    PHX_CU(w.hout.ensure((size_t)std::max<int64_t>(1, num_in) * rb / 4));
+    if (num_in > 0) PHX_CU(cudaMemcpyAsync(w.hin.p, in, (size_t)num_in * rb, cudaMemcpyHostToDevice, st));
+    long long no = 0;
+    rc = lite ? merge_impl<1>(e, w.hin.p, num_in, select_flagmask, time_window, w.hout.p, num_in, &no, st)
+              : merge_impl<0>(e, w.hin.p, num_in, select_flagmask, time_window, w.hout.p, num_in, &no, st);
+    if (num_out) *num_out = no;
+    if (rc) return rc;
+    if (no > out_capacity) return phx_fail(-3, "phx_merge_hits: %lld merged records, out_capacity %lld", no, (long long)out_capacity);
+    if (no > 0) {
+        if (!out) return phx_fail(-1, "phx_merge_hits: null output");
+        PHX_CU(cudaMemcpyAsync(out, w.hout.p, (size_t)no * rb, cudaMemcpyDeviceToHost, st));
+    }
+    PHX_CU(cudaStreamSynchronize(st));
     return 0;
 }

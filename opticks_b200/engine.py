@@ -201,6 +201,46 @@ class Engine:
                                                int(num_per_photon), _ptr(out)), "phx_rng_sequence")
         return out
 
+    # ------------------------------------------------------------------ hit merging
+    def merge_hits(self, records: np.ndarray, select_flagmask: int = 0xFFFFFFFF, time_window: float = 1.0) -> np.ndarray:
+        """SPM::merge_partial_select on host arrays: sphoton (n,4,4) or sphotonlite (n,4) records in,
+        merged records out (ascending (identity, time bucket) key)."""
+        rec = np.ascontiguousarray(records)
+        lite = _record_kind(rec)
+        n = rec.shape[0]
+        out = np.empty_like(rec)
+        no = C.c_int64(0)
+        _lib.check(_lib.lib().phx_merge_hits(self._h, _ptr(rec), int(n), lite, C.c_uint32(select_flagmask & 0xFFFFFFFF),
+                                             float(time_window), _ptr(out), int(n), C.byref(no)), "phx_merge_hits")
+        return out[: no.value]
+
+    def merge_hits_device(self, records_dev, out_dev, select_flagmask: int = 0xFFFFFFFF, time_window: float = 1.0,
+                          stream: int = 0) -> int:
+        """device form on torch CUDA tensors of sphoton (n,4,4) or sphotonlite (n,4) 32-bit words;
+        out_dev needs as many rows as records_dev.  Returns the number of merged records."""
+        shape = tuple(records_dev.shape)
+        lite = 1 if (len(shape) == 2 and shape[1] == 4) else 0
+        if not lite and shape[1:] != (4, 4):
+            raise ValueError(f"records must be (n,4,4) sphoton or (n,4) sphotonlite, got {shape}")
+        if tuple(out_dev.shape[1:]) != shape[1:] or out_dev.shape[0] < shape[0]:
+            raise ValueError("out_dev must match the record layout and hold as many rows as records_dev")
+        no = C.c_int64(0)
+        _lib.check(_lib.lib().phx_merge_hits_device(self._h, C.c_void_p(records_dev.data_ptr()), int(shape[0]), lite,
+                                                    C.c_uint32(select_flagmask & 0xFFFFFFFF), float(time_window),
+                                                    C.c_void_p(out_dev.data_ptr()), int(out_dev.shape[0]), C.byref(no),
+                                                    C.c_void_p(stream) if stream else None), "phx_merge_hits_device")
+        return int(no.value)
+
+
+def _record_kind(rec: np.ndarray) -> int:
+    if rec.dtype.itemsize != 4:
+        raise ValueError("records must be 32-bit words (float32/uint32)")
+    if rec.ndim == 3 and rec.shape[1:] == (4, 4):
+        return 0
+    if rec.ndim == 2 and rec.shape[1] == 4:
+        return 1
+    raise ValueError(f"records must be (n,4,4) sphoton or (n,4) sphotonlite, got {rec.shape}")
+
 
 class CSGOptiXService:
     """gensteps in, hits out (CSGOptiX/CSGOptiXService.h, CSGOptiX/opticks_CSGOptiX.cc:24-110)"""

@@ -3,6 +3,8 @@
 * ``liboracle.so``        C restatement of the simulate path (oracle.c) : CPU, FP32 + FP64 CSG
 * ``_ref/libref_csg.so``  the reference's own CSG intersector compiled for the CPU
 * ``_ref/libref_sim.so``  the reference's own qsim/CSG device code driven on the GPU
+* ``_ref/libref_spm.so``  the reference's own hit merge (sysrap/SPM.cu) on the GPU
+* ``merge.py``            numpy restatement of the hit merge
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and
 only as the checker / the timed CPU baseline.  Nothing in opticks_b200/ imports it.
@@ -19,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_CSG = os.path.join(HERE, "_ref", "libref_csg.so")
 REF_SIM = os.path.join(HERE, "_ref", "libref_sim.so")
+REF_SPM = os.path.join(HERE, "_ref", "libref_spm.so")
 
 
 def build(ref: bool = False) -> None:
@@ -206,6 +209,26 @@ def have_ref_csg() -> bool:
 
 def have_ref_sim() -> bool:
     return os.path.exists(REF_SIM)
+
+
+def have_ref_spm() -> bool:
+    return os.path.exists(REF_SPM)
+
+
+def ref_merge_gpu(records: np.ndarray, select_flagmask: int = 0xFFFFFFFF, time_window: float = 1.0) -> np.ndarray:
+    """SPM::merge_partial_select of the reference on the GPU (sphoton (n,4,4) or sphotonlite (n,4))"""
+    L = C.CDLL(REF_SPM)
+    L.ref_spm_merge.restype = C.c_int
+    L.ref_spm_merge.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_uint, C.c_float, C.c_void_p, C.c_longlong,
+                                C.POINTER(C.c_longlong)]
+    rec = np.ascontiguousarray(records)
+    lite = 1 if rec.ndim == 2 else 0
+    out = np.zeros_like(rec)
+    no = C.c_longlong(0)
+    rc = L.ref_spm_merge(_p(rec), len(rec), lite, select_flagmask & 0xFFFFFFFF, time_window, _p(out), len(rec), C.byref(no))
+    if rc != 0:
+        raise RuntimeError(f"ref_spm_merge failed {rc}")
+    return out[: no.value]
 
 
 def ref_csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, nthread: int = 0):
