@@ -35,6 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "photons/s"
+ENGINE_KW = {}          # engine config overrides from the command line (kernel_mode)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 BYTES_PER_PHOTON_FIXED = 24 + 64 + 32 + 4.0 / 32   # RNG state + sphoton + sseq + hit bit
 
@@ -156,14 +157,14 @@ def run_reference(args):
 
 
 def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=None):
-    """C4: uneven events in one persistent launch (autotuned, CUDA graph) vs the per-event loop"""
+    """C4: uneven events in one batched call vs the per-event loop, each in both loop forms (the
+    one-kernel persistent launch, autotuned and replayed as a CUDA graph, and the wavefront rounds);
+    the speed-up compares the faster batched form with the faster per-event loop"""
     from opticks_b200 import autotune, scenes
     gs = scenes.batched_events(num_event, lib=lib)
     ev = np.arange(len(gs), dtype=np.int32)
     counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
     N = int(counts.sum())
-    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=int(counts.max()), num_sensor=scenes.NUM_PMT), device=dev.index)
-    best = autotune.tune_batched(eng, gs, ev, torch, cache=tune_cache)
     g = torch.from_numpy(gs).to(dev)
     e = torch.from_numpy(ev).to(dev)
     photon = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
@@ -172,52 +173,63 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
     done = torch.zeros((num_event + 1,), dtype=torch.int64, device=dev)
     st = torch.cuda.current_stream(dev)
     assert st.cuda_stream != 0, "run on a non-default stream so the library launches where the events are recorded"
-
-    def batch():
-        return eng.simulate_batched_device(g, e, N, photon=photon, seq=seq, hit=hit, hit_capacity=N, block=best["block"],
-                                           regroup=best["regroup"], chunk=best["chunk"], num_event=num_event,
-                                           event_done_ns=done, stream=st.cuda_stream)
-    batch()                      # warm-up + graph capture
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    nh_b, st_b = batch()
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms_b = e0.elapsed_time(e1)
-    d = done.cpu().numpy()
-    lat_b = (d[:num_event] - d[num_event]) / 1e6    # ms from launch start to each event's last photon
     off = np.concatenate([[0], np.cumsum(counts)])
+    forms = {}
+    for mode in (1, 2):
+        eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=int(counts.max()), num_sensor=scenes.NUM_PMT,
+                                                           kernel_mode=mode), device=dev.index)
+        best = autotune.tune_batched(eng, gs, ev, torch, cache=tune_cache) if mode == 1 else None
+        kw = {k: best[k] for k in ("block", "regroup", "chunk")} if best else {}
 
-    def loop(record=None):
-        for k in range(num_event):
-            t0 = time.perf_counter()
-            eng.simulate_device(g[k:k + 1], int(counts[k]), k, photon=photon[off[k]:off[k + 1]], seq=seq[off[k]:off[k + 1]],
-                                hit=hit[off[k]:off[k + 1]], hit_capacity=int(counts[k]), stream=st.cuda_stream)
-            if record is not None:
-                record.append(time.perf_counter() - t0)
-    loop()                       # warm-up
-    torch.cuda.synchronize()
-    per = []
-    t0 = time.perf_counter()
-    e0.record(st)
-    loop(per)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms_l = e0.elapsed_time(e1)
-    per = np.array(per) * 1e3
-    lat_l = np.cumsum(per)
-    eng.close()
-    return {"workload": f"{num_event} events, one scintillation genstep each, lognormal(median 50k, sigma_ln 1) "
-                        f"clipped [1e3,5e6], {N} photons",
+        def batch():
+            return eng.simulate_batched_device(g, e, N, photon=photon, seq=seq, hit=hit, hit_capacity=N, num_event=num_event,
+                                               event_done_ns=done, stream=st.cuda_stream, **kw)
+        batch()                      # warm-up (+ graph capture in the persistent form)
+        torch.cuda.synchronize()
+        e0.record(st)
+        nh_b, st_b = batch()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_b = e0.elapsed_time(e1)
+        d = done.cpu().numpy()
+        lat_b = (d[:num_event] - d[num_event]) / 1e6    # ms from launch start to each event's last photon
+
+        def loop(record=None):
+            for k in range(num_event):
+                t0 = time.perf_counter()
+                eng.simulate_device(g[k:k + 1], int(counts[k]), k, photon=photon[off[k]:off[k + 1]], seq=seq[off[k]:off[k + 1]],
+                                    hit=hit[off[k]:off[k + 1]], hit_capacity=int(counts[k]), stream=st.cuda_stream)
+                if record is not None:
+                    record.append(time.perf_counter() - t0)
+        loop()                       # warm-up
+        torch.cuda.synchronize()
+        per = []
+        e0.record(st)
+        loop(per)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_l = e0.elapsed_time(e1)
+        per = np.array(per) * 1e3
+        lat_l = np.cumsum(per)
+        eng.close()
+        forms["persistent" if mode == 1 else "wavefront"] = {
             "batched_photons_per_s": N / (ms_b / 1e3), "batched_ms": ms_b,
             "loop_photons_per_s": N / (ms_l / 1e3), "loop_ms": ms_l,
-            "speedup_batched_over_loop": ms_l / ms_b,
             "batched_event_done_ms_p50_p99": [float(np.percentile(lat_b, 50)), float(np.percentile(lat_b, 99))],
             "loop_event_ms_p50_p99": [float(np.percentile(per, 50)), float(np.percentile(per, 99))],
             "loop_event_done_ms_p50_p99": [float(np.percentile(lat_l, 50)), float(np.percentile(lat_l, 99))],
-            "autotuned": {k: best[k] for k in ("block", "regroup", "chunk", "photons_per_s", "sample_photons")},
-            "cuda_graph": True, "hits": nh_b, "status": st_b}
+            "cuda_graph": mode == 1, "hits": nh_b, "status": st_b,
+            **({"autotuned": {k: best[k] for k in ("block", "regroup", "chunk", "photons_per_s", "sample_photons")}}
+               if best else {})}
+    bb = min(forms, key=lambda k: forms[k]["batched_ms"])
+    bl = min(forms, key=lambda k: forms[k]["loop_ms"])
+    return {"workload": f"{num_event} events, one scintillation genstep each, lognormal(median 50k, sigma_ln 1) "
+                        f"clipped [1e3,5e6], {N} photons",
+            "batched_photons_per_s": forms[bb]["batched_photons_per_s"], "batched_form": bb,
+            "loop_photons_per_s": forms[bl]["loop_photons_per_s"], "loop_form": bl,
+            "speedup_batched_over_loop": forms[bl]["loop_ms"] / forms[bb]["batched_ms"],
+            "forms": forms}
 
 
 def measure_scan(torch, E, dev, n_rays=1 << 24):
@@ -366,7 +378,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--kernel-mode", type=int, default=None, help="engine kernel_mode override (1 persistent, 2 wavefront)")
     args = ap.parse_args()
+    if args.kernel_mode is not None:
+        ENGINE_KW["kernel_mode"] = args.kernel_mode
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
@@ -390,7 +405,7 @@ def main():
 
     fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
     N = int(gs.view(np.int32)[:, 0, 3].sum())
-    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=N, num_sensor=scenes.NUM_PMT), device=local)
+    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=N, num_sensor=scenes.NUM_PMT, **ENGINE_KW), device=local)
     g_dev = torch.from_numpy(gs).to(dev)
     photon = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
     seq = torch.empty((N, 2, 2), dtype=torch.int64, device=dev)
@@ -416,15 +431,19 @@ def main():
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        launches = 0
         for s in range(args.steps):
             nh, st = step(base_event + 100 + s)
             hits_total += nh
+            launches += eng.last_call_stats()["kernel_launches"]
         e1.record(stream)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
     ms = e0.elapsed_time(e1)
     ms_max = ms
+    mode = int(eng.config.kernel_mode)
+    rounds = eng.last_call_stats()["wave_rounds"]
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -480,12 +499,16 @@ def main():
                 "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": len(gs), "photons_per_genstep": int(ppg),
                            "photons_per_step": N, "outputs": "photon+seq+hits(SD)+sensor counts",
                            "l2": "inputs larger than L2 (RNG states 240 MB read + 960 MB written per step)",
-                           "kernel": "persistent work queue, block 64, refill every bounce",
+                           "kernel": (f"wavefront: closest-hit and physics kernels over a pool of 2,097,152 paths, "
+                                      f"{rounds} rounds per step" if mode == 2 else
+                                      "persistent work queue, block 64, refill every bounce"),
                            "parallelism": f"{world} independent event streams" if world > 1 else "1 GPU"},
-                "gpu_launches": 7 * args.steps,
+                "gpu_launches": launches,
                 "hit_fraction": f_hit,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": None, "kernel": "k_sim_persistent", "kernel_ms": k_ms,
+                             "traffic": None, "kernel_ms": k_ms,
+                             "kernel": ("k_wave_init + k_wave_trace/k_wave_shade rounds (whole simulate launch sequence)"
+                                        if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
                              "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},
                 "e2e": e2e, "clocks": clocks, "cpu_baseline": cpu, "forms": forms}

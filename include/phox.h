@@ -69,7 +69,8 @@ typedef struct {
     uint32_t hit_mask;                /* OPTICKS_HIT_MASK                          SD */
     int32_t  root_polish;             /* FP64 polish of quadratic leaf roots       0 */
     int32_t  num_sensor;              /* length of the per-sensor hit count output 0 */
-    int32_t  kernel_mode;             /* 0: one thread per photon, 1: persistent threads with refill */
+    int32_t  kernel_mode;             /* 0: one thread per photon, 1: persistent threads with refill,
+                                         2: wavefront rounds (closest hit and physics as separate kernels) */
     int32_t  block;                   /* persistent kernel block size (32, 64, 128, 256) */
     int32_t  regroup;                 /* persistent kernel: bounces between lane refills */
     int32_t  chunk;                   /* persistent kernel: queue grab per warp in units of 32 photons */
@@ -178,6 +179,11 @@ int phx_merge_hits_device(phx_engine* e, const void* d_in, int64_t num_in, int32
 /* host arrays in and out; same semantics */
 int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, uint32_t select_flagmask, float time_window,
                    void* out, int64_t out_capacity, int64_t* num_out);
+
+/* Diagnostics of the last phx_simulate / phx_simulate_device call on this engine (no reference
+ * counterpart): kernels it launched and, in kernel_mode 2, wavefront rounds (one closest-hit and
+ * one physics launch each). */
+int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds);
 
 #ifdef __cplusplus
 }

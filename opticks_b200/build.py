@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libphox.so")
 
 SOURCES = ["phx_engine.cu", "phx_bvh.cc"]
-HEADERS = ["phx_pod.h", "phx_vec.cuh", "phx_csg.cuh", "phx_physics.cuh", "phx_kernels.cuh", "phx_bvh.h"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -139,17 +139,16 @@ static Box world_box(const float* bb6, const float* m)
     return b;
 }
 
-int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out)
+int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, double global_frac, int max_global)
 {
-    const int n = (int)in.size();
+    const int n_all = (int)in.size();
     out.nodes.clear();
     out.leaves.clear();
-    out.leaf_count = n;
-    Builder B;
-    B.boxes.resize(n);
-    B.cent.resize(3 * (size_t)n);
-    B.idx.resize(n);
-    for (int i = 0; i < n; i++) {
+    out.globals.clear();
+    out.cull[0] = out.cull[1] = out.cull[2] = out.cull[3] = 0.f;
+    std::vector<Box> all(n_all);
+    Box scene;
+    for (int i = 0; i < n_all; i++) {
         Box b = world_box(in[i].bbox, in[i].xform);
         // pad: relative to extent and to coordinate magnitude so FP32 slabs stay conservative
         double ext = std::max(b.hi[0] - b.lo[0], std::max(b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]));
@@ -157,16 +156,61 @@ int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out)
         for (int k = 0; k < 3; k++) mag = std::max(mag, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
         double pad = 1e-4 * ext + 4e-6 * mag + 1e-3;
         for (int k = 0; k < 3; k++) { b.lo[k] -= pad; b.hi[k] += pad; }
-        B.boxes[i] = b;
-        for (int k = 0; k < 3; k++) B.cent[3 * i + k] = 0.5 * (b.lo[k] + b.hi[k]);
-        B.idx[i] = i;
+        all[i] = b;
+        scene.grow(b);
+    }
+    // global leaves: the largest boxes covering a large part of the scene
+    std::vector<char> is_global(n_all, 0);
+    {
+        std::vector<int> cand;
+        const double thr = global_frac * scene.area();
+        for (int i = 0; i < n_all; i++)
+            if (global_frac > 0.0 && all[i].area() >= thr) cand.push_back(i);
+        std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return all[a].area() > all[b].area(); });
+        if ((int)cand.size() > max_global) cand.resize(std::max(0, max_global));
+        for (int i : cand) is_global[i] = 1;
+        for (int i = 0; i < n_all; i++) if (is_global[i]) out.globals.push_back(in[i].leaf);
+    }
+    std::vector<int> keep;
+    for (int i = 0; i < n_all; i++) if (!is_global[i]) keep.push_back(i);
+    const int n = (int)keep.size();
+    out.leaf_count = n;
+    Builder B;
+    B.boxes.resize(n);
+    B.cent.resize(3 * (size_t)n);
+    B.idx.resize(n);
+    Box ub;
+    for (int j = 0; j < n; j++) {
+        B.boxes[j] = all[keep[j]];
+        ub.grow(B.boxes[j]);
+        for (int k = 0; k < 3; k++) B.cent[3 * j + k] = 0.5 * (B.boxes[j].lo[k] + B.boxes[j].hi[k]);
+        B.idx[j] = j;
+    }
+    if (n > 0) {
+        // the largest ball about the centre of the hierarchy's box that no leaf box reaches: a ray
+        // segment with both ends inside it cannot hit a hierarchy leaf
+        double c[3], r2 = std::numeric_limits<double>::infinity();
+        for (int k = 0; k < 3; k++) c[k] = 0.5 * (ub.lo[k] + ub.hi[k]);
+        for (int j = 0; j < n; j++) {
+            double d2 = 0.0;
+            for (int k = 0; k < 3; k++) {
+                const double e = std::max(B.boxes[j].lo[k] - c[k], std::max(0.0, c[k] - B.boxes[j].hi[k]));
+                d2 += e * e;
+            }
+            r2 = std::min(r2, d2);
+        }
+        const double r = std::sqrt(r2) * (1.0 - 1e-5) - 1.0;   // 1 mm and a relative margin for FP32 rays
+        if (r > 0.0) {
+            out.cull[0] = (float)c[0]; out.cull[1] = (float)c[1]; out.cull[2] = (float)c[2];
+            out.cull[3] = (float)(r * r);
+        }
     }
     if (n == 0) return 0;
     B.nodes.reserve(2 * (size_t)n);
     int root2 = B.build(0, n, 0);
     // reorder leaves
     out.leaves.resize(n);
-    for (int i = 0; i < n; i++) out.leaves[i] = in[B.idx[i]].leaf;
+    for (int i = 0; i < n; i++) out.leaves[i] = in[keep[B.idx[i]]].leaf;
 
     // collapse to 4-wide. Each BVH2 inner node becomes one BVH4 node whose children are
     // the up-to-4 descendants obtained by opening the largest inner child.

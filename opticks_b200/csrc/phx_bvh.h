@@ -12,8 +12,13 @@ struct PhxLeafInput {
 struct PhxBvh4Result {
     std::vector<phx_bvh4_node> nodes;
     std::vector<phx_leaf> leaves;   // reordered to match the leaf ranges in nodes
+    std::vector<phx_leaf> globals;  // leaves tested by every ray before the traversal (input order)
+    float cull[4] = { 0.f, 0.f, 0.f, 0.f };   // empty ball of the BVH leaves: centre xyz, radius^2 (0: none)
     int leaf_count = 0;
     int max_depth = 0;
 };
 
-int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out);
+// Leaves whose box surface area is at least global_frac of the scene box's (at most max_global of
+// them, the largest) are kept out of the hierarchy: every ray would enter their boxes anyway, so
+// they are tested first, coherently across a warp, and their hit shortens the traversal.
+int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, double global_frac = 0.25, int max_global = 16);

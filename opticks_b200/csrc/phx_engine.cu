@@ -24,6 +24,7 @@
 #include "phx_bvh.h"
 #include "phx_kernels.cuh"
 #include "phx_persist.cuh"
+#include "phx_wave.cuh"
 #include "phx_rngjump.h"
 
 // ------------------------------------------------------------------ error plumbing
@@ -90,7 +91,9 @@ struct phx_engine {
     // geometry
     DevBuf<float4> node, itra, plan, inst_inv;
     DevBuf<phx_bvh4_node> bvh;
-    DevBuf<phx_leaf> leaves;
+    DevBuf<phx_leaf> leaves, globals;
+    int num_global = 0;
+    float cull[4] = { 0.f, 0.f, 0.f, 0.f };
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
     std::vector<int> prim_node_offset;
     // physics
@@ -126,6 +129,13 @@ struct phx_engine {
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
     PhxMergeWs merge;
+    // wavefront pool (kernel_mode 2)
+    DevBuf<PhxWaveSlot> wslot;
+    DevBuf<PhxWavePrd> wprd;
+    DevBuf<long long> wsidx;
+    DevBuf<uint32_t> wact0, wact1;
+    DevBuf<unsigned> wcnt;
+    long long last_launches = 0, last_rounds = 0;   // of the last plain simulate call
 };
 
 static PhxScene scene_of(const phx_engine* e, int polish)
@@ -137,7 +147,11 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.csg.node = e->node.p;
     S.csg.itra = e->itra.p;
     (void)polish;
-    S.empty = e->num_leaf == 0;
+    S.globals = e->globals.p;
+    S.num_global = e->num_global;
+    S.cull = make_float4(e->cull[0], e->cull[1], e->cull[2], e->cull[3]);
+    S.bvh_empty = e->num_leaf == 0;
+    S.empty = e->num_leaf == 0 && e->num_global == 0;
     return S;
 }
 
@@ -503,7 +517,7 @@ void phx_config_default(phx_config* c)
     c->hit_mask = PHX_SURFACE_DETECT;
     c->root_polish = 0;
     c->num_sensor = 0;
-    c->kernel_mode = 1;
+    c->kernel_mode = 2;
     c->block = 64;
     c->regroup = 1;
     c->chunk = 1;
@@ -532,12 +546,13 @@ int phx_destroy(phx_engine* e)
     if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
     e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release();
-    e->bvh.release(); e->leaves.release(); e->optical.release(); e->rng.release();
+    e->bvh.release(); e->leaves.release(); e->globals.release(); e->optical.release(); e->rng.release();
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
     e->jump_pow.release(); e->jump_tab.release();
     e->merge.release();
+    e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wcnt.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -625,6 +640,10 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     if (!bv.nodes.empty()) PHX_TRYCU(cudaMemcpy(e->bvh.p, bv.nodes.data(), bv.nodes.size() * sizeof(phx_bvh4_node), cudaMemcpyHostToDevice));
     PHX_TRYCU(e->leaves.ensure(std::max<size_t>(1, bv.leaves.size())));
     if (!bv.leaves.empty()) PHX_TRYCU(cudaMemcpy(e->leaves.p, bv.leaves.data(), bv.leaves.size() * sizeof(phx_leaf), cudaMemcpyHostToDevice));
+    e->num_global = (int)bv.globals.size();
+    memcpy(e->cull, bv.cull, sizeof(e->cull));
+    PHX_TRYCU(e->globals.ensure(std::max<size_t>(1, bv.globals.size())));
+    if (!bv.globals.empty()) PHX_TRYCU(cudaMemcpy(e->globals.p, bv.globals.data(), bv.globals.size() * sizeof(phx_leaf), cudaMemcpyHostToDevice));
     PHX_TRYCU(e->inst_inv.ensure(inv.size() / 4));
     PHX_TRYCU(cudaMemcpy(e->inst_inv.p, inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice));
 
@@ -719,6 +738,74 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
     }
 }
 
+// Wavefront form (phx_wave.cuh): fill a pool of paths, then rounds of trace + shade launches
+// until no path is live.  The live count is read back every PHX_WAVE_ROUNDS rounds, so the call
+// synchronises the stream; it cannot be captured into a graph.
+#define PHX_WAVE_POOL (1LL << 21)
+#define PHX_WAVE_ROUNDS 4
+
+template <typename K>
+static int wave_grid(K kernel, int dev, int* cache)
+{
+    if (!cache[dev]) {
+        int sms = 0, per_sm = 0;
+        PHX_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0));
+        cache[dev] = sms * std::max(1, per_sm);
+    }
+    return 0;
+}
+
+template <bool POLISH>
+static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
+{
+    static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {};
+    const int dev = e->device;
+    if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
+    int rc;
+    if ((rc = wave_grid(k_wave_init<POLISH>, dev, g_init))) return rc;
+    if ((rc = wave_grid(k_wave_trace<POLISH>, dev, g_trace))) return rc;
+    if ((rc = wave_grid(k_wave_shade<POLISH>, dev, g_shade))) return rc;
+    const long long N = A.N;
+    const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
+    PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
+    PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(2));
+    PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 2 * sizeof(unsigned), st));
+    WaveArgs W;
+    W.A = A;
+    W.slot = e->wslot.p; W.prd = e->wprd.p; W.sidx = e->wsidx.p; W.pool = pool;
+    uint32_t* act[2] = { e->wact0.p, e->wact1.p };
+    unsigned* cnt[2] = { e->wcnt.p, e->wcnt.p + 1 };
+    W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
+    const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
+    k_wave_init<POLISH><<<gi, 128, 0, st>>>(W);
+    PHX_CU(cudaGetLastError());
+    const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
+    e->last_rounds = 0;
+    int cur = 0;
+    bool done = false;
+    for (long long r = 0; r < max_rounds && !done;) {
+        for (int k = 0; k < PHX_WAVE_ROUNDS; k++, r++) {
+            W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
+            k_wave_trace<POLISH><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+            k_wave_shade<POLISH><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
+            cur = 1 - cur;
+        }
+        PHX_CU(cudaGetLastError());
+        PHX_CU(cudaMemcpyAsync(e->h_pinned + 40, cnt[cur], sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        PHX_CU(cudaStreamSynchronize(st));
+        done = e->h_pinned[40] == 0u;
+        e->last_rounds = r;
+    }
+    if (!done) return phx_fail(-5, "wavefront loop did not drain within %lld rounds", max_rounds);
+    return 0;
+}
+
+static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st)
+{
+    return e->cfg.root_polish ? launch_wave_t<true>(e, A, st) : launch_wave_t<false>(e, A, st);
+}
+
 extern "C" {
 
 // device buffers of one plain simulate call (engine buffers, or the fixed no-alloc scratch)
@@ -736,7 +823,7 @@ struct PhxPlainBufs {
 // into the engine's pinned words; the caller synchronises
 static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs, int G, long long N, int event_index,
                          long long photon_offset, phx_photon* photon, phx_seq* seq, phx_photon* hit, long long hcap,
-                         uint32_t* sensor, bool want_hits, cudaStream_t st)
+                         uint32_t* sensor, bool want_hits, cudaStream_t st, bool wave_ok = false)
 {
     const long long nword = (N + 31) / 32;
     PHX_CU(cudaMemsetAsync(b.status, 0, sizeof(unsigned), st));
@@ -763,20 +850,26 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
     a.hitword = want_hits ? b.hitword : nullptr;
     a.hit_mask = e->cfg.hit_mask;
     a.status = b.status;
-    if (N > 0 && e->cfg.kernel_mode == 1) {
-        // persistent threads with per-lane refill (phx_persist.cuh); hit bits are OR-ed in
+    if (N > 0 && (e->cfg.kernel_mode == 1 || e->cfg.kernel_mode == 2)) {
+        // persistent threads with per-lane refill (phx_persist.cuh), or the wavefront rounds
+        // (phx_wave.cuh); hit bits are OR-ed in
         if (want_hits) PHX_CU(cudaMemsetAsync(b.hitword, 0, sizeof(uint32_t) * (size_t)nword, st));
         PersistArgs A = persist_args_from(e, a);
         A.queue = reinterpret_cast<unsigned long long*>(b.counters + 1);
         A.regroup = e->cfg.regroup;
         A.chunk = e->cfg.chunk;
-        int rc = launch_persistent(e, A, e->cfg.block, st);
+        const bool wave = e->cfg.kernel_mode == 2 && wave_ok;
+        e->last_rounds = 0;
+        int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
+        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (wave ? 1 + 2 * e->last_rounds : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         const int B = PHX_SIM_BLOCK;
         if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
         else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
         PHX_CU(cudaGetLastError());
+        e->last_rounds = 0;
+        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + 1 + (want_hits ? 3 : 0);
     }
     if (sensor) PHX_CU(cudaMemsetAsync(sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
     if (want_hits && N > 0) {
@@ -813,7 +906,8 @@ static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long lo
     PHX_CU(e->blocksum.ensure((size_t)std::max<long long>(1, (nword + 255) / 256)));
     PHX_CU(e->jump_tab.ensure(PHX_JUMP_MATW));
     PhxPlainBufs b = { e->gs_off.p, e->hitword.p, e->wordoff.p, e->blocksum.p, e->counters.p, e->status.p, e->jump_tab.p };
-    rc = plain_enqueue(e, b, d_gs, G, N, event_index, photon_offset, photon, d_seq, d_hit, hit_capacity, d_sensor, want_hits, st);
+    rc = plain_enqueue(e, b, d_gs, G, N, event_index, photon_offset, photon, d_seq, d_hit, hit_capacity, d_sensor, want_hits, st,
+                       true);
     if (rc) return rc;
     PHX_CU(cudaStreamSynchronize(st));
     long long nh = 0;
@@ -988,7 +1082,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
         A.num_event = c.num_event;
     }
     if (N > 0) {
-        int rc = launch_persistent(e, A, c.block, st);
+        int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st) : launch_persistent(e, A, c.block, st);
         if (rc) return rc;
     }
     if (want_hits && N > 0) {
@@ -1041,7 +1135,7 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
     }
     if (c.num_event > 0) PHX_CU(e->ev_left.ensure((size_t)c.num_event));
     PHX_CU(e->jump_tab.ensure((size_t)std::max(1, c.G) * PHX_JUMP_MATW));
-    if (e->cfg.use_graph) {
+    if (e->cfg.use_graph && e->cfg.kernel_mode != 2) {
         // the captured graph bakes in every engine buffer pointer: reuse it only if none moved
         const void* bufs[11] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
                                  e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p };
@@ -1408,5 +1502,13 @@ int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, 
         PHX_CU(cudaMemcpyAsync(out, w.hout.p, (size_t)no * rb, cudaMemcpyDeviceToHost, st));
     }
     PHX_CU(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds)
+{
+    if (!e) return phx_fail(-1, "phx_last_call_stats: null engine");
+    if (kernel_launches) *kernel_launches = e->last_launches;
+    if (wave_rounds) *wave_rounds = e->last_rounds;
     return 0;
 }

@@ -11,14 +11,48 @@
 struct PhxScene {
     const phx_bvh4_node* bvh;   // root at 0
     const phx_leaf* leaves;
+    const phx_leaf* globals;    // leaves tested first by every ray (boxes spanning much of the scene)
     const float4* inst_inv;     // (num_inst*4) rows of the world->object 4x4 (row-vector convention)
     PhxCsgCtx csg;
+    float4 cull;                // ball no hierarchy leaf reaches: centre xyz, radius^2 (0: none)
+    int num_global;
+    int bvh_empty;              // no hierarchy leaves
     int empty;                  // no leaves at all
 };
+
+struct PhxBest {
+    float t;
+    int4 L;                     // leaf (inst, node_offset, gp_bd, ii_id); L.x < 0 : none
+    float4 isect;
+    float lposcost;
+};
+
+// IS program of CSGOptiX/CSGOptiX7.cu:896-967 for one (instance, prim) leaf: object-frame
+// intersect_prim, keep the closest hit and its lposcost
+template <bool POLISH>
+PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float3& o, const float3& d, float tmin, PhxBest& B,
+                         unsigned& status)
+{
+    const float4* q = S.inst_inv + 4 * L.x;
+    float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
+    const float3 lo = xform_row(m, o, 1.f);
+    const float3 ld = xform_row(m, d, 0.f);
+    float4 is;
+    const bool valid = intersect_prim<POLISH>(is, S.csg, L.y, tmin, lo, ld, status);
+    if (valid && is.w < B.t) {
+        B.t = is.w;
+        B.L = L;
+        B.isect = is;
+        const float3 lpos = lo + is.w * ld;
+        B.lposcost = lpos.z / sqrtf(dot(lpos, lpos));
+    }
+}
 
 // Closest hit over all (instance, prim) leaves: restates optixTrace over the IAS with the
 // IS program CSGOptiX/CSGOptiX7.cu:896-967 (object-frame intersect_prim, lposcost) and the
 // CH program :776-874 (object->world normal, iindex<<16|identity, globalPrimIdx<<16|boundary).
+// The global leaves are tested first, then the hierarchy is traversed unless the segment
+// [tmin, closest so far] lies inside the ball no hierarchy leaf reaches.
 // Returns false for a miss (prd boundary 0xffff).
 template <bool POLISH>
 PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float tmin, float tmax, PhxPRD& prd, unsigned& status)
@@ -29,100 +63,96 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
     prd.distance = 0.f;
     prd.lposcost = 0.f;
     if (S.empty) return false;
-    const float3 dd = make_float3(fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x,
-                                  fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y,
-                                  fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
-    const float3 inv = make_float3(1.f / dd.x, 1.f / dd.y, 1.f / dd.z);
-    const float3 oi = make_float3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
-    float best_t = tmax;
-    int best_leaf = -1;
-    float4 best_isect = make_float4(0.f, 0.f, 0.f, 0.f);
-    float best_lposcost = 0.f;
-
-    int stk[PHX_BVH_STACK];
-    float stt[PHX_BVH_STACK];
-    int sp = 0;
-    stk[sp] = 0; stt[sp] = tmin; sp++;
-    while (sp > 0) {
-        sp--;
-        const int ni = stk[sp];
-        if (stt[sp] > best_t) continue;
-        const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
-        const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
-        const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
-        const int4 ch = __ldg(reinterpret_cast<const int4*>(nf + 6));
-        const float lxa[4] = { lx.x, lx.y, lx.z, lx.w }, hxa[4] = { hx.x, hx.y, hx.z, hx.w };
-        const float lya[4] = { ly.x, ly.y, ly.z, ly.w }, hya[4] = { hy.x, hy.y, hy.z, hy.w };
-        const float lza[4] = { lz.x, lz.y, lz.z, lz.w }, hza[4] = { hz.x, hz.y, hz.z, hz.w };
-        const int cha[4] = { ch.x, ch.y, ch.z, ch.w };
-        float tn[4];
-        int hitmask = 0;
+    PhxBest B;
+    B.t = tmax;
+    B.L = make_int4(-1, 0, 0, 0);
+    B.isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    B.lposcost = 0.f;
+    for (int g = 0; g < S.num_global; g++)
+        phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), o, d, tmin, B, status);
+    bool traverse = !S.bvh_empty;
+    if (traverse && S.cull.w > 0.f) {
+        const float3 c = make_float3(S.cull.x, S.cull.y, S.cull.z);
+        const float3 p0 = o + tmin * d - c;
+        const float3 p1 = o + B.t * d - c;
+        traverse = !(dot(p0, p0) < S.cull.w && dot(p1, p1) < S.cull.w);
+    }
+    if (traverse) {
+        const float3 dd = make_float3(fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x,
+                                      fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y,
+                                      fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
+        const float3 inv = make_float3(1.f / dd.x, 1.f / dd.y, 1.f / dd.z);
+        const float3 oi = make_float3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
+        int stk[PHX_BVH_STACK];
+        float stt[PHX_BVH_STACK];
+        int sp = 0;
+        stk[sp] = 0; stt[sp] = tmin; sp++;
+        while (sp > 0) {
+            sp--;
+            const int ni = stk[sp];
+            if (stt[sp] > B.t) continue;
+            const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
+            const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
+            const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
+            const int4 ch = __ldg(reinterpret_cast<const int4*>(nf + 6));
+            const float lxa[4] = { lx.x, lx.y, lx.z, lx.w }, hxa[4] = { hx.x, hx.y, hx.z, hx.w };
+            const float lya[4] = { ly.x, ly.y, ly.z, ly.w }, hya[4] = { hy.x, hy.y, hy.z, hy.w };
+            const float lza[4] = { lz.x, lz.y, lz.z, lz.w }, hza[4] = { hz.x, hz.y, hz.z, hz.w };
+            const int cha[4] = { ch.x, ch.y, ch.z, ch.w };
+            float tn[4];
+            int hitmask = 0;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float tx0 = fmaf(lxa[c], inv.x, oi.x), tx1 = fmaf(hxa[c], inv.x, oi.x);
-            const float ty0 = fmaf(lya[c], inv.y, oi.y), ty1 = fmaf(hya[c], inv.y, oi.y);
-            const float tz0 = fmaf(lza[c], inv.z, oi.z), tz1 = fmaf(hza[c], inv.z, oi.z);
-            const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-            const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), best_t));
-            // slab arithmetic slack: boxes are padded on the host, and a relative slack here
-            tn[c] = tnear;
-            if (tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
-        }
-        // leaves first (closest box first), then push inner nodes far-to-near
-        int order[4] = { 0, 1, 2, 3 };
-#pragma unroll
-        for (int i = 1; i < 4; i++)
-#pragma unroll
-            for (int j = i; j > 0; j--) {
-                if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
+            for (int c = 0; c < 4; c++) {
+                const float tx0 = fmaf(lxa[c], inv.x, oi.x), tx1 = fmaf(hxa[c], inv.x, oi.x);
+                const float ty0 = fmaf(lya[c], inv.y, oi.y), ty1 = fmaf(hya[c], inv.y, oi.y);
+                const float tz0 = fmaf(lza[c], inv.z, oi.z), tz1 = fmaf(hza[c], inv.z, oi.z);
+                const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+                const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), B.t));
+                // slab arithmetic slack: boxes are padded on the host, and a relative slack here
+                tn[c] = tnear;
+                if (tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
             }
+            // leaves first (closest box first), then push inner nodes far-to-near
+            int order[4] = { 0, 1, 2, 3 };
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int c = order[k];
-            if (!(hitmask & (1 << c))) continue;
-            const int child = cha[c];
-            if (child >= 0) continue;
-            if (tn[c] > best_t) continue;
-            const int enc = -child - 1;
-            const int first = enc >> 3;
-            const int count = (enc & 7) + 1;
-            for (int li = first; li < first + count; li++) {
-                const int4 L = __ldg(reinterpret_cast<const int4*>(S.leaves + li));
-                const float4* q = S.inst_inv + 4 * L.x;
-                float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
-                const float3 lo = xform_row(m, o, 1.f);
-                const float3 ld = xform_row(m, d, 0.f);
-                float4 is;
-                const bool valid = intersect_prim<POLISH>(is, S.csg, L.y, tmin, lo, ld, status);
-                if (valid && is.w < best_t) {
-                    best_t = is.w;
-                    best_leaf = li;
-                    best_isect = is;
-                    const float3 lpos = lo + is.w * ld;
-                    best_lposcost = lpos.z / sqrtf(dot(lpos, lpos));
+            for (int i = 1; i < 4; i++)
+#pragma unroll
+                for (int j = i; j > 0; j--) {
+                    if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
                 }
-            }
-        }
 #pragma unroll
-        for (int k = 3; k >= 0; k--) {
-            const int c = order[k];
-            if (!(hitmask & (1 << c))) continue;
-            const int child = cha[c];
-            if (child <= 0) continue;
-            if (tn[c] > best_t) continue;
-            if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
-            stk[sp] = child; stt[sp] = tn[c]; sp++;
+            for (int k = 0; k < 4; k++) {
+                const int c = order[k];
+                if (!(hitmask & (1 << c))) continue;
+                const int child = cha[c];
+                if (child >= 0) continue;
+                if (tn[c] > B.t) continue;
+                const int enc = -child - 1;
+                const int first = enc >> 3;
+                const int count = (enc & 7) + 1;
+                for (int li = first; li < first + count; li++)
+                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), o, d, tmin, B, status);
+            }
+#pragma unroll
+            for (int k = 3; k >= 0; k--) {
+                const int c = order[k];
+                if (!(hitmask & (1 << c))) continue;
+                const int child = cha[c];
+                if (child <= 0) continue;
+                if (tn[c] > B.t) continue;
+                if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
+                stk[sp] = child; stt[sp] = tn[c]; sp++;
+            }
         }
     }
-    if (best_leaf < 0) return false;
-    const int4 L = __ldg(reinterpret_cast<const int4*>(S.leaves + best_leaf));
-    const float4* q = S.inst_inv + 4 * L.x;
+    if (B.L.x < 0) return false;
+    const float4* q = S.inst_inv + 4 * B.L.x;
     float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
-    prd.normal = xform_col(m, make_float3(best_isect.x, best_isect.y, best_isect.z), 0.f);
-    prd.distance = best_t;
-    prd.lposcost = best_lposcost;
-    prd.gp_bd = (unsigned)L.z;
-    prd.ii_id = (unsigned)L.w;
+    prd.normal = xform_col(m, make_float3(B.isect.x, B.isect.y, B.isect.z), 0.f);
+    prd.distance = B.t;
+    prd.lposcost = B.lposcost;
+    prd.gp_bd = (unsigned)B.L.z;
+    prd.ii_id = (unsigned)B.L.w;
     return true;
 }
 

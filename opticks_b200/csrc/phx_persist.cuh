@@ -57,6 +57,42 @@ PHX_D unsigned long long phx_globaltimer()
     return t;
 }
 
+// One compiled copy of the closest-hit search and of the physics step, called by the one-kernel
+// loop and by the wavefront kernels: with fast-math contraction decided per inlining context,
+// sharing the code is what keeps the two forms bit-identical.
+#ifndef PHX_STEP_OUTLINE_TRACE
+#define PHX_STEP_OUTLINE_TRACE 0
+#endif
+#ifndef PHX_STEP_OUTLINE_PROP
+#define PHX_STEP_OUTLINE_PROP 1
+#endif
+#if PHX_STEP_OUTLINE_TRACE
+#define PHX_STEPFN_T __device__ __noinline__
+#else
+#define PHX_STEPFN_T __device__ __forceinline__
+#endif
+#if PHX_STEP_OUTLINE_PROP
+#define PHX_STEPFN_P __device__ __noinline__
+#else
+#define PHX_STEPFN_P __device__ __forceinline__
+#endif
+
+template <bool POLISH>
+PHX_STEPFN_T PhxPRD phx_trace_step(const PhxScene S, const float3 o, const float3 d, const float tmin, const float tmax,
+                                 unsigned& status)
+{
+    PhxPRD prd;
+    phx_trace<POLISH>(S, o, d, tmin, tmax, prd, status);
+    return prd;
+}
+
+// the PRD normal is normalised here (CSGOptiX/CSGOptiX7.cu:491-498) as part of the shared step
+PHX_STEPFN_P int phx_propagate_step(PhxPhoton& p, curandStateXORWOW& rng, PhxPRD prd, const PhxProps P, unsigned& status)
+{
+    prd.normal = normalize(prd.normal);
+    return propagate<false>(p, rng, prd, P, status, nullptr);
+}
+
 struct PhxLane {
     PhxPhoton p;
     curandStateXORWOW rng;
@@ -140,17 +176,30 @@ PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status, PhxS
     if (!(L.bounce < A.C.max_bounce && L.p.time < A.C.max_time)) return true;
     const float tmin = (L.p.obf & A.C.eps0_mask) ? A.C.tmin0 : A.C.tmin;
     PhxPRD prd;
-    phx_trace<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
+    if (ADJ) phx_trace<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
+    else prd = phx_trace_step<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, status);
     if (prd.boundary() == 0xffffu) return true;
-    prd.normal = normalize(prd.normal);
-    const int command = propagate<ADJ>(L.p, L.rng, prd, A.P, status, sc);
+    int command;
+    if (ADJ) {
+        prd.normal = normalize(prd.normal);
+        command = propagate<ADJ>(L.p, L.rng, prd, A.P, status, sc);
+    } else {
+        command = phx_propagate_step(L.p, L.rng, prd, A.P, status);
+    }
     L.bounce++;
     seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
     return command == PHX_BREAK;
 }
 
+// Minimum resident warps per SM asked of the compiler (caps registers per thread); 0 leaves the
+// register count to the compiler.
+#ifndef PHX_PERSIST_MIN_WARPS
+#define PHX_PERSIST_MIN_WARPS 0
+#endif
+#define PHX_PERSIST_MINB(BLOCK) ((PHX_PERSIST_MIN_WARPS * 32 / (BLOCK)) > 0 ? (PHX_PERSIST_MIN_WARPS * 32 / (BLOCK)) : 1)
+
 template <bool POLISH, int BLOCK, bool ADJ = false>
-__global__ void __launch_bounds__(BLOCK) k_sim_persistent(PersistArgs A)
+__global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persistent(PersistArgs A)
 {
     PhxScore score;
     if (ADJ) {

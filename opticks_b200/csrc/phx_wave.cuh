@@ -1,0 +1,211 @@
+// phx_wave.cuh : wavefront form of the photon loop — closest-hit search and physics as separate
+// kernels over a pool of in-flight paths held in HBM.
+//
+// The one-kernel loop (phx_persist.cuh) keeps every path in registers, so the whole bounce —
+// traversal, CSG, generation, propagate, bookkeeping — is compiled as one function whose register
+// count (about 200) leaves ten warps per SM to hide the latency of the traversal's dependent
+// loads.  Here a round is two launches:
+//   k_wave_trace  reads ray origin/direction of every live path, runs phx_trace and writes the PRD
+//                 (a lean kernel: 128 registers, 16 warps per SM)
+//   k_wave_shade  reads the path and its PRD, runs propagate / seq nibble / finish exactly as the
+//                 one-kernel loop does, refills finished slots with new photons from the queue
+//                 (generation) and appends live slots to the next round's list
+// Path state is 128 B per slot (sphoton, the XORWOW words, bounce, event, seqhis/seqbnd) plus a
+// 32 B PRD; the extra HBM traffic is about 0.4 KB per bounce against microseconds of traversal.
+// Every photon consumes its random numbers in the same order as in the one-kernel loop, so
+// photons, seq and hits are bit-identical to it.
+//
+// The host drives rounds until the live count reaches zero (read back every few rounds); the
+// number of rounds is bounded by (N / pool + 1) * (max_bounce + 1).
+#pragma once
+#include "phx_persist.cuh"
+
+struct PhxWaveSlot {          // 128 B
+    float4 q0, q1, q2, q3;    // sphoton
+    uint4 ra;                 // xorwow d, v0, v1, v2
+    uint4 rb;                 // xorwow v3, v4, bounce, event
+    ulonglong2 his, bnd;      // seqhis[2], seqbnd[2]
+};
+
+struct PhxWavePrd {           // 32 B
+    float4 nd;                // normal.xyz, distance
+    uint4 lgi;                // lposcost bits, gp_bd, ii_id, 0
+};
+
+struct WaveArgs {
+    PersistArgs A;            // scene, physics, gensteps, outputs, queue, status
+    PhxWaveSlot* slot;
+    PhxWavePrd* prd;
+    long long* sidx;          // photon index per slot
+    const uint32_t* act_in;   // live slots of this round
+    uint32_t* act_out;        // live slots of the next round
+    const unsigned* n_in;
+    unsigned* n_out;
+    long long pool;           // slots (init only)
+};
+
+PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L)
+{
+    PhxWaveSlot* o = W.slot + s;
+    const PhxPhoton& p = L.p;
+    o->q0 = make_float4(p.pos.x, p.pos.y, p.pos.z, p.time);
+    o->q1 = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float(p.hitcount_iindex));
+    o->q2 = make_float4(p.pol.x, p.pol.y, p.pol.z, p.wavelength);
+    o->q3 = make_float4(__uint_as_float(p.obf), __uint_as_float(p.identity), __uint_as_float(p.index), __uint_as_float(p.flagmask));
+    o->ra = make_uint4(L.rng.d, L.rng.v[0], L.rng.v[1], L.rng.v[2]);
+    o->rb = make_uint4(L.rng.v[3], L.rng.v[4], (unsigned)L.bounce, (unsigned)L.ev);
+    o->his = make_ulonglong2(L.seqhis[0], L.seqhis[1]);
+    o->bnd = make_ulonglong2(L.seqbnd[0], L.seqbnd[1]);
+    W.sidx[s] = L.idx;
+}
+
+PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
+{
+    const PhxWaveSlot* o = W.slot + s;
+    const float4 q0 = o->q0, q1 = o->q1, q2 = o->q2, q3 = o->q3;
+    PhxPhoton& p = L.p;
+    p.pos = make_float3(q0.x, q0.y, q0.z); p.time = q0.w;
+    p.mom = make_float3(q1.x, q1.y, q1.z); p.hitcount_iindex = __float_as_uint(q1.w);
+    p.pol = make_float3(q2.x, q2.y, q2.z); p.wavelength = q2.w;
+    p.obf = __float_as_uint(q3.x); p.identity = __float_as_uint(q3.y);
+    p.index = __float_as_uint(q3.z); p.flagmask = __float_as_uint(q3.w);
+    const uint4 ra = o->ra, rb = o->rb;
+    L.rng.d = ra.x; L.rng.v[0] = ra.y; L.rng.v[1] = ra.z; L.rng.v[2] = ra.w;
+    L.rng.v[3] = rb.x; L.rng.v[4] = rb.y;
+    L.rng.boxmuller_flag = 0; L.rng.boxmuller_flag_double = 0;
+    L.rng.boxmuller_extra = 0.f; L.rng.boxmuller_extra_double = 0.0;
+    L.bounce = (int)rb.z; L.ev = (int)rb.w;
+    const ulonglong2 h = o->his, b = o->bnd;
+    L.seqhis[0] = h.x; L.seqhis[1] = h.y; L.seqbnd[0] = b.x; L.seqbnd[1] = b.y;
+    L.idx = W.sidx[s];
+}
+
+// a path may take another bounce (the loop condition of CSGOptiX/CSGOptiX7.cu:477)
+PHX_D bool wave_can_trace(const PhxLane& L, const PersistArgs& A)
+{
+    return L.bounce < A.C.max_bounce && L.p.time < A.C.max_time;
+}
+
+// warp-aggregated append of slot s to the next round's list
+PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(FULL, keep);
+    if (!m) return;
+    const unsigned leader = __ffs(m) - 1u;
+    unsigned base = 0u;
+    if (lane == leader) base = atomicAdd(W.n_out, (unsigned)__popc(m));
+    base = __shfl_sync(FULL, base, leader);
+    if (keep) W.act_out[base + __popc(m & ((1u << lane) - 1u))] = s;
+}
+
+// Lanes in `need` take new photons from the queue until each has a path that can be traced
+// (photons that cannot take a first bounce are finished at once) or the queue is empty.
+// Returns true in the lanes that hold a live path.  Warp-collective.
+template <bool POLISH>
+PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    bool live = false;
+    for (int guard = 0; guard < 64; guard++) {
+        const unsigned m = __ballot_sync(FULL, need);
+        if (!m) break;
+        unsigned long long base = 0ull;
+        if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(A.queue, (unsigned long long)__popc(m));
+        base = __shfl_sync(FULL, base, __ffs(m) - 1);
+        if ((long long)base >= A.N) break;                  // queue exhausted for every lane
+        if (need) {
+            const long long idx = (long long)base + __popc(m & ((1u << lane) - 1u));
+            if (idx >= A.N) {
+                need = false;
+            } else {
+                persist_start<POLISH, false>(L, A, idx, status, nullptr);
+                if (wave_can_trace(L, A)) { live = true; need = false; }
+                else persist_finish<POLISH, false>(L, A, nullptr);
+            }
+        }
+    }
+    return live;
+}
+
+// fill the pool: every slot takes photons until it holds a live path or the queue is empty
+template <bool POLISH>
+__global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
+{
+    unsigned status = 0;
+    PhxLane L;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < W.pool; base += stride) {
+        const long long s = base + (threadIdx.x & 31);
+        const bool live = wave_refill<POLISH>(L, W.A, s < W.pool, status);
+        if (live) wave_store(W, (uint32_t)s, L);
+        wave_append(W, live, (uint32_t)s);
+    }
+    if (status) atomicOr(W.A.status, status);
+}
+
+// closest hit of every live path (CSGOptiX/CSGOptiX7.cu:477-490: tmin by the last flag, optixTrace)
+template <bool POLISH>
+__global__ void __launch_bounds__(128, 4) k_wave_trace(WaveArgs W)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) *W.n_out = 0u;   // the shade launch after this one appends
+    const unsigned n = *W.n_in;
+    unsigned status = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)n; i += stride) {
+        const uint32_t s = W.act_in[i];
+        const PhxWaveSlot* o = W.slot + s;
+        const float4 q0 = o->q0, q1 = o->q1;
+        const unsigned obf = __float_as_uint(o->q3.x);
+        const float tmin = (obf & W.A.C.eps0_mask) ? W.A.C.tmin0 : W.A.C.tmin;
+        const PhxPRD prd = phx_trace_step<POLISH>(W.A.S, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z), tmin,
+                                                  W.A.C.tmax, status);
+        W.prd[s].nd = make_float4(prd.normal.x, prd.normal.y, prd.normal.z, prd.distance);
+        W.prd[s].lgi = make_uint4(__float_as_uint(prd.lposcost), prd.gp_bd, prd.ii_id, 0u);
+    }
+    if (status) atomicOr(W.A.status, status);
+}
+
+// physics of every live path after its closest hit (CSGOptiX/CSGOptiX7.cu:491-509), finishing
+// and refilling slots; live slots go to the next round's list
+template <bool POLISH>
+__global__ void __launch_bounds__(128) k_wave_shade(WaveArgs W)
+{
+    const unsigned n = *W.n_in;
+    unsigned status = 0;
+    PhxLane L;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
+        const long long i = base + (threadIdx.x & 31);
+        const bool valid = i < (long long)n;
+        uint32_t s = 0u;
+        bool live = false;
+        if (valid) {
+            s = W.act_in[i];
+            wave_load(W, s, L);
+            const float4 nd = W.prd[s].nd;
+            const uint4 lgi = W.prd[s].lgi;
+            PhxPRD prd;
+            prd.normal = make_float3(nd.x, nd.y, nd.z);
+            prd.distance = nd.w;
+            prd.lposcost = __uint_as_float(lgi.x);
+            prd.gp_bd = lgi.y;
+            prd.ii_id = lgi.z;
+            bool done = true;
+            if (prd.boundary() != 0xffffu) {
+                const int command = phx_propagate_step(L.p, L.rng, prd, W.A.P, status);
+                L.bounce++;
+                seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
+                done = command == PHX_BREAK || !wave_can_trace(L, W.A);
+            }
+            if (done) persist_finish<POLISH, false>(L, W.A, nullptr);
+            live = !done;
+        }
+        if (wave_refill<POLISH>(L, W.A, valid && !live, status)) live = true;
+        if (live) wave_store(W, s, L);
+        wave_append(W, live, s);
+    }
+    if (status) atomicOr(W.A.status, status);
+}

@@ -201,6 +201,12 @@ class Engine:
                                                int(num_per_photon), _ptr(out)), "phx_rng_sequence")
         return out
 
+    def last_call_stats(self) -> dict:
+        """kernel launches and wavefront rounds of the last simulate call"""
+        k, r = C.c_int64(0), C.c_int64(0)
+        _lib.check(_lib.lib().phx_last_call_stats(self._h, C.byref(k), C.byref(r)), "phx_last_call_stats")
+        return {"kernel_launches": int(k.value), "wave_rounds": int(r.value)}
+
     # ------------------------------------------------------------------ hit merging
     def merge_hits(self, records: np.ndarray, select_flagmask: int = 0xFFFFFFFF, time_window: float = 1.0) -> np.ndarray:
         """SPM::merge_partial_select on host arrays: sphoton (n,4,4) or sphotonlite (n,4) records in,
