@@ -145,6 +145,8 @@ int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, doub
     out.nodes.clear();
     out.leaves.clear();
     out.globals.clear();
+    out.leaf_sphere.clear();
+    out.global_sphere.clear();
     out.cull[0] = out.cull[1] = out.cull[2] = out.cull[3] = 0.f;
     std::vector<Box> all(n_all);
     Box scene;
@@ -169,7 +171,11 @@ int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, doub
         std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) { return all[a].area() > all[b].area(); });
         if ((int)cand.size() > max_global) cand.resize(std::max(0, max_global));
         for (int i : cand) is_global[i] = 1;
-        for (int i = 0; i < n_all; i++) if (is_global[i]) out.globals.push_back(in[i].leaf);
+        for (int i = 0; i < n_all; i++)
+            if (is_global[i]) {
+                out.globals.push_back(in[i].leaf);
+                out.global_sphere.insert(out.global_sphere.end(), in[i].sphere, in[i].sphere + 4);
+            }
     }
     std::vector<int> keep;
     for (int i = 0; i < n_all; i++) if (!is_global[i]) keep.push_back(i);
@@ -210,7 +216,11 @@ int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, doub
     int root2 = B.build(0, n, 0);
     // reorder leaves
     out.leaves.resize(n);
-    for (int i = 0; i < n; i++) out.leaves[i] = in[keep[B.idx[i]]].leaf;
+    out.leaf_sphere.resize(4 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        out.leaves[i] = in[keep[B.idx[i]]].leaf;
+        for (int k = 0; k < 4; k++) out.leaf_sphere[4 * (size_t)i + k] = in[keep[B.idx[i]]].sphere[k];
+    }
 
     // collapse to 4-wide. Each BVH2 inner node becomes one BVH4 node whose children are
     // the up-to-4 descendants obtained by opening the largest inner child.

@@ -6,6 +6,7 @@
 struct PhxLeafInput {
     float bbox[6];      // prim box in the instance (object) frame : mn.xyz, mx.xyz
     float xform[16];    // instance transform, row-vector convention (rows q0..q3), object -> world
+    float sphere[4];    // world-space bounding sphere of the leaf: centre xyz, radius
     phx_leaf leaf;
 };
 
@@ -13,6 +14,7 @@ struct PhxBvh4Result {
     std::vector<phx_bvh4_node> nodes;
     std::vector<phx_leaf> leaves;   // reordered to match the leaf ranges in nodes
     std::vector<phx_leaf> globals;  // leaves tested by every ray before the traversal (input order)
+    std::vector<float> leaf_sphere, global_sphere;   // 4 floats per leaf, same orders
     float cull[4] = { 0.f, 0.f, 0.f, 0.f };   // empty ball of the BVH leaves: centre xyz, radius^2 (0: none)
     int leaf_count = 0;
     int max_depth = 0;

@@ -92,6 +92,7 @@ struct phx_engine {
     DevBuf<float4> node, itra, plan, inst_inv;
     DevBuf<phx_bvh4_node> bvh;
     DevBuf<phx_leaf> leaves, globals;
+    DevBuf<float4> leaf_sph, global_sph;   // world bounding sphere per leaf (centre, radius)
     int num_global = 0;
     float cull[4] = { 0.f, 0.f, 0.f, 0.f };
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
@@ -148,6 +149,8 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.csg.itra = e->itra.p;
     (void)polish;
     S.globals = e->globals.p;
+    S.leaf_sph = e->leaf_sph.p;
+    S.global_sph = e->global_sph.p;
     S.num_global = e->num_global;
     S.cull = make_float4(e->cull[0], e->cull[1], e->cull[2], e->cull[3]);
     S.bvh_empty = e->num_leaf == 0;
@@ -435,6 +438,122 @@ static bool invert_affine(const float* q, float* out)
     return true;
 }
 
+// ------------------------------------------------------------------ leaf bounding spheres
+// A conservative sphere around each (instance, prim) leaf lets the traversal reject a leaf with
+// one ray-sphere test before it loads the instance transform and walks the CSG tree.  The prim's
+// sphere is the smaller of the sphere around its box and one composed over its CSG tree (leaf
+// spheres, enclosing sphere for union, the smaller operand for intersection, A for A - B;
+// complemented leaves are unbounded).
+struct PhxSph { double c[3]; double r; };
+
+static const double PHX_SPH_INF = 1e300;
+
+static PhxSph sph_union(const PhxSph& a, const PhxSph& b)
+{
+    if (a.r >= PHX_SPH_INF || b.r >= PHX_SPH_INF) return { { 0, 0, 0 }, PHX_SPH_INF };
+    double dv[3] = { b.c[0] - a.c[0], b.c[1] - a.c[1], b.c[2] - a.c[2] };
+    const double d = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (d + b.r <= a.r) return a;
+    if (d + a.r <= b.r) return b;
+    const double r = 0.5 * (d + a.r + b.r);
+    PhxSph s;
+    for (int k = 0; k < 3; k++) s.c[k] = a.c[k] + dv[k] / d * (r - a.r);
+    s.r = r;
+    return s;
+}
+
+// largest stretch of the 3x3 linear part of a row-vector affine matrix (power iteration on M^T M)
+static double max_scale(const double* m)
+{
+    double v[3] = { 0.577, 0.577, 0.577 }, lam = 0.0;
+    for (int it = 0; it < 64; it++) {
+        double w[3], u[3];
+        for (int c = 0; c < 3; c++) w[c] = v[0] * m[0 * 4 + c] + v[1] * m[1 * 4 + c] + v[2] * m[2 * 4 + c];
+        for (int r = 0; r < 3; r++) u[r] = m[r * 4 + 0] * w[0] + m[r * 4 + 1] * w[1] + m[r * 4 + 2] * w[2];
+        const double n = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (!(n > 0.0)) return 0.0;
+        lam = n;
+        for (int k = 0; k < 3; k++) v[k] = u[k] / n;
+    }
+    return std::sqrt(lam) * (1.0 + 1e-9);
+}
+
+static PhxSph sph_transform(const PhxSph& s, const double* m)
+{
+    if (s.r >= PHX_SPH_INF) return s;
+    PhxSph o;
+    for (int c = 0; c < 3; c++) o.c[c] = s.c[0] * m[0 * 4 + c] + s.c[1] * m[1 * 4 + c] + s.c[2] * m[2 * 4 + c] + m[3 * 4 + c];
+    o.r = s.r * max_scale(m);
+    return o;
+}
+
+// sphere of node i (level order) of the complete tree rooted at node offset no, in the prim frame
+static PhxSph node_sphere(const phx_geometry* geo, int no, int i, int num)
+{
+    const PhxSph inf = { { 0, 0, 0 }, PHX_SPH_INF };
+    if (i >= num || no + i >= geo->num_node) return inf;
+    const float* q = geo->node + 16 * (size_t)(no + i);
+    uint32_t tc, tw;
+    memcpy(&tc, q + 14, 4);
+    memcpy(&tw, q + 15, 4);
+    if (tc == PHX_CSG_UNION || tc == PHX_CSG_INTERSECTION || tc == PHX_CSG_DIFFERENCE) {
+        const PhxSph a = node_sphere(geo, no, 2 * i + 1, num), b = node_sphere(geo, no, 2 * i + 2, num);
+        if (tc == PHX_CSG_UNION) return sph_union(a, b);
+        if (tc == PHX_CSG_INTERSECTION) return a.r <= b.r ? a : b;
+        return a;
+    }
+    if (tw & 0x80000000u) return inf;   // complemented leaf
+    PhxSph s = inf;
+    switch (tc) {
+        case PHX_CSG_SPHERE:
+        case PHX_CSG_ZSPHERE:
+            s = { { q[0], q[1], q[2] }, std::fabs((double)q[3]) };
+            break;
+        case PHX_CSG_CYLINDER: {
+            const double r = q[3], z1 = q[4], z2 = q[5];
+            s = { { q[0], q[1], 0.5 * (z1 + z2) }, std::sqrt(r * r + 0.25 * (z2 - z1) * (z2 - z1)) };
+            break;
+        }
+        case PHX_CSG_BOX3:
+            s = { { 0, 0, 0 }, 0.5 * std::sqrt((double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2]) };
+            break;
+        case PHX_CSG_TORUS:
+            s = { { 0, 0, 0 }, std::fabs((double)q[2]) + std::fabs((double)q[1]) };
+            break;
+        default:
+            return inf;
+    }
+    const uint32_t g = tw & 0x7fffffffu;
+    if (g > 0) {
+        if ((int)g > geo->num_itra || !geo->itra) return inf;
+        float fwd[16];
+        if (!invert_affine(geo->itra + 16 * (size_t)(g - 1), fwd)) return inf;
+        double m[16];
+        for (int k = 0; k < 16; k++) m[k] = fwd[k];
+        s = sph_transform(s, m);
+    }
+    return s;
+}
+
+// prim-frame sphere: the smaller of the box sphere and the tree sphere
+static PhxSph prim_sphere(const phx_geometry* geo, int p)
+{
+    const float* pr = geo->prim + 16 * (size_t)p;
+    int32_t nn, no;
+    memcpy(&nn, pr + 0, 4);
+    memcpy(&no, pr + 1, 4);
+    PhxSph b;
+    double h2 = 0.0;
+    for (int k = 0; k < 3; k++) {
+        b.c[k] = 0.5 * ((double)pr[8 + k] + (double)pr[11 + k]);
+        const double h = 0.5 * ((double)pr[11 + k] - (double)pr[8 + k]);
+        h2 += h * h;
+    }
+    b.r = std::sqrt(h2);
+    const PhxSph t = node_sphere(geo, no, 0, std::max(1, nn));
+    return t.r < b.r ? t : b;
+}
+
 static int make_texture_f4(cudaArray_t& arr, cudaTextureObject_t& tex, const float* data, int width, int height)
 {
     cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
@@ -546,7 +665,7 @@ int phx_destroy(phx_engine* e)
     if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
     e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release();
-    e->bvh.release(); e->leaves.release(); e->globals.release(); e->optical.release(); e->rng.release();
+    e->bvh.release(); e->leaves.release(); e->globals.release(); e->leaf_sph.release(); e->global_sph.release(); e->optical.release(); e->rng.release();
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
@@ -600,6 +719,8 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     }
     std::vector<float> inv((size_t)std::max(1, geo->num_inst) * 16, 0.f);
     std::vector<PhxLeafInput> leaves;
+    std::vector<PhxSph> psph((size_t)std::max(1, geo->num_prim));
+    for (int p = 0; p < geo->num_prim; p++) psph[p] = prim_sphere(geo, p);
     for (int i = 0; i < geo->num_inst; i++) {
         const float* q = geo->inst + 16 * i;
         float m[16];
@@ -619,6 +740,16 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
             L.bbox[0] = pr[8]; L.bbox[1] = pr[9]; L.bbox[2] = pr[10];
             L.bbox[3] = pr[11]; L.bbox[4] = pr[12]; L.bbox[5] = pr[13];
             memcpy(L.xform, m, sizeof(m));
+            {
+                double md[16];
+                for (int k = 0; k < 16; k++) md[k] = m[k];
+                const PhxSph w = sph_transform(psph[p], md);
+                const double cn = std::sqrt(w.c[0] * w.c[0] + w.c[1] * w.c[1] + w.c[2] * w.c[2]);
+                // pad: relative, plus absolute for FP32 rays at these coordinates (never excludes a hit)
+                const double r = w.r >= PHX_SPH_INF ? 3e38 : w.r * (1.0 + 1e-4) + 1e-5 * (cn + w.r) + 0.5;
+                L.sphere[0] = (float)w.c[0]; L.sphere[1] = (float)w.c[1]; L.sphere[2] = (float)w.c[2];
+                L.sphere[3] = (float)std::min(r, 3e38);
+            }
             int32_t gpi;
             memcpy(&gpi, pr + 15, 4);
             const int no = e->prim_node_offset[p];
@@ -640,6 +771,10 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     if (!bv.nodes.empty()) PHX_TRYCU(cudaMemcpy(e->bvh.p, bv.nodes.data(), bv.nodes.size() * sizeof(phx_bvh4_node), cudaMemcpyHostToDevice));
     PHX_TRYCU(e->leaves.ensure(std::max<size_t>(1, bv.leaves.size())));
     if (!bv.leaves.empty()) PHX_TRYCU(cudaMemcpy(e->leaves.p, bv.leaves.data(), bv.leaves.size() * sizeof(phx_leaf), cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->leaf_sph.ensure(std::max<size_t>(1, bv.leaf_sphere.size() / 4)));
+    if (!bv.leaf_sphere.empty()) PHX_TRYCU(cudaMemcpy(e->leaf_sph.p, bv.leaf_sphere.data(), bv.leaf_sphere.size() * sizeof(float), cudaMemcpyHostToDevice));
+    PHX_TRYCU(e->global_sph.ensure(std::max<size_t>(1, bv.global_sphere.size() / 4)));
+    if (!bv.global_sphere.empty()) PHX_TRYCU(cudaMemcpy(e->global_sph.p, bv.global_sphere.data(), bv.global_sphere.size() * sizeof(float), cudaMemcpyHostToDevice));
     e->num_global = (int)bv.globals.size();
     memcpy(e->cull, bv.cull, sizeof(e->cull));
     PHX_TRYCU(e->globals.ensure(std::max<size_t>(1, bv.globals.size())));

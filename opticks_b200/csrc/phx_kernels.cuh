@@ -12,6 +12,8 @@ struct PhxScene {
     const phx_bvh4_node* bvh;   // root at 0
     const phx_leaf* leaves;
     const phx_leaf* globals;    // leaves tested first by every ray (boxes spanning much of the scene)
+    const float4* leaf_sph;     // world bounding sphere (centre, radius) of each hierarchy leaf
+    const float4* global_sph;   // and of each global leaf
     const float4* inst_inv;     // (num_inst*4) rows of the world->object 4x4 (row-vector convention)
     PhxCsgCtx csg;
     float4 cull;                // ball no hierarchy leaf reaches: centre xyz, radius^2 (0: none)
@@ -29,10 +31,24 @@ struct PhxBest {
 
 // IS program of CSGOptiX/CSGOptiX7.cu:896-967 for one (instance, prim) leaf: object-frame
 // intersect_prim, keep the closest hit and its lposcost
+// Can the ray segment (tmin, tmax) meet the ball (centre, radius)?  The radius is padded on the
+// host beyond FP32 error, so a false answer never hides a hit of the leaf inside the ball.
+PHX_D bool phx_ball_overlaps(const float4 b, const float3& o, const float3& d, float tmin, float tmax)
+{
+    const float3 oc = make_float3(b.x - o.x, b.y - o.y, b.z - o.z);
+    const float dd = dot(d, d);
+    const float tc = dot(oc, d) / dd;
+    const float3 q = oc - tc * d;
+    if (dot(q, q) > b.w * b.w) return false;
+    const float h = b.w * rsqrtf(dd);
+    return tc + h >= tmin && tc - h <= tmax;
+}
+
 template <bool POLISH>
-PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float3& o, const float3& d, float tmin, PhxBest& B,
+PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, const float3& o, const float3& d, float tmin, PhxBest& B,
                          unsigned& status)
 {
+    if (!phx_ball_overlaps(ball, o, d, tmin, B.t)) return;
     const float4* q = S.inst_inv + 4 * L.x;
     float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
     const float3 lo = xform_row(m, o, 1.f);
@@ -69,7 +85,7 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
     B.isect = make_float4(0.f, 0.f, 0.f, 0.f);
     B.lposcost = 0.f;
     for (int g = 0; g < S.num_global; g++)
-        phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), o, d, tmin, B, status);
+        phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B, status);
     bool traverse = !S.bvh_empty;
     if (traverse && S.cull.w > 0.f) {
         const float3 c = make_float3(S.cull.x, S.cull.y, S.cull.z);
@@ -131,7 +147,8 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                 const int first = enc >> 3;
                 const int count = (enc & 7) + 1;
                 for (int li = first; li < first + count; li++)
-                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), o, d, tmin, B, status);
+                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin,
+                                          B, status);
             }
 #pragma unroll
             for (int k = 3; k >= 0; k--) {
