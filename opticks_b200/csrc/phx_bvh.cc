@@ -12,6 +12,19 @@
 #include <cstring>
 #include <limits>
 
+// SAH build parameters: centroid bins per axis, largest leaf range a node may keep, and the cost of
+// visiting a node relative to one leaf test (0: split whenever the SAH sum does not grow).  On
+// the 17,612-PMT detector the tree splits down to single leaves for any of these settings.
+#ifndef PHX_BVH_BINS
+#define PHX_BVH_BINS 16
+#endif
+#ifndef PHX_BVH_MAX_LEAF
+#define PHX_BVH_MAX_LEAF 4
+#endif
+#ifndef PHX_BVH_TRAV_COST
+#define PHX_BVH_TRAV_COST 0.0
+#endif
+
 namespace {
 
 struct Box {
@@ -39,7 +52,7 @@ struct Builder {
     std::vector<double> cent;   // 3 per leaf
     std::vector<int> idx;
     std::vector<Node2> nodes;
-    int max_leaf = 4;
+    int max_leaf = PHX_BVH_MAX_LEAF;
 
     int build(int first, int count, int depth)
     {
@@ -51,7 +64,7 @@ struct Builder {
         // centroid bounds
         Box cb;
         for (int i = first; i < first + count; i++) cb.grow(&cent[3 * idx[i]]);
-        const int NB = 16;
+        const int NB = PHX_BVH_BINS;
         double best_cost = std::numeric_limits<double>::infinity();
         int best_axis = -1, best_split = -1;
         for (int ax = 0; ax < 3; ax++) {
@@ -77,6 +90,7 @@ struct Builder {
             }
         }
         double leaf_cost = nodes[me].box.area() * count;
+        best_cost += PHX_BVH_TRAV_COST * nodes[me].box.area();
         if (best_axis < 0 || (count <= max_leaf && best_cost >= leaf_cost)) {
             if (count <= max_leaf || best_axis < 0) {
                 if (count > max_leaf) {

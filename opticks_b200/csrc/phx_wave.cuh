@@ -6,7 +6,7 @@
 // count (about 200) leaves ten warps per SM to hide the latency of the traversal's dependent
 // loads.  Here a round is two launches:
 //   k_wave_trace  reads ray origin/direction of every live path, runs phx_trace and writes the PRD
-//                 (a lean kernel: 128 registers, 16 warps per SM)
+//                 (a lean kernel: 168 registers, 12 warps per SM, against about 200 and 10)
 //   k_wave_shade  reads the path and its PRD, runs propagate / seq nibble / finish exactly as the
 //                 one-kernel loop does, refills finished slots with new photons from the queue
 //                 (generation) and appends live slots to the next round's list
@@ -147,8 +147,14 @@ __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
 }
 
 // closest hit of every live path (CSGOptiX/CSGOptiX7.cu:477-490: tmin by the last flag, optixTrace)
+// resident 128-thread blocks per SM asked of the compiler for the closest-hit kernel (caps its
+// registers: 3 -> 168 registers, 12 warps per SM, no spills; 4 -> 128 with spills, measured slower)
+#ifndef PHX_WAVE_TRACE_MINB
+#define PHX_WAVE_TRACE_MINB 3
+#endif
+
 template <bool POLISH>
-__global__ void __launch_bounds__(128, 4) k_wave_trace(WaveArgs W)
+__global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArgs W)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) *W.n_out = 0u;   // the shade launch after this one appends
     const unsigned n = *W.n_in;
