@@ -7,6 +7,10 @@
 #include "phx_physics.cuh"
 
 #define PHX_BVH_STACK 48
+// leaf steps are taken when leaf-ready lanes x this weight >= node-ready lanes (or no node work is left)
+#ifndef PHX_TRACE_LEAF_WEIGHT
+#define PHX_TRACE_LEAF_WEIGHT 1
+#endif
 
 struct PhxScene {
     const phx_bvh4_node* bvh;   // root at 0
@@ -103,10 +107,30 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
         float stt[PHX_BVH_STACK];
         int sp = 0;
         stk[sp] = 0; stt[sp] = tmin; sp++;
-        while (sp > 0) {
+        // Each step the lanes of the warp that traverse together vote: either the lanes whose next
+        // entry is an inner node visit it, or the lanes whose next entry is a leaf range test it.
+        // Every lane still takes its own entries in its own near-first order; the vote only
+        // gathers the expensive leaf tests into steps where many lanes run them.
+        const unsigned mask = __activemask();
+        for (;;) {
+            while (sp > 0 && stt[sp - 1] > B.t) sp--;
+            const bool leaf_top = sp > 0 && stk[sp - 1] < 0;
+            const unsigned want_leaf = __ballot_sync(mask, leaf_top);
+            const unsigned want_node = __ballot_sync(mask, sp > 0 && !leaf_top);
+            if (!(want_leaf | want_node)) break;
+            const bool leaf_step = want_node == 0u || __popc(want_leaf) * PHX_TRACE_LEAF_WEIGHT >= __popc(want_node);
+            if (sp == 0 || leaf_top != leaf_step) continue;
             sp--;
             const int ni = stk[sp];
-            if (stt[sp] > B.t) continue;
+            if (leaf_step) {
+                const int enc = -ni - 1;
+                const int first = enc >> 3;
+                const int count = (enc & 7) + 1;
+                for (int li = first; li < first + count; li++)
+                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin,
+                                          B, status);
+                continue;
+            }
             const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
             const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
             const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
@@ -126,9 +150,9 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                 const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), B.t));
                 // slab arithmetic slack: boxes are padded on the host, and a relative slack here
                 tn[c] = tnear;
-                if (tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
+                if (cha[c] != 0 && tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
             }
-            // leaves first (closest box first), then push inner nodes far-to-near
+            // push the hit children (inner nodes and leaf ranges) far-to-near: the nearest is next
             int order[4] = { 0, 1, 2, 3 };
 #pragma unroll
             for (int i = 1; i < 4; i++)
@@ -137,28 +161,11 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                     if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
                 }
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int c = order[k];
-                if (!(hitmask & (1 << c))) continue;
-                const int child = cha[c];
-                if (child >= 0) continue;
-                if (tn[c] > B.t) continue;
-                const int enc = -child - 1;
-                const int first = enc >> 3;
-                const int count = (enc & 7) + 1;
-                for (int li = first; li < first + count; li++)
-                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin,
-                                          B, status);
-            }
-#pragma unroll
             for (int k = 3; k >= 0; k--) {
                 const int c = order[k];
                 if (!(hitmask & (1 << c))) continue;
-                const int child = cha[c];
-                if (child <= 0) continue;
-                if (tn[c] > B.t) continue;
                 if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
-                stk[sp] = child; stt[sp] = tn[c]; sp++;
+                stk[sp] = cha[c]; stt[sp] = tn[c]; sp++;
             }
         }
     }
