@@ -6,12 +6,15 @@ Headline (`value`): photons/s of the plain form on the full synthetic detector â
 in HBM, device time from CUDA events on the launch stream.
 
 Also on the line:
-  e2e          photons/s through the host API phx_simulate (H2D gensteps, D2H photon+seq+hits
-               into pinned buffers), timed per step
-  roofline     k_sim_persistent: 120.1 algorithmic bytes/photon / its duration vs measured HBM
+  e2e          photons/s through the reference-facing host call (CSGOptiXService.simulate:
+               H2D gensteps, D2H hits into pinned buffers), timed per step; e2e_full also returns
+               every photon and its seq (about 1 GB per step over PCIe)
+  roofline     the simulate launch sequence: 120.1 algorithmic bytes/photon / its duration vs
+               measured HBM (the path is latency-bound ray tracing, far from the HBM roof)
   cpu_baseline the CPU oracle (port of the reference's path) on a bounded sample, all threads
-  forms        batched (4,096 lognormal events in one persistent launch, CUDA graph, autotuned)
-               vs the per-event launch loop with per-event latency p50/p99; the CSG scan
+  forms        batched (4,096 lognormal events in one call; the one-kernel persistent form
+               autotuned and replayed as a CUDA graph, and the wavefront form) vs the per-event
+               loop, with per-event latency p50/p99; the adjoint (C5) cost and FD table; the CSG scan
                (16,777,216 rays vs the 15-node tree with torus, rays/s, FP64 distance error)
 
 --impl reference: the reference's CPU implementation of the path on the host cores.  Its qsim
@@ -465,21 +468,26 @@ def main():
     peak, peak_kind = load_peaks()
     achieved = N * bytes_per_photon / (k_ms / 1e3) / 1e9
 
-    # end to end through the host API with pinned buffers
+    # end to end through the host API with pinned buffers.  e2e: the reference-facing service call
+    # (CSGOptiXService.simulate: gensteps in, hits out); e2e_full: photons + seq + hits returned
     ph_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
     sq_h = torch.empty((N, 2, 2), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
     ht_h = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
     gs_h = torch.from_numpy(gs).pin_memory().numpy()
-    times, d2h = [], []
-    for s in range(args.e2e_steps + 1):
-        t0 = time.perf_counter()
-        out = eng.simulate_into(gs_h, base_event + 300 + s, ph_h, sq_h, ht_h)
-        dt = time.perf_counter() - t0
-        if s > 0:
-            times.append(dt)
-            d2h.append(N * 64 + N * 32 + out["num_hit"] * 64)
-    e2e = {"value": N / statistics.mean(times), "unit": METRIC, "h2d_bytes_per_step": int(gs.nbytes),
-           "d2h_bytes_per_step": int(statistics.mean(d2h)), "ms_per_step": 1e3 * statistics.mean(times)}
+
+    def host_run(full, ev0):
+        times, d2h = [], []
+        for s in range(args.e2e_steps + 1):
+            t0 = time.perf_counter()
+            out = eng.simulate_into(gs_h, ev0 + s, ph_h if full else None, sq_h if full else None, ht_h)
+            dt = time.perf_counter() - t0
+            if s > 0:
+                times.append(dt)
+                d2h.append((N * 96 if full else 0) + out["num_hit"] * 64)
+        return {"value": N / statistics.mean(times), "unit": METRIC, "h2d_bytes_per_step": int(gs.nbytes),
+                "d2h_bytes_per_step": int(statistics.mean(d2h)), "ms_per_step": 1e3 * statistics.mean(times)}
+    e2e = dict(host_run(False, base_event + 300), api="phx_simulate: host gensteps in, host hits out (CSGOptiXService.simulate)")
+    e2e_full = dict(host_run(True, base_event + 400), api="phx_simulate: host gensteps in, host photons + seq + hits out")
     eng.close()
     del photon, seq, hit
     torch.cuda.empty_cache()
@@ -511,7 +519,7 @@ def main():
                                         if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
                              "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},
-                "e2e": e2e, "clocks": clocks, "cpu_baseline": cpu, "forms": forms}
+                "e2e": e2e, "e2e_full": e2e_full, "clocks": clocks, "cpu_baseline": cpu, "forms": forms}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

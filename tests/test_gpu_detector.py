@@ -116,3 +116,25 @@ def test_cerenkov_matches_cpu_oracle(ck):
     print(f"cerenkov vs CPU oracle: seqhis match {m:.6f} close {fc:.6f}")
     assert m >= 0.995
     assert fc >= 0.995
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_pinned_outputs_equal_pageable(det, mode):
+    """phx_simulate writes photons and seq straight into pinned (device-mapped) host buffers while
+    the kernels run; the result equals the staged copy into pageable buffers"""
+    import torch
+    from opticks_b200 import engine as E
+    gs = det["gs"]
+    N = int(gs.view(np.int32)[:, 0, 3].sum())
+    eng = E.Engine(det["fd"].arrays(), det["phys"], E.default_config(max_photon=N, num_sensor=scenes.NUM_PMT, kernel_mode=mode))
+    ref = eng.simulate(gs, 4, sensor_hits=True)
+    ph = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
+    sq = torch.empty((N, 2, 2), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    ht = torch.empty((N, 4, 4), dtype=torch.float32, pin_memory=True).numpy()
+    ph.fill(7.0)
+    out = eng.simulate_into(gs, 4, ph, sq, ht)
+    eng.close()
+    assert out["status"] == 0 and out["num_hit"] == ref["num_hit"]
+    np.testing.assert_array_equal(ph.view(np.uint32), ref["photon"].view(np.uint32))
+    np.testing.assert_array_equal(sq, ref["seq"])
+    np.testing.assert_array_equal(ht[: out["num_hit"]].view(np.uint32), ref["hit"].view(np.uint32))
