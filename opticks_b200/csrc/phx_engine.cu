@@ -124,9 +124,10 @@ struct phx_engine {
     DevBuf<long long> ev_start;
     DevBuf<unsigned> ev_left;
     DevBuf<uint32_t> jump_pow, jump_tab;   // P_k = T^(skip 2^k) and per-call event jump matrices
+    DevBuf<uint32_t> ev_rng;               // per-call event-advanced XORWOW states (k_rng_event)
     cudaGraphExec_t batch_exec = nullptr;   // cached batched launch sequence (use_graph)
     PhxBatchCall batch_call;
-    const void* batch_bufs[11] = {};
+    const void* batch_bufs[12] = {};
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
     PhxMergeWs merge;
@@ -669,7 +670,7 @@ int phx_destroy(phx_engine* e)
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
-    e->jump_pow.release(); e->jump_tab.release();
+    e->jump_pow.release(); e->jump_tab.release(); e->ev_rng.release();
     e->merge.release();
     e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wcnt.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
@@ -877,6 +878,9 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // until no path is live.  The live count is read back every PHX_WAVE_ROUNDS rounds, so the call
 // synchronises the stream; it cannot be captured into a graph.
 #define PHX_WAVE_POOL (1LL << 21)
+// calls of at most this many photons get their event-advanced RNG states in one coherent pass
+// ahead of the loop (24 B per photon of scratch); larger ones advance each state as it starts
+#define PHX_EV_RNG_MAX (1LL << 26)
 #define PHX_WAVE_ROUNDS 4
 
 template <typename K>
@@ -994,10 +998,17 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         A.regroup = e->cfg.regroup;
         A.chunk = e->cfg.chunk;
         const bool wave = e->cfg.kernel_mode == 2 && wave_ok;
+        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX) {
+            PHX_CU(e->ev_rng.ensure((size_t)N * 6));
+            k_rng_event<<<(unsigned)std::min<long long>((N + 255) / 256, 148LL * 16), 256, 0, st>>>(A, e->ev_rng.p, N);
+            PHX_CU(cudaGetLastError());
+            A.ev_rng = e->ev_rng.p;
+            A.ev_rng_n = N;
+        }
         e->last_rounds = 0;
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
-        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (wave ? 1 + 2 * e->last_rounds : 1) + (want_hits ? 3 : 0);
+        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (A.ev_rng ? 1 : 0) + (wave ? 1 + 2 * e->last_rounds : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         const int B = PHX_SIM_BLOCK;
         if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
@@ -1216,6 +1227,12 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
         A.ev_done_ns = reinterpret_cast<unsigned long long*>(c.done);
         A.num_event = c.num_event;
     }
+    if (N > 0 && e->ev_rng.n >= (size_t)N * 6) {
+        k_rng_event<<<(unsigned)std::min<long long>((N + 255) / 256, 148LL * 16), 256, 0, st>>>(A, e->ev_rng.p, N);
+        PHX_CU(cudaGetLastError());
+        A.ev_rng = e->ev_rng.p;
+        A.ev_rng_n = N;
+    }
     if (N > 0) {
         int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st) : launch_persistent(e, A, c.block, st);
         if (rc) return rc;
@@ -1269,11 +1286,12 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
         PHX_CU(e->blocksum.ensure((size_t)std::max<long long>(1, (nword + 255) / 256)));
     }
     if (c.num_event > 0) PHX_CU(e->ev_left.ensure((size_t)c.num_event));
+    if (N > 0 && N <= PHX_EV_RNG_MAX) PHX_CU(e->ev_rng.ensure((size_t)N * 6));
     PHX_CU(e->jump_tab.ensure((size_t)std::max(1, c.G) * PHX_JUMP_MATW));
     if (e->cfg.use_graph && e->cfg.kernel_mode != 2) {
         // the captured graph bakes in every engine buffer pointer: reuse it only if none moved
-        const void* bufs[11] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
-                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p };
+        const void* bufs[12] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
+                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p, e->ev_rng.p };
         const bool reuse = e->batch_exec && e->batch_call == c && memcmp(bufs, e->batch_bufs, sizeof(bufs)) == 0;
         if (!reuse) {
             if (e->batch_exec) { cudaGraphExecDestroy(e->batch_exec); e->batch_exec = nullptr; }

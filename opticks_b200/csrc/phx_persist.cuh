@@ -31,6 +31,8 @@ struct PersistArgs {
     const uint32_t* rng;
     long long rng_slots;
     const uint32_t* jump;           // event jump matrices: one (single event) or one per genstep (batched)
+    const uint32_t* ev_rng;         // optional: XORWOW states already advanced to each photon's event
+    long long ev_rng_n;             //   (six planes of ev_rng_n words, by photon index; k_rng_event)
     phx_photon* photon;
     phx_seq* seq;
     uint32_t* hitword;              // zeroed before launch; bits set with atomicOr
@@ -102,6 +104,22 @@ struct PhxLane {
     int ev;
 };
 
+// the XORWOW state of RNG slot `slot` advanced by skipahead(event * skip) (qudarap/qrng.h:85-90)
+PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, long long slot, unsigned long long ev, unsigned& status)
+{
+    if (slot < A.rng_slots) {
+        phx_load_rng(s, A.rng, A.rng_slots, slot);
+    } else {
+        // same state as a prepared slot, computed on the fly (slower; flagged)
+        status |= PHX_STATUS_RNG_RANGE;
+        curand_init(A.seed, (unsigned long long)slot, A.rng_offset, &s);
+    }
+    if (ev > 0ull) {
+        if (A.jump) phx_rng_jump(s, A.jump + (A.gs_event ? (size_t)gi * 1280 : 0), A.skip * ev);
+        else skipahead(A.skip * ev, &s);
+    }
+}
+
 template <bool POLISH, bool ADJ>
 PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status, PhxScore* sc)
 {
@@ -122,16 +140,10 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
         ev = A.event_index;
         slot = A.photon_offset + idx;
     }
-    if (slot < A.rng_slots) {
-        phx_load_rng(L.rng, A.rng, A.rng_slots, slot);
+    if (A.ev_rng) {
+        phx_load_rng(L.rng, A.ev_rng, A.ev_rng_n, idx);
     } else {
-        // same state as a prepared slot, computed on the fly (slower; flagged)
-        status |= PHX_STATUS_RNG_RANGE;
-        curand_init(A.seed, (unsigned long long)slot, A.rng_offset, &L.rng);
-    }
-    if (ev > 0ull) {
-        if (A.jump) phx_rng_jump(L.rng, A.jump + (A.gs_event ? (size_t)gi * 1280 : 0), A.skip * ev);
-        else skipahead(A.skip * ev, &L.rng);
+        phx_event_rng(L.rng, A, gi, slot, ev, status);
     }
     memset(&L.p, 0, sizeof(L.p));
     generate_photon(L.p, L.rng, g, (unsigned long long)slot, A.P, status);
@@ -288,4 +300,33 @@ __global__ void k_event_max(const long long* gs_off, const long long* ev_start, 
 __global__ void k_stamp(unsigned long long* t)
 {
     *t = phx_globaltimer();
+}
+
+// Event-advanced XORWOW state of every photon of the call, by photon index, ahead of the loop:
+// consecutive photons share their genstep and jump matrix, so the 160-column GF(2) product runs
+// with whole warps here instead of in the few lanes that start a photon at a time in the loop.
+__global__ void k_rng_event(PersistArgs A, uint32_t* out, long long n)
+{
+    unsigned status = 0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int gi = phx_find_genstep(A.gs_off, A.G, idx);
+        long long slot;
+        unsigned long long ev;
+        if (A.gs_event) {
+            ev = (unsigned long long)__ldg(A.gs_event + gi);
+            slot = idx - __ldg(A.ev_start + gi);
+        } else {
+            ev = A.event_index;
+            slot = A.photon_offset + idx;
+        }
+        curandStateXORWOW s;
+        phx_event_rng(s, A, gi, slot, ev, status);
+        out[idx] = s.d;
+        out[n * 1 + idx] = s.v[0];
+        out[n * 2 + idx] = s.v[1];
+        out[n * 3 + idx] = s.v[2];
+        out[n * 4 + idx] = s.v[3];
+        out[n * 5 + idx] = s.v[4];
+    }
+    if (status) atomicOr(A.status, status);
 }

@@ -176,8 +176,14 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
 
 // physics of every live path after its closest hit (CSGOptiX/CSGOptiX7.cu:491-509), finishing
 // and refilling slots; live slots go to the next round's list
+// resident 128-thread blocks per SM asked for the physics kernel (its loads of path state are
+// latency-bound, so occupancy matters more than registers)
+#ifndef PHX_WAVE_SHADE_MINB
+#define PHX_WAVE_SHADE_MINB 1
+#endif
+
 template <bool POLISH>
-__global__ void __launch_bounds__(128) k_wave_shade(WaveArgs W)
+__global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
     const unsigned n = *W.n_in;
     unsigned status = 0;
