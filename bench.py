@@ -507,8 +507,8 @@ def main():
                 "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": len(gs), "photons_per_genstep": int(ppg),
                            "photons_per_step": N, "outputs": "photon+seq+hits(SD)+sensor counts",
                            "l2": "inputs larger than L2 (RNG states 240 MB read + 960 MB written per step)",
-                           "kernel": (f"wavefront: closest-hit and physics kernels over a pool of 2,097,152 paths, "
-                                      f"{rounds} rounds per step" if mode == 2 else
+                           "kernel": (f"wavefront: closest-hit and physics kernels over every photon of the event "
+                                      f"in flight, {rounds} rounds per step" if mode == 2 else
                                       "persistent work queue, block 64, refill every bounce"),
                            "parallelism": f"{world} independent event streams" if world > 1 else "1 GPU"},
                 "gpu_launches": launches,

@@ -135,7 +135,7 @@ struct phx_engine {
     DevBuf<PhxWaveSlot> wslot;
     DevBuf<PhxWavePrd> wprd;
     DevBuf<long long> wsidx;
-    DevBuf<uint32_t> wact0, wact1;
+    DevBuf<uint32_t> wact0, wact1, wfree;
     DevBuf<unsigned> wcnt;
     long long last_launches = 0, last_rounds = 0;   // of the last plain simulate call
 };
@@ -672,7 +672,7 @@ int phx_destroy(phx_engine* e)
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
     e->jump_pow.release(); e->jump_tab.release(); e->ev_rng.release();
     e->merge.release();
-    e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wcnt.release();
+    e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wfree.release(); e->wcnt.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -877,7 +877,13 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // Wavefront form (phx_wave.cuh): fill a pool of paths, then rounds of trace + shade launches
 // until no path is live.  The live count is read back every PHX_WAVE_ROUNDS rounds, so the call
 // synchronises the stream; it cannot be captured into a graph.
-#define PHX_WAVE_POOL (1LL << 21)
+// Paths in flight: an event of up to this many photons starts all of them at once (generation
+// in one coherent pass, no refill) at 176 B of HBM per path; larger calls refill slots as paths
+// finish.  Measured on the 10M-photon detector event: 2^21 slots 339M, 2^22 367M, 2^23 416M,
+// 2^24 (no refill) 439M photons/s.
+#ifndef PHX_WAVE_POOL
+#define PHX_WAVE_POOL (1LL << 26)
+#endif
 // calls of at most this many photons get their event-advanced RNG states in one coherent pass
 // ahead of the loop (24 B per photon of scratch); larger ones advance each state as it starts
 #define PHX_EV_RNG_MAX (1LL << 26)
@@ -898,23 +904,28 @@ static int wave_grid(K kernel, int dev, int* cache)
 template <bool POLISH>
 static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
-    static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {};
+    static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {};
     const int dev = e->device;
     if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
     int rc;
     if ((rc = wave_grid(k_wave_init<POLISH>, dev, g_init))) return rc;
     if ((rc = wave_grid(k_wave_trace<POLISH>, dev, g_trace))) return rc;
     if ((rc = wave_grid(k_wave_shade<POLISH>, dev, g_shade))) return rc;
+    if ((rc = wave_grid(k_wave_fill<POLISH>, dev, g_fill))) return rc;
     const long long N = A.N;
     const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
-    PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(2));
-    PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 2 * sizeof(unsigned), st));
+    PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(3));
+    const bool refill = N > pool;
+    PHX_CU(e->wfree.ensure((size_t)pool));
+    PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 3 * sizeof(unsigned), st));
     WaveArgs W;
     W.A = A;
     W.slot = e->wslot.p; W.prd = e->wprd.p; W.sidx = e->wsidx.p; W.pool = pool;
     uint32_t* act[2] = { e->wact0.p, e->wact1.p };
     unsigned* cnt[2] = { e->wcnt.p, e->wcnt.p + 1 };
+    W.free_list = e->wfree.p;
+    W.n_free = e->wcnt.p + 2;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
     k_wave_init<POLISH><<<gi, 128, 0, st>>>(W);
@@ -928,6 +939,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
             k_wave_trace<POLISH><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
             k_wave_shade<POLISH><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
+            if (refill) k_wave_fill<POLISH><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
             cur = 1 - cur;
         }
         PHX_CU(cudaGetLastError());
@@ -1008,7 +1020,8 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         e->last_rounds = 0;
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
-        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (A.ev_rng ? 1 : 0) + (wave ? 1 + 2 * e->last_rounds : 1) + (want_hits ? 3 : 0);
+        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (A.ev_rng ? 1 : 0) +
+                           (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         const int B = PHX_SIM_BLOCK;
         if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);

@@ -8,8 +8,11 @@
 //   k_wave_trace  reads ray origin/direction of every live path, runs phx_trace and writes the PRD
 //                 (a lean kernel: 168 registers, 12 warps per SM, against about 200 and 10)
 //   k_wave_shade  reads the path and its PRD, runs propagate / seq nibble / finish exactly as the
-//                 one-kernel loop does, refills finished slots with new photons from the queue
-//                 (generation) and appends live slots to the next round's list
+//                 one-kernel loop does, and appends live slots to the next round's list and
+//                 finished slots to a free list
+//   k_wave_fill   (only when the event has more photons than slots) gives every free slot the next
+//                 photon from the queue: whole warps take consecutive photons of one genstep, so
+//                 generation runs coherently instead of in the few lanes that just finished
 // Path state is 128 B per slot (sphoton, the XORWOW words, bounce, event, seqhis/seqbnd) plus a
 // 32 B PRD; the extra HBM traffic is about 0.4 KB per bounce against microseconds of traversal.
 // Every photon consumes its random numbers in the same order as in the one-kernel loop, so
@@ -41,6 +44,8 @@ struct WaveArgs {
     uint32_t* act_out;        // live slots of the next round
     const unsigned* n_in;
     unsigned* n_out;
+    uint32_t* free_list;      // slots freed by this round's physics (refilled by k_wave_fill)
+    unsigned* n_free;
     long long pool;           // slots (init only)
 };
 
@@ -86,8 +91,8 @@ PHX_D bool wave_can_trace(const PhxLane& L, const PersistArgs& A)
     return L.bounce < A.C.max_bounce && L.p.time < A.C.max_time;
 }
 
-// warp-aggregated append of slot s to the next round's list
-PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s)
+// warp-aggregated append of slot s to a list (the next round's live list, or the free list)
+PHX_D void wave_push(uint32_t* list, unsigned* count, bool keep, uint32_t s)
 {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
@@ -95,10 +100,12 @@ PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s)
     if (!m) return;
     const unsigned leader = __ffs(m) - 1u;
     unsigned base = 0u;
-    if (lane == leader) base = atomicAdd(W.n_out, (unsigned)__popc(m));
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
     base = __shfl_sync(FULL, base, leader);
-    if (keep) W.act_out[base + __popc(m & ((1u << lane) - 1u))] = s;
+    if (keep) list[base + __popc(m & ((1u << lane) - 1u))] = s;
 }
+
+PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s) { wave_push(W.act_out, W.n_out, keep, s); }
 
 // Lanes in `need` take new photons from the queue until each has a path that can be traced
 // (photons that cannot take a first bounce are finished at once) or the queue is empty.
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
 template <bool POLISH>
 __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArgs W)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) *W.n_out = 0u;   // the shade launch after this one appends
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *W.n_out = 0u; *W.n_free = 0u; }   // the launches after this one append
     const unsigned n = *W.n_in;
     unsigned status = 0;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -215,7 +222,27 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
             if (done) persist_finish<POLISH, false>(L, W.A, nullptr);
             live = !done;
         }
-        if (wave_refill<POLISH>(L, W.A, valid && !live, status)) live = true;
+        if (live) wave_store(W, s, L);
+        wave_append(W, live, s);
+        wave_push(W.free_list, W.n_free, valid && !live, s);
+    }
+    if (status) atomicOr(W.A.status, status);
+}
+
+// new photons from the queue into the slots freed this round (warp-coherent generation)
+template <bool POLISH>
+__global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
+{
+    const unsigned n = *W.n_free;
+    if ((long long)*W.A.queue >= W.A.N) return;
+    unsigned status = 0;
+    PhxLane L;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
+        const long long i = base + (threadIdx.x & 31);
+        const bool valid = i < (long long)n;
+        const uint32_t s = valid ? W.free_list[i] : 0u;
+        const bool live = wave_refill<POLISH>(L, W.A, valid, status);
         if (live) wave_store(W, s, L);
         wave_append(W, live, s);
     }
