@@ -1010,7 +1010,10 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         A.regroup = e->cfg.regroup;
         A.chunk = e->cfg.chunk;
         const bool wave = e->cfg.kernel_mode == 2 && wave_ok;
-        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX) {
+        // the pre-pass pays off where photons start a few lanes at a time (persistent refill,
+        // wavefront refill); when every photon starts in the wavefront's first kernel, whole
+        // warps advance their states there
+        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX && !(wave && N <= PHX_WAVE_POOL)) {
             PHX_CU(e->ev_rng.ensure((size_t)N * 6));
             k_rng_event<<<(unsigned)std::min<long long>((N + 255) / 256, 148LL * 16), 256, 0, st>>>(A, e->ev_rng.p, N);
             PHX_CU(cudaGetLastError());
