@@ -136,6 +136,7 @@ struct phx_engine {
     DevBuf<PhxWavePrd> wprd;
     DevBuf<long long> wsidx;
     DevBuf<uint32_t> wact0, wact1, wfree;
+    DevBuf<float4> wscore;                          // adjoint score terms per slot
     DevBuf<unsigned> wcnt;
     long long last_launches = 0, last_rounds = 0;   // of the last plain simulate call
 };
@@ -672,7 +673,7 @@ int phx_destroy(phx_engine* e)
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
     e->jump_pow.release(); e->jump_tab.release(); e->ev_rng.release();
     e->merge.release();
-    e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wfree.release(); e->wcnt.release();
+    e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wfree.release(); e->wscore.release(); e->wcnt.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -901,23 +902,24 @@ static int wave_grid(K kernel, int dev, int* cache)
     return 0;
 }
 
-template <bool POLISH>
+template <bool POLISH, bool ADJ = false>
 static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
     static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {};
     const int dev = e->device;
     if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
     int rc;
-    if ((rc = wave_grid(k_wave_init<POLISH>, dev, g_init))) return rc;
+    if ((rc = wave_grid(k_wave_init<POLISH, ADJ>, dev, g_init))) return rc;
     if ((rc = wave_grid(k_wave_trace<POLISH>, dev, g_trace))) return rc;
-    if ((rc = wave_grid(k_wave_shade<POLISH>, dev, g_shade))) return rc;
-    if ((rc = wave_grid(k_wave_fill<POLISH>, dev, g_fill))) return rc;
+    if ((rc = wave_grid(k_wave_shade<POLISH, ADJ>, dev, g_shade))) return rc;
+    if ((rc = wave_grid(k_wave_fill<POLISH, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
     const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
     PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(3));
     const bool refill = N > pool;
     PHX_CU(e->wfree.ensure((size_t)pool));
+    if (ADJ) PHX_CU(e->wscore.ensure((size_t)pool * 8));
     PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 3 * sizeof(unsigned), st));
     WaveArgs W;
     W.A = A;
@@ -925,10 +927,11 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     uint32_t* act[2] = { e->wact0.p, e->wact1.p };
     unsigned* cnt[2] = { e->wcnt.p, e->wcnt.p + 1 };
     W.free_list = e->wfree.p;
+    W.score = ADJ ? e->wscore.p : nullptr;
     W.n_free = e->wcnt.p + 2;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
-    k_wave_init<POLISH><<<gi, 128, 0, st>>>(W);
+    k_wave_init<POLISH, ADJ><<<gi, 128, 0, st>>>(W);
     PHX_CU(cudaGetLastError());
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
     e->last_rounds = 0;
@@ -938,8 +941,8 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
         for (int k = 0; k < PHX_WAVE_ROUNDS; k++, r++) {
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
             k_wave_trace<POLISH><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
-            k_wave_shade<POLISH><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
-            if (refill) k_wave_fill<POLISH><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
+            k_wave_shade<POLISH, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
+            if (refill) k_wave_fill<POLISH, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
             cur = 1 - cur;
         }
         PHX_CU(cudaGetLastError());
@@ -1424,7 +1427,7 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     A.adj_wl_lo = wl_lo;
     A.adj_binw = binw;
     if (N > 0) {
-        rc = launch_persistent_t<false, 64, true>(e, A, st);
+        rc = e->cfg.kernel_mode == 2 ? launch_wave_t<false, true>(e, A, st) : launch_persistent_t<false, 64, true>(e, A, st);
         if (rc) return rc;
     }
     PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));

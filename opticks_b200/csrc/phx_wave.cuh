@@ -44,6 +44,7 @@ struct WaveArgs {
     uint32_t* act_out;        // live slots of the next round
     const unsigned* n_in;
     unsigned* n_out;
+    float4* score;            // ADJ: 8 float4 (the 32 score terms) per slot
     uint32_t* free_list;      // slots freed by this round's physics (refilled by k_wave_fill)
     unsigned* n_free;
     long long pool;           // slots (init only)
@@ -85,6 +86,29 @@ PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
     L.idx = W.sidx[s];
 }
 
+PHX_D void wave_store_score(const WaveArgs& W, uint32_t s, const PhxScore* sc)
+{
+    float4* o = W.score + 8 * (size_t)s;
+#pragma unroll
+    for (int k = 0; k < 8; k++) o[k] = make_float4(sc->g[4 * k], sc->g[4 * k + 1], sc->g[4 * k + 2], sc->g[4 * k + 3]);
+}
+
+PHX_D void wave_load_score(const WaveArgs& W, uint32_t s, PhxScore* sc)
+{
+    const float4* o = W.score + 8 * (size_t)s;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const float4 v = o[k];
+        sc->g[4 * k] = v.x; sc->g[4 * k + 1] = v.y; sc->g[4 * k + 2] = v.z; sc->g[4 * k + 3] = v.w;
+    }
+}
+
+PHX_D void wave_score_setup(PhxScore& score, const PersistArgs& A)
+{
+    score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
+    score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
+}
+
 // a path may take another bounce (the loop condition of CSGOptiX/CSGOptiX7.cu:477)
 PHX_D bool wave_can_trace(const PhxLane& L, const PersistArgs& A)
 {
@@ -110,8 +134,8 @@ PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s) { wave_push(W.a
 // Lanes in `need` take new photons from the queue until each has a path that can be traced
 // (photons that cannot take a first bounce are finished at once) or the queue is empty.
 // Returns true in the lanes that hold a live path.  Warp-collective.
-template <bool POLISH>
-PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status)
+template <bool POLISH, bool ADJ = false>
+PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status, PhxScore* sc = nullptr)
 {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
@@ -128,9 +152,9 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
             if (idx >= A.N) {
                 need = false;
             } else {
-                persist_start<POLISH, false>(L, A, idx, status, nullptr);
+                persist_start<POLISH, ADJ>(L, A, idx, status, sc);
                 if (wave_can_trace(L, A)) { live = true; need = false; }
-                else persist_finish<POLISH, false>(L, A, nullptr);
+                else persist_finish<POLISH, ADJ>(L, A, sc);
             }
         }
     }
@@ -138,16 +162,21 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
 }
 
 // fill the pool: every slot takes photons until it holds a live path or the queue is empty
-template <bool POLISH>
+template <bool POLISH, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
 {
     unsigned status = 0;
     PhxLane L;
+    PhxScore score;
+    if (ADJ) wave_score_setup(score, W.A);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < W.pool; base += stride) {
         const long long s = base + (threadIdx.x & 31);
-        const bool live = wave_refill<POLISH>(L, W.A, s < W.pool, status);
-        if (live) wave_store(W, (uint32_t)s, L);
+        const bool live = wave_refill<POLISH, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
+        if (live) {
+            wave_store(W, (uint32_t)s, L);
+            if (ADJ) wave_store_score(W, (uint32_t)s, &score);
+        }
         wave_append(W, live, (uint32_t)s);
     }
     if (status) atomicOr(W.A.status, status);
@@ -189,12 +218,14 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
 #define PHX_WAVE_SHADE_MINB 1
 #endif
 
-template <bool POLISH>
+template <bool POLISH, bool ADJ = false>
 __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
     const unsigned n = *W.n_in;
     unsigned status = 0;
     PhxLane L;
+    PhxScore score;
+    if (ADJ) wave_score_setup(score, W.A);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
         const long long i = base + (threadIdx.x & 31);
@@ -204,6 +235,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
         if (valid) {
             s = W.act_in[i];
             wave_load(W, s, L);
+            if (ADJ) wave_load_score(W, s, &score);
             const float4 nd = W.prd[s].nd;
             const uint4 lgi = W.prd[s].lgi;
             PhxPRD prd;
@@ -214,15 +246,24 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
             prd.ii_id = lgi.z;
             bool done = true;
             if (prd.boundary() != 0xffffu) {
-                const int command = phx_propagate_step(L.p, L.rng, prd, W.A.P, status);
+                int command;
+                if (ADJ) {
+                    prd.normal = normalize(prd.normal);
+                    command = propagate<true>(L.p, L.rng, prd, W.A.P, status, &score);
+                } else {
+                    command = phx_propagate_step(L.p, L.rng, prd, W.A.P, status);
+                }
                 L.bounce++;
                 seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
                 done = command == PHX_BREAK || !wave_can_trace(L, W.A);
             }
-            if (done) persist_finish<POLISH, false>(L, W.A, nullptr);
+            if (done) persist_finish<POLISH, ADJ>(L, W.A, ADJ ? &score : nullptr);
             live = !done;
         }
-        if (live) wave_store(W, s, L);
+        if (live) {
+            wave_store(W, s, L);
+            if (ADJ) wave_store_score(W, s, &score);
+        }
         wave_append(W, live, s);
         wave_push(W.free_list, W.n_free, valid && !live, s);
     }
@@ -230,20 +271,25 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
 }
 
 // new photons from the queue into the slots freed this round (warp-coherent generation)
-template <bool POLISH>
+template <bool POLISH, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
 {
     const unsigned n = *W.n_free;
     if ((long long)*W.A.queue >= W.A.N) return;
     unsigned status = 0;
     PhxLane L;
+    PhxScore score;
+    if (ADJ) wave_score_setup(score, W.A);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
         const long long i = base + (threadIdx.x & 31);
         const bool valid = i < (long long)n;
         const uint32_t s = valid ? W.free_list[i] : 0u;
-        const bool live = wave_refill<POLISH>(L, W.A, valid, status);
-        if (live) wave_store(W, s, L);
+        const bool live = wave_refill<POLISH, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
+        if (live) {
+            wave_store(W, s, L);
+            if (ADJ) wave_store_score(W, s, &score);
+        }
         wave_append(W, live, s);
     }
     if (status) atomicOr(W.A.status, status);
