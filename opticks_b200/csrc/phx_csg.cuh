@@ -84,6 +84,7 @@ PHX_D int phx_csg_lookup(int op, int sa, int sb, bool aCloser)
 struct PhxCsgCtx {
     const float4* node;   // (Nn*4) float4 : CSGNode table
     const float4* itra;   // (Nt*4) float4 : inverse node transforms
+    const float4* plan;   // (Nl) float4 : planes of convex polyhedra (n, w)
 };
 
 PHX_D unsigned nd_u(const float4& q, int k) { return __float_as_uint(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w); }
@@ -414,6 +415,232 @@ PHX_COLD float4 leaf_torus(const float4 q0, const float t_min, const float3 o, c
     return isect;
 }
 
+// ---------------------------------------------------------------- further leaves
+// cone   CSG/csg_intersect_leaf_newcone.h        hyperboloid CSG/csg_intersect_leaf_hyperboloid.h
+// convexpolyhedron CSG/csg_intersect_leaf_convexpolyhedron.h   phicut CSG/csg_intersect_leaf_phicut.h
+// halfspace, slab, infcylinder, disc   CSG/csg_intersect_leaf_{halfspace,slab,infcylinder,disc}.h
+// Each keeps the reference's order of FP32 operations (parity against its intersector).
+#define PHX_RT_MAX 1.e27f
+
+PHX_D float fmin4(float a, float b, float c, float d) { return fminf(fminf(a, b), fminf(c, d)); }
+
+// cone frustum: q0 = (r1, z1, r2, z2), z2 > z1, with end caps
+PHX_COLD float4 leaf_cone(const float4 q0, const float t_min, const float3 o, const float3 d)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float r1 = q0.x, z1 = q0.y, r2 = q0.z, z2 = q0.w;
+    const float r1r1 = r1 * r1, r2r2 = r2 * r2;
+    const float tth = (r2 - r1) / (z2 - z1);
+    const float tth2 = tth * tth;
+    const float z0 = (z2 * r1 - z1 * r2) / (r1 - r2);
+    const float idz = 1.f / d.z;
+    float t_cap1 = d.z == 0.f ? PHX_RT_MAX : (z1 - o.z) * idz;
+    float t_cap2 = d.z == 0.f ? PHX_RT_MAX : (z2 - o.z) * idz;
+    const float rr_cap1 = (o.x + t_cap1 * d.x) * (o.x + t_cap1 * d.x) + (o.y + t_cap1 * d.y) * (o.y + t_cap1 * d.y);
+    const float rr_cap2 = (o.x + t_cap2 * d.x) * (o.x + t_cap2 * d.x) + (o.y + t_cap2 * d.y) * (o.y + t_cap2 * d.y);
+    t_cap1 = rr_cap1 < r1r1 && t_cap1 > t_min ? t_cap1 : PHX_RT_MAX;
+    t_cap2 = rr_cap2 < r2r2 && t_cap2 > t_min ? t_cap2 : PHX_RT_MAX;
+    const float c2 = d.x * d.x + d.y * d.y - d.z * d.z * tth2;
+    const float c1 = o.x * d.x + o.y * d.y - (o.z - z0) * d.z * tth2;
+    const float c0 = o.x * o.x + o.y * o.y - (o.z - z0) * (o.z - z0) * tth2;
+    float t_near, t_far, disc, sdisc;
+    robust_roots_disq(PHX_RT_MAX, t_near, t_far, disc, sdisc, c2, c1, c0);
+    const float z_near = o.z + t_near * d.z;
+    const float z_far = o.z + t_far * d.z;
+    t_near = z_near > z1 && z_near < z2 && t_near > t_min ? t_near : PHX_RT_MAX;
+    t_far = z_far > z1 && z_far < z2 && t_far > t_min ? t_far : PHX_RT_MAX;
+    const float t_cand = fmin4(t_near, t_far, t_cap1, t_cap2);
+    if (t_cand > t_min && t_cand < PHX_RT_MAX) {
+        if (t_cand == t_cap1 || t_cand == t_cap2) {
+            isect.z = t_cand == t_cap2 ? 1.f : -1.f;
+        } else {
+            const float3 n = normalize(make_float3(o.x + t_cand * d.x, o.y + t_cand * d.y, (z0 - (o.z + t_cand * d.z)) * tth2));
+            isect.x = n.x; isect.y = n.y; isect.z = n.z;
+        }
+        isect.w = t_cand;
+    }
+    return isect;
+}
+
+// one-sheet hyperboloid x^2 + y^2 = r0^2 ((z/zf)^2 + 1) between z1 < z2: q0 = (r0, zf, z1, z2)
+PHX_COLD float4 leaf_hyperboloid(const float4 q0, const float t_min, const float3 o, const float3 s)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float r0 = q0.x, zf = q0.y, z1 = q0.z, z2 = q0.w;
+    const float rr0 = r0 * r0;
+    const float z1s = z1 / zf, z2s = z2 / zf;
+    const float rr1 = rr0 * (z1s * z1s + 1.f);
+    const float rr2 = rr0 * (z2s * z2s + 1.f);
+    const float A = -rr0 / (zf * zf);
+    const float B = -rr0;
+    const float dd = s.x * s.x + s.y * s.y + A * s.z * s.z;
+    const float b = o.x * s.x + o.y * s.y + A * o.z * s.z;
+    const float c = o.x * o.x + o.y * o.y + A * o.z * o.z + B;
+    float t1hyp, t2hyp, disc, sdisc;
+    robust_roots(t1hyp, t2hyp, disc, sdisc, dd, b, c);
+    const float h1z = o.z + t1hyp * s.z;
+    const float h2z = o.z + t2hyp * s.z;
+    const float osz = 1.f / s.z;
+    const float t2cap = (z2 - o.z) * osz;
+    const float t1cap = (z1 - o.z) * osz;
+    const float3 c1 = o + t1cap * s;
+    const float3 c2 = o + t2cap * s;
+    const float crr1 = c1.x * c1.x + c1.y * c1.y;
+    const float crr2 = c2.x * c2.x + c2.y * c2.y;
+    const float a0 = t1hyp > t_min && disc > 0.f && h1z > z1 && h1z < z2 ? t1hyp : PHX_RT_MAX;
+    const float a1 = t2hyp > t_min && disc > 0.f && h2z > z1 && h2z < z2 ? t2hyp : PHX_RT_MAX;
+    const float a2 = t2cap > t_min && crr2 < rr2 ? t2cap : PHX_RT_MAX;
+    const float a3 = t1cap > t_min && crr1 < rr1 ? t1cap : PHX_RT_MAX;
+    const float t_cand = fmin4(a0, a1, a2, a3);
+    if (t_cand > t_min && t_cand < PHX_RT_MAX) {
+        isect.w = t_cand;
+        if (t_cand == t1hyp || t_cand == t2hyp) {
+            const float3 p = o + t_cand * s;
+            const float3 n = normalize(make_float3(p.x, p.y, A * p.z));
+            isect.x = n.x; isect.y = n.y; isect.z = n.z;
+        } else {
+            isect.z = t_cand == t1cap ? -1.f : 1.f;
+        }
+    }
+    return isect;
+}
+
+// convex polyhedron: the intersection of planeNum half-spaces n.x <= w from the plan table, starting
+// at planeIdx (q0 words x, y); entering keeps the latest entry, exiting the earliest exit
+PHX_COLD float4 leaf_convexpolyhedron(const float4 q0, const float4* __restrict__ plan, const float t_min, const float3 o, const float3 d)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const unsigned planeIdx = __float_as_uint(q0.x), planeNum = __float_as_uint(q0.y);
+    const float INF = __int_as_float(0x7f800000);
+    float t0 = -INF, t1 = INF;
+    float3 n0 = make_float3(0.f, 0.f, 0.f), n1 = make_float3(0.f, 0.f, 0.f);
+    for (unsigned i = 0; i < planeNum && i < 256u; i++) {
+        const float4 pl = __ldg(plan + planeIdx + i);
+        const float3 n = make_float3(pl.x, pl.y, pl.z);
+        const float nd = dot(n, d);
+        const float no = dot(n, o);
+        const float dist = no - pl.w;
+        const float t_cand = -dist / nd;
+        if (nd == 0.f && dist < 0.f) continue;          // parallel, inside this half-space
+        if (nd == 0.f && dist > 0.f) return isect;      // parallel, outside: no intersect
+        if (nd < 0.f) { if (t_cand > t0) { t0 = t_cand; n0 = n; } }
+        else          { if (t_cand < t1) { t1 = t_cand; n1 = n; } }
+    }
+    if (t0 < t1) {
+        if (t0 > t_min) isect = make_float4(n0.x, n0.y, n0.z, t0);
+        else if (t1 > t_min) isect = make_float4(n1.x, n1.y, n1.z, t1);
+    }
+    return isect;
+}
+
+// phi wedge between the half-planes at phi0 and phi1: q0 = (cos phi0, sin phi0, cos phi1, sin phi1);
+// a miss with an unbounded exit carries y = -0 (promoted to EXIT by the tree evaluator)
+PHX_COLD float4 leaf_phicut(const float4 q0, const float t_min, const float3 o, const float3 d)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float cosPhi0 = q0.x, sinPhi0 = q0.y, cosPhi1 = q0.z, sinPhi1 = q0.w;
+    const float d_n0 = d.x * sinPhi0 + d.y * (-cosPhi0);
+    const float d_n1 = d.x * (-sinPhi1) + d.y * (cosPhi1);
+    const float o_n0 = o.x * sinPhi0 + o.y * (-cosPhi0);
+    const float o_n1 = o.x * (-sinPhi1) + o.y * (cosPhi1);
+    float t0 = d_n0 == 0.f ? t_min : -o_n0 / d_n0;
+    float t1 = d_n1 == 0.f ? t_min : -o_n1 / d_n1;
+    const float PR = d_n0 == 0.f ? -o_n0 : -d_n0;
+    const float QR = d_n1 == 0.f ? -o_n1 : -d_n1;
+    const float PQ = cosPhi0 * sinPhi1 - cosPhi1 * sinPhi0;
+    const bool unbounded_exit = PQ >= 0.f ? (PR >= 0.f && QR <= 0.f) : (PR >= 0.f || QR <= 0.f);
+    const float side0 = o.x * cosPhi0 + o.y * sinPhi0 + (d.x * cosPhi0 + d.y * sinPhi0) * t0;
+    const float side1 = o.x * cosPhi1 + o.y * sinPhi1 + (d.x * cosPhi1 + d.y * sinPhi1) * t1;
+    if (side0 < 0.f) t0 = t_min;
+    if (side1 < 0.f) t1 = t_min;
+    const float t_near = fminf(t0, t1);
+    const float t_far = fmaxf(t0, t1);
+    const float t_cand = t_near > t_min ? t_near : (t_far > t_min ? t_far : t_min);
+    if (t_cand > t_min) {
+        isect.x = t_cand == t1 ? -sinPhi1 : sinPhi0;
+        isect.y = t_cand == t1 ? cosPhi1 : -cosPhi0;
+        isect.w = t_cand;
+    } else if (unbounded_exit) {
+        isect.y = -isect.y;
+    }
+    return isect;
+}
+
+// half-space n.x <= w: q0 = (n, w); a miss from inside carries y = -0 (unbounded exit)
+PHX_COLD float4 leaf_halfspace(const float4 q0, const float t_min, const float3 o, const float3 d)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float3 n = make_float3(q0.x, q0.y, q0.z);
+    const float on = dot(o, n);
+    const float dn = dot(d, n);
+    const float on_w = on - q0.w;
+    const bool inside = on_w < -1e-9f;
+    const float t = fabsf(dn) > 0.f ? -on_w / dn : t_min;
+    if (t > t_min) isect = make_float4(n.x, n.y, n.z, t);
+    else if (inside) isect.y = -0.f;
+    return isect;
+}
+
+// slab a <= n.x <= b: q0 = n, q1 = (a, b)
+PHX_COLD float4 leaf_slab(const float4 q0, const float4 q1, const float t_min, const float3 o, const float3 d)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float3 n = make_float3(q0.x, q0.y, q0.z);
+    const float idn = 1.f / dot(d, n);
+    const float on = dot(o, n);
+    const float ta = (q1.x - on) * idn;
+    const float tb = (q1.y - on) * idn;
+    const float t_near = fminf(ta, tb);
+    const float t_far = fmaxf(ta, tb);
+    const float t_cand = t_near > t_min ? t_near : (t_far > t_min ? t_far : t_min);
+    if (t_cand > t_min) {
+        const bool b_hit = t_cand == tb;
+        isect = make_float4(b_hit ? n.x : -n.x, b_hit ? n.y : -n.y, b_hit ? n.z : -n.z, t_cand);
+    }
+    return isect;
+}
+
+// infinite cylinder about z of radius q0.w
+PHX_COLD float4 leaf_infcylinder(const float4 q0, const float t_min, const float3 O, const float3 D)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float r = q0.w;
+    const float a = D.x * D.x + D.y * D.y;
+    const float b = O.x * D.x + O.y * D.y;
+    const float c = O.x * O.x + O.y * O.y - r * r;
+    const float disc0 = b * b - a * c;
+    if (disc0 > 0.f) {
+        float t_NEAR, t_FAR, disc, sdisc;
+        robust_roots(t_NEAR, t_FAR, disc, sdisc, a, b, c);
+        const float t_cand = sdisc > 0.f ? (t_NEAR > t_min ? t_NEAR : t_FAR) : t_min;
+        if (t_cand > t_min) isect = make_float4((O.x + t_cand * D.x) / r, (O.y + t_cand * D.y) / r, 0.f, t_cand);
+    }
+    return isect;
+}
+
+// annular disc of thickness z2 - z1 about (q0.x, q0.y, (z1+z2)/2), inner radius q0.z, outer q0.w
+PHX_COLD float4 leaf_disc(const float4 q0, const float4 q1, const float t_min, const float3 ray_origin, const float3 n)
+{
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float inner = q0.z, radius = q0.w, z1 = q1.x, z2 = q1.y;
+    const float zc = (z1 + z2) / 2.f;
+    const float zdelta = (z2 - z1) / 2.f;
+    const float3 center = make_float3(q0.x, q0.y, zc);
+    const float3 m = ray_origin - center;
+    const float3 dn = make_float3(0.f, 0.f, 1.f);
+    const float rr = radius * radius, ii = inner * inner;
+    const float mm = dot(m, m), nn = dot(n, n), nd = dot(n, dn), md = dot(m, dn), mn = dot(m, n);
+    const float t_center = -md / nd;
+    const float rsq = t_center * (2.f * mn + t_center * nn) + mm;
+    const float t_delta = nd < 0.f ? -zdelta / nd : zdelta / nd;
+    const float root1 = t_center - t_delta;
+    const float root2 = t_center + t_delta;
+    const float t_cand = (rsq < rr && rsq > ii) ? (root1 > t_min ? root1 : root2) : t_min;
+    const float side = md + t_cand * nd;
+    if (t_cand > t_min) isect = make_float4(0.f, 0.f, side > 0.f ? 1.f : -1.f, t_cand);
+    return isect;
+}
+
 // ---------------------------------------------------------------- leaf with transform
 #if PHX_OUTLINE
 #define PHX_LEAFFN __device__ __noinline__
@@ -424,8 +651,8 @@ PHX_COLD float4 leaf_torus(const float4 q0, const float t_min, const float3 o, c
 // prims; arguments and result by value so nothing goes through the stack.  A miss returns w=0
 // (with x=-0 for a complemented leaf), a hit has w = t > t_min.
 template <bool POLISH>
-PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __restrict__ itra, const int ni, const float t_min,
-                            const float3 ray_o, const float3 ray_d)
+PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __restrict__ itra, const float4* __restrict__ plan,
+                            const int ni, const float t_min, const float3 ray_o, const float3 ray_d)
 {
     float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 q0 = __ldg(node + 4 * ni + 0);
@@ -451,6 +678,14 @@ PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __res
         case PHX_CSG_CYLINDER: valid = leaf_cylinder<POLISH>(isect, q0, q1, t_min, origin, direction); break;
         case PHX_CSG_BOX3:     isect = leaf_box3(q0, t_min, origin, direction); valid = isect.w > t_min; break;
         case PHX_CSG_TORUS:    isect = leaf_torus(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_CONE:     isect = leaf_cone(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_HYPERBOLOID: isect = leaf_hyperboloid(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_CONVEXPOLYHEDRON: isect = leaf_convexpolyhedron(q0, plan, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_PHICUT:   isect = leaf_phicut(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_HALFSPACE: isect = leaf_halfspace(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_SLAB:     isect = leaf_slab(q0, q1, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_INFCYLINDER: isect = leaf_infcylinder(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_DISC:     isect = leaf_disc(q0, q1, t_min, origin, direction); valid = isect.w > t_min; break;
         default: break;
     }
     if (valid && q) {
@@ -469,7 +704,7 @@ template <bool POLISH>
 PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
 {
     (void)err;
-    isect = leaf_eval<POLISH>(g.node, g.itra, ni, t_min, ray_o, ray_d);
+    isect = leaf_eval<POLISH>(g.node, g.itra, g.plan, ni, t_min, ray_o, ray_d);
     return isect.w > t_min;
 }
 
@@ -494,8 +729,8 @@ PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
 template <bool POLISH>
 PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned op, float t_min, const float3& o, const float3& d, unsigned& err)
 {
-    float4 L = leaf_eval<POLISH>(g.node, g.itra, root + 1, t_min, o, d);
-    float4 R = leaf_eval<POLISH>(g.node, g.itra, root + 2, t_min, o, d);
+    float4 L = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 1, t_min, o, d);
+    float4 R = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 2, t_min, o, d);
     for (int it = 0; it < PHX_TREE3_LOOP_CAP; it++) {
         int l_state = phx_classify(L, d, t_min);
         int r_state = phx_classify(R, d, t_min);
@@ -512,8 +747,8 @@ PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned
             isect = result;
             return isect.w > 0.f;
         }
-        if (ctrl == PHX_CTRL_LOOP_A) L = leaf_eval<POLISH>(g.node, g.itra, root + 1, fabsf(L.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
-        else R = leaf_eval<POLISH>(g.node, g.itra, root + 2, fabsf(R.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+        if (ctrl == PHX_CTRL_LOOP_A) L = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 1, fabsf(L.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+        else R = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 2, fabsf(R.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
     }
     err |= PHX_STATUS_CSG_STACK;
     isect = make_float4(0.f, 0.f, 0.f, 0.f);

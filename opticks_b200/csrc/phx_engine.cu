@@ -149,6 +149,7 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.inst_inv = e->inst_inv.p;
     S.csg.node = e->node.p;
     S.csg.itra = e->itra.p;
+    S.csg.plan = e->plan.p;
     (void)polish;
     S.globals = e->globals.p;
     S.leaf_sph = e->leaf_sph.p;
@@ -522,6 +523,22 @@ static PhxSph node_sphere(const phx_geometry* geo, int no, int i, int num)
         case PHX_CSG_TORUS:
             s = { { 0, 0, 0 }, std::fabs((double)q[2]) + std::fabs((double)q[1]) };
             break;
+        case PHX_CSG_CONE: {
+            const double r = std::max(std::fabs((double)q[0]), std::fabs((double)q[2])), h = 0.5 * ((double)q[3] - q[1]);
+            s = { { 0, 0, 0.5 * ((double)q[1] + q[3]) }, std::sqrt(r * r + h * h) };
+            break;
+        }
+        case PHX_CSG_HYPERBOLOID: {
+            const double r0 = q[0], zf = q[1], z1 = q[2], z2 = q[3];
+            const double zm = std::max(std::fabs(z1), std::fabs(z2)) / zf, h = 0.5 * (z2 - z1);
+            s = { { 0, 0, 0.5 * (z1 + z2) }, std::sqrt(r0 * r0 * (zm * zm + 1.0) + h * h) };
+            break;
+        }
+        case PHX_CSG_DISC: {
+            const double r = q[3], h = 0.5 * ((double)q[5] - q[4]);
+            s = { { q[0], q[1], 0.5 * ((double)q[4] + q[5]) }, std::sqrt(r * r + h * h) };
+            break;
+        }
         default:
             return inf;
     }
@@ -1140,6 +1157,7 @@ int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d
     PhxCsgCtx csg;
     csg.node = e->node.p;
     csg.itra = e->itra.p;
+    csg.plan = e->plan.p;
     if (n > 0) {
         const int B = 128;
         const unsigned grid = (unsigned)((n + B - 1) / B);

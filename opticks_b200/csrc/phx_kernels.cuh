@@ -59,7 +59,9 @@ PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, con
     const float3 ld = xform_row(m, d, 0.f);
     float4 is;
     const bool valid = intersect_prim<POLISH>(is, S.csg, L.y, tmin, lo, ld, status);
-    if (valid && is.w < B.t) {
+    // OptiX's interval rule: a report outside [tmin, tmax] is ignored (a convexpolyhedron wholly
+    // behind the ray reports valid with t = 0, CSG/csg_intersect_leaf_convexpolyhedron.h:85-101)
+    if (valid && is.w >= tmin && is.w < B.t) {
         B.t = is.w;
         B.L = L;
         B.isect = is;

@@ -73,7 +73,15 @@ enum {
     PHX_CSG_ZSPHERE = 103,
     PHX_CSG_CYLINDER = 105,
     PHX_CSG_BOX3 = 110,
-    PHX_CSG_TORUS = 116
+    PHX_CSG_TORUS = 116,
+    PHX_CSG_SLAB = 106,
+    PHX_CSG_CONE = 108,
+    PHX_CSG_CONVEXPOLYHEDRON = 112,
+    PHX_CSG_DISC = 113,
+    PHX_CSG_HYPERBOLOID = 117,
+    PHX_CSG_INFCYLINDER = 119,
+    PHX_CSG_PHICUT = 121,
+    PHX_CSG_HALFSPACE = 125
 };
 
 // ---- surface kinds held in optical[line].y ----

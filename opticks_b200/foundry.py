@@ -31,6 +31,15 @@ CSG_ZSPHERE = 103
 CSG_CYLINDER = 105
 CSG_BOX3 = 110
 CSG_TORUS = 116
+CSG_SLAB = 106
+CSG_CONE = 108
+CSG_CONVEXPOLYHEDRON = 112
+CSG_DISC = 113
+CSG_HYPERBOLOID = 117
+CSG_INFCYLINDER = 119
+CSG_PHICUT = 121
+CSG_HALFSPACE = 125
+UNBOUNDED = 1.0e9     # box half-extent given to unbounded leaves (halfspace, slab, phicut, infcylinder)
 
 OPS = {"union": CSG_UNION, "intersection": CSG_INTERSECTION, "difference": CSG_DIFFERENCE}
 
@@ -45,6 +54,7 @@ class Node:
     transform: np.ndarray | None = None   # 4x4 row-vector (object -> parent frame)
     complement: bool = False
     bbox: tuple | None = None             # local (object frame) box of this leaf
+    planes: np.ndarray | None = None      # convex polyhedron: (n,4) planes (unit normal, distance)
 
     @property
     def is_leaf(self) -> bool:
@@ -77,6 +87,59 @@ def torus(rmajor, rminor):
     return Node(CSG_TORUS, (0.0, r, R, 0.0, 360.0, 0.0), bbox=(-(R + r), -(R + r), -r, R + r, R + r, r))
 
 
+def cone(r1, z1, r2, z2):
+    """cone frustum about z from radius r1 at z1 to r2 at z2 (z2 > z1), capped (CSGNode::Cone)"""
+    R = max(r1, r2)
+    return Node(CSG_CONE, (r1, z1, r2, z2, 0.0, 0.0), bbox=(-R, -R, z1, R, R, z2))
+
+
+def hyperboloid(r0, zf, z1, z2):
+    """one-sheet hyperboloid x^2+y^2 = r0^2((z/zf)^2+1) between z1 < z2, capped (CSGNode::Hyperboloid)"""
+    R = r0 * math.sqrt((max(abs(z1), abs(z2)) / zf) ** 2 + 1.0)
+    return Node(CSG_HYPERBOLOID, (r0, zf, z1, z2, 0.0, 0.0), bbox=(-R, -R, z1, R, R, z2))
+
+
+def convexpolyhedron(planes, bbox):
+    """intersection of half-spaces n.x <= w, planes (n,4) rows (nx, ny, nz, w) with unit normals"""
+    pl = np.asarray(planes, dtype=np.float32).reshape(-1, 4)
+    return Node(CSG_CONVEXPOLYHEDRON, (0.0,) * 6, bbox=tuple(bbox), planes=pl)
+
+
+def cube_planes(h):
+    """the six planes of the cube |x|,|y|,|z| <= h"""
+    return [(1, 0, 0, h), (-1, 0, 0, h), (0, 1, 0, h), (0, -1, 0, h), (0, 0, 1, h), (0, 0, -1, h)]
+
+
+def phicut(phi0, phi1):
+    """wedge between the half-planes at azimuths phi0 < phi1 (radians) about z (CSGNode::PhiCut)"""
+    U = UNBOUNDED
+    return Node(CSG_PHICUT, (math.cos(phi0), math.sin(phi0), math.cos(phi1), math.sin(phi1), 0.0, 0.0),
+                bbox=(-U, -U, -U, U, U, U))
+
+
+def halfspace(n, w):
+    """half-space n.x <= w (unit normal n)"""
+    U = UNBOUNDED
+    return Node(CSG_HALFSPACE, (n[0], n[1], n[2], w, 0.0, 0.0), bbox=(-U, -U, -U, U, U, U))
+
+
+def slab(n, a, b):
+    """slab a <= n.x <= b (unit normal n)"""
+    U = UNBOUNDED
+    return Node(CSG_SLAB, (n[0], n[1], n[2], 0.0, a, b), bbox=(-U, -U, -U, U, U, U))
+
+
+def infcylinder(r):
+    """cylinder of radius r about z, unbounded in z"""
+    U = UNBOUNDED
+    return Node(CSG_INFCYLINDER, (0.0, 0.0, 0.0, r, 0.0, 0.0), bbox=(-r, -r, -U, r, r, U))
+
+
+def disc(inner, radius, z1, z2, cx=0.0, cy=0.0):
+    """annulus inner < rho < radius about (cx, cy) between z1 < z2 (CSGNode::Disc)"""
+    return Node(CSG_DISC, (cx, cy, inner, radius, z1, z2), bbox=(cx - radius, cy - radius, z1, cx + radius, cy + radius, z2))
+
+
 def op(name, a: Node, b: Node) -> Node:
     return Node(OPS[name], left=a, right=b)
 
@@ -101,14 +164,24 @@ def _bbox_transformed(bb, m):
 
 
 def _tree_bbox(n: Node):
+    """bbox of a subtree in the frame of its parent (the node's own transform applied)"""
     if n.is_leaf:
         return _bbox_transformed(n.bbox, n.transform)
     a, b = _tree_bbox(n.left), _tree_bbox(n.right)
     if n.typecode == CSG_UNION:
-        return tuple(min(a[k], b[k]) for k in range(3)) + tuple(max(a[k], b[k]) for k in range(3, 6))
-    if n.typecode == CSG_INTERSECTION:
-        return tuple(max(a[k], b[k]) for k in range(3)) + tuple(min(a[k], b[k]) for k in range(3, 6))
-    return a   # difference bounded by A
+        bb = tuple(min(a[k], b[k]) for k in range(3)) + tuple(max(a[k], b[k]) for k in range(3, 6))
+    elif n.typecode == CSG_INTERSECTION:
+        bb = tuple(max(a[k], b[k]) for k in range(3)) + tuple(min(a[k], b[k]) for k in range(3, 6))
+    else:
+        bb = a   # difference bounded by A
+    return _bbox_transformed(bb, n.transform)
+
+
+def _compose(local, parent):
+    """row-vector transforms: a point takes ``local`` first, then ``parent``"""
+    if local is None:
+        return parent
+    return local if parent is None else np.asarray(local) @ np.asarray(parent)
 
 
 @dataclass
@@ -119,6 +192,7 @@ class Foundry:
     inst: list = field(default_factory=list)
     tran: list = field(default_factory=list)
     itra: list = field(default_factory=list)
+    plan: list = field(default_factory=list)
 
     # -------------------------------------------------------------- building
     def _add_transform(self, m) -> int:
@@ -132,12 +206,17 @@ class Foundry:
         num = (1 << (h + 1)) - 1
         slots: list[Node | None] = [None] * num
 
-        def place(n, i):
+        gtran: list = [None] * num
+
+        # a transform on an operator node moves its whole subtree: each leaf carries the product
+        # of its own and its ancestors' transforms (the leaf's gtransform, as in CSG/CSGNode.h)
+        def place(n, i, parent_m):
             slots[i] = n
+            gtran[i] = _compose(n.transform, parent_m)
             if not n.is_leaf:
-                place(n.left, 2 * i + 1)
-                place(n.right, 2 * i + 2)
-        place(root, 0)
+                place(n.left, 2 * i + 1, gtran[i])
+                place(n.right, 2 * i + 2, gtran[i])
+        place(root, 0, None)
         offset = len(self.node)
         for i, n in enumerate(slots):
             q = np.zeros((4, 4), dtype=np.float32)
@@ -148,6 +227,10 @@ class Foundry:
                 if n.is_leaf:
                     q[0, :4] = n.param[:4]
                     q[1, :2] = n.param[4:6]
+                    if n.planes is not None:       # convex polyhedron: planeIdx, planeNum (CSG/CSGNode.h:204-207)
+                        qu[0, 0] = len(self.plan)
+                        qu[0, 1] = len(n.planes)
+                        self.plan.extend(np.asarray(n.planes, np.float32))
                     bb = n.bbox
                 else:
                     bb = _tree_bbox(n)
@@ -155,7 +238,7 @@ class Foundry:
                 q[2, 3] = bb[3]
                 q[3, 0:2] = bb[4:6]
                 qu[3, 2] = n.typecode
-                tidx = self._add_transform(n.transform) if (n.is_leaf and n.transform is not None) else 0
+                tidx = self._add_transform(gtran[i]) if (n.is_leaf and gtran[i] is not None) else 0
                 qu[3, 3] = (tidx & 0x7FFFFFFF) | (0x80000000 if n.complement else 0)
             qu[1, 2] = boundary
             qu[1, 3] = i
@@ -209,7 +292,7 @@ class Foundry:
             "inst": stack(self.inst, (4, 4), np.float32),
             "tran": stack([m.astype(np.float32) for m in self.tran], (4, 4), np.float32),
             "itra": stack([m.astype(np.float32) for m in self.itra], (4, 4), np.float32),
-            "plan": np.zeros((0, 4), dtype=np.float32),
+            "plan": stack(self.plan, (4,), np.float32),
         }
 
     def save(self, fold: str) -> None:

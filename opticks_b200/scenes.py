@@ -120,6 +120,74 @@ def csg_scan_tree(with_torus: bool = True):
     return fd, p
 
 
+# zoo prims whose trees hold a slab, infcylinder or disc leaf: the reference compiles those three
+# leaves only under CSG_EXTRA (CSG/csg_intersect_leaf.h:100-108,224-232), so its tree intersector
+# misses them; they are compared leaf by leaf against the reference's leaf functions instead
+ZOO_EXTRA_PRIMS = (8, 9, 10, 13)
+
+
+def csg_leaf_zoo():
+    """(foundry, prim indices) exercising the cone, hyperboloid, convexpolyhedron, phicut,
+    halfspace, slab, infcylinder and disc leaves alone, transformed, complemented and inside small
+    trees (unbounded leaves always cut by a bounded one)"""
+    octa = [(sx / math.sqrt(3.0), sy / math.sqrt(3.0), sz / math.sqrt(3.0), 180.0)
+            for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)]
+    comp_phi = F.phicut(0.5, 2.0)
+    comp_phi.complement = True
+    trees = [
+        F.cone(200.0, -150.0, 50.0, 150.0),
+        F.translate(F.cone(80.0, -100.0, 220.0, 120.0), 30.0, -40.0, 20.0),
+        F.hyperboloid(150.0, 120.0, -200.0, 200.0),
+        F.convexpolyhedron(F.cube_planes(150.0), (-150, -150, -150, 150, 150, 150)),
+        F.convexpolyhedron(octa, (-312, -312, -312, 312, 312, 312)),
+        F.op("intersection", F.sphere(250.0), F.phicut(0.3, 2.5)),
+        F.op("intersection", F.cylinder(250.0, -200.0, 200.0), F.phicut(-1.0, 3.5)),
+        F.op("intersection", F.sphere(250.0), F.halfspace((0.0, 0.0, 1.0), 50.0)),
+        F.op("intersection", F.box3(500.0, 500.0, 500.0), F.slab((0.6, 0.8, 0.0), -100.0, 150.0)),
+        F.op("intersection", F.infcylinder(120.0), F.box3(600.0, 600.0, 400.0)),
+        F.disc(50.0, 250.0, -10.0, 10.0),
+        F.op("difference", F.cone(220.0, -200.0, 20.0, 200.0), F.convexpolyhedron(F.cube_planes(90.0), (-90, -90, -90, 90, 90, 90))),
+        F.op("intersection", F.sphere(240.0), comp_phi),
+        F.op("union", F.hyperboloid(100.0, 80.0, -150.0, 150.0), F.disc(0.0, 230.0, -5.0, 5.0)),
+    ]
+    fd = F.Foundry()
+    prims = [fd.add_prim(t, 0) for t in trees]
+    fd.add_solid("zoo", prims)
+    fd.add_inst(np.eye(4), 0)
+    return fd, prims
+
+
+def leaf_zoo_detector(num_photon: int = 100_000):
+    """photons from the centre of a water-filled box whose walls detect, through acrylic bodies
+    made of the further leaves: a cone, a hyperboloid, an octahedral convexpolyhedron, a sphere cut
+    by a phicut wedge, a sphere cut by a halfspace and a cone minus a convexpolyhedron cube"""
+    lib = M.BoundaryLib()
+    lib.mat(VACUUM)
+    lib.mat(M.Material("Rock", rindex=1.5, absorption_length=1.0, scattering_length=1e9))
+    lib.mat(WATER_C1)
+    lib.mat(M.Material("Acrylic", rindex=1.49, absorption_length=1e6, scattering_length=1e6))
+    lib.sur(M.Surface("Detector", detect=1.0, absorb=0.0))
+    b_box = lib.add("Rock", "", "Detector", "Water")
+    b_acr = lib.add("Water", "", "", "Acrylic")
+    octa = [(sx / math.sqrt(3.0), sy / math.sqrt(3.0), sz / math.sqrt(3.0), 180.0)
+            for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)]
+    bodies = [
+        F.translate(F.cone(200.0, -150.0, 50.0, 150.0), 800.0, 0.0, 0.0),
+        F.translate(F.hyperboloid(120.0, 100.0, -200.0, 200.0), -800.0, 0.0, 0.0),
+        F.translate(F.convexpolyhedron(octa, (-312, -312, -312, 312, 312, 312)), 0.0, 800.0, 0.0),
+        F.translate(F.op("intersection", F.sphere(250.0), F.phicut(0.3, 2.5)), 0.0, -800.0, 0.0),
+        F.translate(F.op("intersection", F.sphere(250.0), F.halfspace((0.0, 0.0, 1.0), 50.0)), 0.0, 0.0, 800.0),
+        F.translate(F.op("difference", F.cone(220.0, -200.0, 20.0, 200.0),
+                         F.convexpolyhedron(F.cube_planes(90.0), (-90, -90, -90, 90, 90, 90))), 0.0, 0.0, -800.0),
+    ]
+    fd = F.Foundry()
+    prims = [fd.add_prim(F.box3(3000.0, 3000.0, 3000.0), b_box)] + [fd.add_prim(b, b_acr) for b in bodies]
+    s0 = fd.add_solid("zoo", prims)
+    fd.add_inst(np.eye(4), s0)
+    gs = torch_genstep(num_photon, wavelength=440.0, radius=0.0, type_=T_SPHERE, distance=0.25)[None]
+    return fd, lib, None, gs
+
+
 def scan_rays(n: int, seed: int = 0, half: float = 1000.0) -> np.ndarray:
     """(6,n) SoA: origins uniform in a 2 m cube, directions uniform on the sphere"""
     rng = np.random.Generator(np.random.PCG64(seed))

@@ -31,6 +31,7 @@ typedef struct {
     const float* node;
     const float* itra;
     int polish;
+    const float* plan;          /* (Nl,4) convex polyhedron planes, or NULL */
 } oracle_csg;
 
 /* Kensler single-hit CSG actions: 0 miss, 1 return A, 2 return B, 3 return flipped B,
@@ -107,10 +108,10 @@ static int oracle_quartic_first_root(const double* c, double lo, double hi, doub
 
 /* ------------------------------------------------------------------ CSG scan entry points */
 /* rays SoA (6,n); out (n,4) normal.xyz,t (t=0 miss); returns OR of evaluator errors */
-int oracle_csg_scan(const float* node, const float* itra, int root, float tmin, const float* rays, long long n,
-                    float* out, int use_double, int polish)
+int oracle_csg_scan(const float* node, const float* itra, const float* plan, int root, float tmin, const float* rays,
+                    long long n, float* out, int use_double, int polish)
 {
-    oracle_csg g = { node, itra, polish };
+    oracle_csg g = { node, itra, polish, plan };
     int err_all = 0;
 #pragma omp parallel for schedule(static) reduction(| : err_all)
     for (long long i = 0; i < n; i++) {
@@ -134,9 +135,10 @@ int oracle_csg_scan(const float* node, const float* itra, int root, float tmin, 
 }
 
 /* FP64 distance along each ray (t, 0 for miss) for intersection-distance error statistics */
-int oracle_csg_scan_t64(const float* node, const float* itra, int root, float tmin, const float* rays, long long n, double* t)
+int oracle_csg_scan_t64(const float* node, const float* itra, const float* plan, int root, float tmin, const float* rays,
+                        long long n, double* t)
 {
-    oracle_csg g = { node, itra, 0 };
+    oracle_csg g = { node, itra, 0, plan };
     int err_all = 0;
 #pragma omp parallel for schedule(static) reduction(| : err_all)
     for (long long i = 0; i < n; i++) {
@@ -214,6 +216,7 @@ typedef struct {
     unsigned eps0_mask, hit_mask;
     int polish;
     const float* pair_bbox;     /* (Np,6) padded world boxes, or NULL for no culling */
+    const float* plan;          /* (Nl,4) convex polyhedron planes, or NULL */
 } oracle_scene;
 
 typedef struct { const float* u; int n; int k; int over; } ustream;
@@ -385,7 +388,7 @@ static int trace(const oracle_scene* S, v3 o, v3 d, float tmin, prd_t* prd, int*
     int bi = -1;
     float bis[4] = { 0, 0, 0, 0 };
     float blc = 0.f;
-    oracle_csg g = { S->node, S->itra, S->polish };
+    oracle_csg g = { S->node, S->itra, S->polish, S->plan };
     double inv[3] = { 1.0 / d.x, 1.0 / d.y, 1.0 / d.z };
     double oo[3] = { o.x, o.y, o.z };
     for (int k = 0; k < S->num_pair; k++) {
@@ -404,7 +407,9 @@ static int trace(const oracle_scene* S, v3 o, v3 d, float tmin, prd_t* prd, int*
         const float* m = S->inst_inv + 16 * S->pair_inst[k];
         vec_f lo = rowx_f(m, mk_f(o.x, o.y, o.z), 1.f), ld = rowx_f(m, mk_f(d.x, d.y, d.z), 0.f);
         float is[4];
-        if (prim_f(is, &g, S->pair_node[k], tmin, lo, ld, err) && is[3] < best) {
+        /* OptiX ignores a report outside [tmin, tmax]: a convexpolyhedron wholly behind the ray
+           reports valid with t = 0 (CSG/csg_intersect_leaf_convexpolyhedron.h:85-101) */
+        if (prim_f(is, &g, S->pair_node[k], tmin, lo, ld, err) && is[3] >= tmin && is[3] < best) {
             best = is[3]; bi = k;
             memcpy(bis, is, sizeof(bis));
             float lx = lo.x + is[3] * ld.x, ly = lo.y + is[3] * ld.y, lz = lo.z + is[3] * ld.z;

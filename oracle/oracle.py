@@ -40,7 +40,7 @@ class OracleScene(C.Structure):
         ("optical", C.c_void_p), ("icdf", C.c_void_p), ("icdf_w", C.c_int), ("icdf_h", C.c_int), ("hd_factor", C.c_int),
         ("max_bounce", C.c_int), ("max_time", C.c_float), ("tmin", C.c_float), ("tmin0", C.c_float),
         ("eps0_mask", C.c_uint), ("hit_mask", C.c_uint), ("polish", C.c_int),
-        ("pair_bbox", C.c_void_p),
+        ("pair_bbox", C.c_void_p), ("plan", C.c_void_p),
     ]
 
 
@@ -57,10 +57,11 @@ def lib() -> C.CDLL:
         L.oracle_simulate.argtypes = [C.POINTER(OracleScene), C.c_void_p, C.c_int, C.c_longlong, C.c_longlong,
                                       C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_csg_scan.restype = C.c_int
-        L.oracle_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p,
-                                      C.c_int, C.c_int]
+        L.oracle_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong,
+                                      C.c_void_p, C.c_int, C.c_int]
         L.oracle_csg_scan_t64.restype = C.c_int
-        L.oracle_csg_scan_t64.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p]
+        L.oracle_csg_scan_t64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong,
+                                          C.c_void_p]
         L.oracle_csg_action.restype = C.c_int
         L.oracle_csg_action.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
         L.oracle_tex2d_f1.restype = C.c_float
@@ -146,12 +147,13 @@ class Scene:
         self.icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
         nb, nwl = self.bnd.shape[0], self.bnd.shape[3]
         self.pair_bbox = pair_world_boxes(geom, self.pin, self.pnode) if cull else None
+        self.plan = _plan(geom.get("plan"))
         self.s = OracleScene(
             _p(self.node), _p(self.itra), _p(self.inst_inv), _p(self.pin), _p(self.pnode), _p(self.pgb), _p(self.pid),
             len(self.pin), _p(self.bnd), nwl, nb * 8, float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)),
             _p(self.optical), _p(self.icdf), 0 if self.icdf is None else self.icdf.shape[1],
             0 if self.icdf is None else self.icdf.shape[0], int(phys.get("hd_factor", 20)),
-            max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox))
+            max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox), _p(self.plan))
 
     def simulate(self, gs: np.ndarray, uniforms: np.ndarray, first: int = 0):
         gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
@@ -176,23 +178,30 @@ class Scene:
         return hits, grad, err
 
 
-def csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, use_double: bool = False, polish: bool = False):
+def _plan(plan):
+    return np.ascontiguousarray(plan if plan is not None and len(plan) else np.zeros((1, 4)), np.float32)
+
+
+def csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, use_double: bool = False, polish: bool = False,
+             plan=None):
     node = np.ascontiguousarray(node, np.float32)
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    pl = _plan(plan)
     rays = np.ascontiguousarray(rays, np.float32)
     n = rays.shape[1]
     out = np.zeros((n, 4), np.float32)
-    err = lib().oracle_csg_scan(_p(node), _p(itra), root, tmin, _p(rays), n, _p(out), int(use_double), int(polish))
+    err = lib().oracle_csg_scan(_p(node), _p(itra), _p(pl), root, tmin, _p(rays), n, _p(out), int(use_double), int(polish))
     return out, err
 
 
-def csg_scan_t64(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0):
+def csg_scan_t64(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, plan=None):
     node = np.ascontiguousarray(node, np.float32)
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    pl = _plan(plan)
     rays = np.ascontiguousarray(rays, np.float32)
     n = rays.shape[1]
     t = np.zeros((n,), np.float64)
-    err = lib().oracle_csg_scan_t64(_p(node), _p(itra), root, tmin, _p(rays), n, _p(t))
+    err = lib().oracle_csg_scan_t64(_p(node), _p(itra), _p(pl), root, tmin, _p(rays), n, _p(t))
     return t, err
 
 
@@ -231,49 +240,91 @@ def ref_merge_gpu(records: np.ndarray, select_flagmask: int = 0xFFFFFFFF, time_w
     return out[: no.value]
 
 
-def ref_csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, nthread: int = 0):
+def ref_csg_scan(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, nthread: int = 0, plan=None):
     L = C.CDLL(REF_CSG)
     L.ref_csg_scan.restype = C.c_int
-    L.ref_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p, C.c_int]
+    L.ref_csg_scan.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p,
+                               C.c_int]
     node = np.ascontiguousarray(node, np.float32)
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    pl = _plan(plan)
     rays = np.ascontiguousarray(rays, np.float32)
     n = rays.shape[1]
     out = np.zeros((n, 4), np.float32)
-    L.ref_csg_scan(_p(node), _p(itra), root, tmin, _p(rays), n, _p(out), nthread or (os.cpu_count() or 1))
+    L.ref_csg_scan(_p(node), _p(itra), _p(pl), root, tmin, _p(rays), n, _p(out), nthread or (os.cpu_count() or 1))
     return out
 
 
-def ref_scan_gpu(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0):
+def ref_leaf_extra_scan(typecode: int, q0q1, rays: np.ndarray, tmin: float = 0.0):
+    """one slab / infcylinder / disc leaf through the reference's own leaf function (CPU)"""
+    L = C.CDLL(REF_CSG)
+    L.ref_leaf_extra_scan.restype = C.c_int
+    L.ref_leaf_extra_scan.argtypes = [C.c_int, C.c_void_p, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p]
+    q = np.ascontiguousarray(np.asarray(q0q1, np.float32).reshape(8))
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[1]
+    out = np.zeros((n, 4), np.float32)
+    if L.ref_leaf_extra_scan(typecode, _p(q), tmin, _p(rays), n, _p(out)) != 0:
+        raise ValueError(f"typecode {typecode} is not a slab, infcylinder or disc")
+    return out
+
+
+def ref_scan_gpu(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, plan=None):
     L = C.CDLL(REF_SIM)
     L.ref_scan_run.restype = C.c_int
-    L.ref_scan_run.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_longlong, C.c_void_p]
+    L.ref_scan_run.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p,
+                               C.c_longlong, C.c_void_p]
     node = np.ascontiguousarray(node, np.float32)
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
     rays = np.ascontiguousarray(rays, np.float32)
     n = rays.shape[1]
     out = np.zeros((n, 4), np.float32)
-    rc = L.ref_scan_run(_p(node), len(node), _p(itra), len(itra), root, tmin, _p(rays), n, _p(out))
+    pl = _plan(plan)
+    rc = L.ref_scan_run(_p(node), len(node), _p(itra), len(itra), _p(pl), len(pl), root, tmin, _p(rays), n, _p(out))
     if rc != 0:
         raise RuntimeError(f"ref_scan_run failed {rc}")
     return out
 
 
+# gencodes the driver gives the reference's qsim::generate_photon everything for
+# (qudarap/qsim.h:2532-2561): torch, Cerenkov and scintillation
+REF_GENCODES = (6, 15, 16)
+# torch types the reference's storch::generate fills a photon for (sysrap/storchtype.h:8-18,
+# sysrap/storch.h:207-470): disc, line, point, circle, rectangle, sphere_marsaglia, sphere
+REF_TORCH_TYPES = range(1, 8)
+
+
+def ref_genstep_check(gs: np.ndarray) -> None:
+    """refuse gensteps the reference's device code is not given the means to generate: a torch
+    genstep of another type, or without a wavelength, leaves the photon's wavelength at zero, and
+    qsim::generate_photon then samples the Planck texture (qudarap/qsim.h:2541-2544), which this
+    driver does not set up"""
+    gi = gs.view(np.int32)
+    for k in range(len(gs)):
+        code = int(gi[k, 0, 0])
+        if code not in REF_GENCODES:
+            raise ValueError(f"genstep {k}: gencode {code} is not one the reference driver generates")
+        if code == 6 and (int(gi[k, 5, 3]) not in REF_TORCH_TYPES or not gs[k, 3, 3] > 0.0):
+            raise ValueError(f"genstep {k}: torch type {int(gi[k, 5, 3])} / wavelength {gs[k, 3, 3]} is not a reference torch genstep")
+
+
 def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 0, seed: int = 0, skip: int = 100000,
                      max_bounce: int = 31, max_time: float = 1e27, tmin: float = 0.05, tmin0: float = 0.05,
-                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10):
-    """run the reference's qsim on the GPU through ref_sim.cu; returns photon (N,4,4), seq (N,2,2)"""
+                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10, record: bool = False):
+    """run the reference's qsim on the GPU through ref_sim.cu; returns photon (N,4,4), seq (N,2,2)
+    and, with ``record``, the per-point sphoton records (N,max_bounce+1,4,4) and per-trace prd
+    (N,max_bounce+1,2,4) that the reference's sctx::point / sctx::trace write"""
     L = C.CDLL(REF_SIM)
     f = L.ref_sim_run
     f.restype = C.c_int
-    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                   C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
                   C.c_void_p, C.c_int, C.c_int, C.c_int,
                   C.c_ulonglong, C.c_ulonglong, C.c_int,
                   C.c_void_p, C.c_int, C.c_longlong,
                   C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint,
-                  C.c_void_p, C.c_void_p]
+                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     node = np.ascontiguousarray(geom["node"], np.float32)
     itra = geom.get("itra")
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
@@ -283,13 +334,20 @@ def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 
     icdf = phys.get("icdf")
     icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
     gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
+    ref_genstep_check(gs)
     N = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
     photon = np.zeros((N, 4, 4), np.float32)
     seq = np.zeros((N, 2, 2), np.uint64)
-    rc = f(_p(node), len(node), _p(itra), len(itra), _p(inv), len(inv), _p(pin), _p(pnode), _p(pgb), _p(pid), len(pin),
+    max_record = max_bounce + 1 if record else 0
+    rec = np.zeros((N, max_record, 4, 4), np.float32) if record else None
+    prd = np.zeros((N, max_record, 2, 4), np.float32) if record else None
+    pl = _plan(geom.get("plan"))
+    rc = f(_p(node), len(node), _p(itra), len(itra), _p(pl), len(pl), _p(inv), len(inv), _p(pin), _p(pnode), _p(pgb), _p(pid),
+           len(pin),
            _p(bnd), bnd.shape[0], bnd.shape[3], float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)), _p(optical),
            _p(icdf), 0 if icdf is None else icdf.shape[1], 0 if icdf is None else icdf.shape[0], int(phys.get("hd_factor", 20)),
-           seed, skip, event_index, _p(gs), len(gs), N, max_bounce, max_time, tmin, tmin0, eps0_mask, _p(photon), _p(seq))
+           seed, skip, event_index, _p(gs), len(gs), N, max_bounce, max_time, tmin, tmin0, eps0_mask, _p(photon), _p(seq),
+           _p(rec) if record else None, _p(prd) if record else None, max_record)
     if rc != 0:
         raise RuntimeError(f"ref_sim_run failed {rc}")
-    return photon, seq
+    return (photon, seq, rec, prd) if record else (photon, seq)

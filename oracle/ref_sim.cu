@@ -55,7 +55,10 @@ __device__ void ref_trace(const RefScene& S, const float3& o, const float3& d, f
         float3 ld = m->right_multiply(d, 0.f);
         float4 is = make_float4(0.f, 0.f, 0.f, 0.f);
         bool v = intersect_prim(is, S.node + S.pair_node[k], S.plan, S.itra, tmin, lo, ld, false);
-        if (v && is.w < best) {
+        // OptiX ignores a reported intersection outside the ray's [tmin, tmax] interval; a leaf
+        // can report valid with t = 0 (a convexpolyhedron wholly behind the ray leaves isect
+        // unset, CSG/csg_intersect_leaf_convexpolyhedron.h:85-101), which that rule drops
+        if (v && is.w >= tmin && is.w < best) {
             best = is.w; bi = k; bis = is;
             const float3 lpos = lo + is.w * ld;
             blc = normalize_cost(lpos);
@@ -102,6 +105,7 @@ __global__ void ref_simulate_k(qsim* sim, sevent* evt, RefScene S, float tmin, f
         if (prd.boundary() == 0xffffu) break;
         float3* normal = prd.normal();
         *normal = normalize(*normal);
+        ctx.trace(bounce);
         command = sim->propagate(bounce, rng, ctx);
         bounce++;
         ctx.point(bounce);
@@ -119,14 +123,14 @@ __global__ void ref_curand_init_k(unsigned long long seed, int n, XORWOW* states
 }
 
 // reference CSG on the device for the scan comparison
-__global__ void ref_scan_k(const CSGNode* node, const qat4* itra, float tmin, const float* rays, long long n, float4* out)
+__global__ void ref_scan_k(const CSGNode* node, const float4* plan, const qat4* itra, float tmin, const float* rays, long long n, float4* out)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 o = make_float3(rays[i], rays[n + i], rays[2 * n + i]);
     float3 d = make_float3(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]);
     float4 is = make_float4(0.f, 0.f, 0.f, 0.f);
-    bool v = intersect_prim(is, node, nullptr, itra, tmin, o, d, false);
+    bool v = intersect_prim(is, node, plan, itra, tmin, o, d, false);
     out[i] = v ? is : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -170,15 +174,18 @@ static cudaTextureObject_t tex_f1(const float* data, int w, int h, cudaArray_t* 
 }
 
 extern "C" int ref_sim_run(
-    const float* node, int nn, const float* itra, int nt, const float* inst_inv, int ni,
+    const float* node, int nn, const float* itra, int nt, const float* plan, int npl, const float* inst_inv, int ni,
     const int* pair_inst, const int* pair_node, const unsigned* pair_gpbd, const unsigned* pair_iiid, int npair,
     const float* bnd, int nb, int nwl, float nm0, float nms, const unsigned* optical,
     const float* icdf, int icdf_w, int icdf_h, int hd_factor,
     unsigned long long seed, unsigned long long skip, int event_index,
     const float* gs, int G, long long N,
     int max_bounce, float max_time, float tmin, float tmin0, unsigned eps0mask,
-    float* photon_out, unsigned long long* seq_out)
+    float* photon_out, unsigned long long* seq_out, float* record_out, float* prd_out, int max_record)
 {
+    // record_out (N, max_record, 4, 4) sphoton per point and prd_out (N, max_record, 2, 4) quad2 per
+    // trace, as the reference's sctx::point / sctx::trace write them; max_record >= max_bounce + 1
+    if (record_out && max_record < max_bounce + 1) return -3;
     std::vector<int> seed_h((size_t)N);
     long long k = 0;
     for (int g = 0; g < G; g++) {
@@ -189,7 +196,7 @@ extern "C" int ref_sim_run(
 
     RefScene S;
     S.node = up((const CSGNode*)node, (size_t)nn);
-    S.plan = nullptr;
+    S.plan = npl > 0 ? up((const float4*)plan, (size_t)npl) : nullptr;
     S.itra = up((const qat4*)itra, (size_t)nt);
     S.inst_inv = up((const qat4*)inst_inv, (size_t)ni);
     S.pair_inst = up(pair_inst, (size_t)npair);
@@ -245,6 +252,15 @@ extern "C" int ref_sim_run(
     cudaMalloc(&ev_h.photon, sizeof(sphoton) * (N > 0 ? N : 1));
     cudaMalloc(&ev_h.seq, sizeof(sseq) * (N > 0 ? N : 1));
     cudaMemset(ev_h.seq, 0, sizeof(sseq) * (N > 0 ? N : 1));
+    const size_t nrec = record_out && N > 0 ? (size_t)N * (size_t)max_record : 0;
+    if (nrec) {
+        ev_h.max_record = max_record;
+        ev_h.max_prd = max_record;
+        cudaMalloc(&ev_h.record, sizeof(sphoton) * nrec);
+        cudaMalloc(&ev_h.prd, sizeof(quad2) * nrec);
+        cudaMemset(ev_h.record, 0, sizeof(sphoton) * nrec);
+        cudaMemset(ev_h.prd, 0, sizeof(quad2) * nrec);
+    }
     sevent* ev_d = up(&ev_h, 1);
 
     qsim sim_h; memset(&sim_h, 0, sizeof(sim_h));
@@ -257,10 +273,15 @@ extern "C" int ref_sim_run(
     if (e == cudaSuccess && N > 0) {
         cudaMemcpy(photon_out, ev_h.photon, sizeof(sphoton) * N, cudaMemcpyDeviceToHost);
         cudaMemcpy(seq_out, ev_h.seq, sizeof(sseq) * N, cudaMemcpyDeviceToHost);
+        if (nrec) {
+            cudaMemcpy(record_out, ev_h.record, sizeof(sphoton) * nrec, cudaMemcpyDeviceToHost);
+            cudaMemcpy(prd_out, ev_h.prd, sizeof(quad2) * nrec, cudaMemcpyDeviceToHost);
+        }
     }
+    if (nrec) { cudaFree(ev_h.record); cudaFree(ev_h.prd); }
     cudaDestroyTextureObject(t_bnd); cudaDestroyTextureObject(t_icdf);
     cudaFreeArray(a_bnd); cudaFreeArray(a_icdf);
-    cudaFree((void*)S.node); cudaFree((void*)S.itra); cudaFree((void*)S.inst_inv); cudaFree((void*)S.pair_inst);
+    cudaFree((void*)S.node); if (S.plan) cudaFree((void*)S.plan); cudaFree((void*)S.itra); cudaFree((void*)S.inst_inv); cudaFree((void*)S.pair_inst);
     cudaFree((void*)S.pair_node); cudaFree((void*)S.pair_gpbd); cudaFree((void*)S.pair_iiid);
     cudaFree(meta_d); cudaFree(bnd_h.optical); cudaFree(bnd_d); cudaFree(sc_d); cudaFree(base_d); cudaFree(ck_d);
     cudaFree(states); cudaFree(rng_d); cudaFree(ev_h.genstep); cudaFree(ev_h.seed); cudaFree(ev_h.photon);
@@ -268,17 +289,18 @@ extern "C" int ref_sim_run(
     return e == cudaSuccess ? 0 : -2;
 }
 
-extern "C" int ref_scan_run(const float* node, int nn, const float* itra, int nt, int root, float tmin,
+extern "C" int ref_scan_run(const float* node, int nn, const float* itra, int nt, const float* plan, int npl, int root, float tmin,
                             const float* rays, long long n, float* out)
 {
     const CSGNode* dn = up((const CSGNode*)node, (size_t)nn);
     const qat4* dt = up((const qat4*)itra, (size_t)nt);
+    const float4* dp = up((const float4*)plan, (size_t)npl);
     float* dr = up(rays, (size_t)(6 * n));
     float4* dout = nullptr;
     cudaMalloc(&dout, sizeof(float4) * (n > 0 ? n : 1));
-    if (n > 0) ref_scan_k<<<(unsigned)((n + 127) / 128), 128>>>(dn + root, dt, tmin, dr, n, dout);
+    if (n > 0) ref_scan_k<<<(unsigned)((n + 127) / 128), 128>>>(dn + root, dp, dt, tmin, dr, n, dout);
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess && n > 0) cudaMemcpy(out, dout, sizeof(float4) * n, cudaMemcpyDeviceToHost);
-    cudaFree((void*)dn); cudaFree((void*)dt); cudaFree(dr); cudaFree(dout);
+    cudaFree((void*)dn); cudaFree((void*)dt); cudaFree((void*)dp); cudaFree(dr); cudaFree(dout);
     return e == cudaSuccess ? 0 : -2;
 }

@@ -4,6 +4,10 @@ csg_scan_ref.npz : rays and the intersects computed by the reference's CSG inter
                    (CSG/csg_intersect_tree.h etc. compiled for the CPU by oracle/Makefile `ref`
                    into oracle/_ref/libref_csg.so) for the benchmark tree without the torus
                    (the reference intersector has no torus leaf) and for each leaf alone.
+csg_zoo_ref.npz  : the same for the further leaves (scenes.csg_leaf_zoo: cone, hyperboloid,
+                   convexpolyhedron with its plan table, phicut, halfspace) through the reference's
+                   tree intersector, and the slab / infcylinder / disc leaves one at a time through
+                   the reference's own leaf functions (compiled there only under CSG_EXTRA).
 
 Run from the repository root where the reference checkout is present:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -58,6 +62,32 @@ def main():
     out["leaf_rays"] = lr
     out["leaf_isect"] = np.stack([O.ref_csg_scan(B["node"], B["itra"], int(r), lr, 0.0) for r in out["leaf_roots"]])
     np.savez_compressed(os.path.join(ROOT, "tests", "golden", "csg_scan_ref.npz"), **out)
+    print({k: getattr(v, "shape", v) for k, v in out.items()})
+    zoo()
+
+
+EXTRA_LEAVES = (F.slab((0.6, 0.8, 0.0), -100.0, 150.0), F.infcylinder(120.0),
+                F.disc(50.0, 250.0, -10.0, 10.0), F.disc(0.0, 230.0, -5.0, 5.0, 20.0, -30.0))
+
+
+def zoo():
+    fd, prims = scenes.csg_leaf_zoo()
+    A = fd.arrays()
+    rays = scenes.scan_rays(2000, seed=13, half=400.0)
+    keep = [p for k, p in enumerate(prims) if k not in scenes.ZOO_EXTRA_PRIMS]
+    roots = np.array([int(A["prim"].view(np.int32)[p, 0, 1]) for p in keep], np.int32)
+    out = {"node": A["node"], "itra": A["itra"], "plan": A["plan"], "prims": np.array(keep, np.int32),
+           "roots": roots, "rays": rays}
+    out["isect"] = np.stack([O.ref_csg_scan(A["node"], A["itra"], int(r), rays, 0.0, plan=A["plan"]) for r in roots])
+    fe = F.Foundry()
+    ep = [fe.add_prim(n, 0) for n in EXTRA_LEAVES]
+    B = fe.arrays()
+    q = np.stack([B["node"][int(B["prim"].view(np.int32)[p, 0, 1])].reshape(-1)[:8] for p in ep])
+    tc = np.array([int(B["node"].view(np.uint32)[int(B["prim"].view(np.int32)[p, 0, 1]), 3, 2]) for p in ep], np.int32)
+    out["extra_q"] = q
+    out["extra_typecode"] = tc
+    out["extra_isect"] = np.stack([O.ref_leaf_extra_scan(int(t), qq, rays) for t, qq in zip(tc, q)])
+    np.savez_compressed(os.path.join(ROOT, "tests", "golden", "csg_zoo_ref.npz"), **out)
     print({k: getattr(v, "shape", v) for k, v in out.items()})
 
 

@@ -130,3 +130,49 @@ def test_scan_edge_cases(notorus_engine):
     t, _ = O.csg_scan(A["node"], A["itra"], int(A["prim"].view(np.int32)[p, 0, 1]), rays, 0.0)
     np.testing.assert_array_equal(out[:, 3] > 0, t[:, 3] > 0)
     np.testing.assert_allclose(out[:, 3], t[:, 3], rtol=1e-6)
+
+
+@pytest.fixture(scope="module")
+def zoo_engine(cuda):
+    from opticks_b200 import engine as E
+    fd, prims = scenes.csg_leaf_zoo()
+    _, lib, _, _ = scenes.sphere_in_box(1)
+    eng = E.Engine(fd.arrays(), lib.arrays(), E.default_config(max_photon=1024))
+    yield eng, fd.arrays(), prims
+    eng.close()
+
+
+def test_scan_further_leaves_match_reference_golden(zoo_engine):
+    """cone, hyperboloid, convexpolyhedron (plan table), phicut, halfspace trees against the
+    intersects of the reference's own tree intersector"""
+    eng, A, prims = zoo_engine
+    g = np.load(os.path.join(ROOT, "tests", "golden", "csg_zoo_ref.npz"))
+    np.testing.assert_array_equal(A["node"], g["node"])
+    for k, p in enumerate(g["prims"]):
+        ref = g["isect"][k]
+        out = eng.scan(int(p), g["rays"], 0.0)
+        hr, ho = ref[:, 3] > 0, out[:, 3] > 0
+        mism = int((hr != ho).sum())
+        assert mism <= 2, (int(p), mism)
+        both = hr & ho
+        np.testing.assert_allclose(out[both, 3], ref[both, 3], rtol=1e-4, atol=1e-4, err_msg=f"prim {int(p)}")
+        np.testing.assert_allclose(out[both, :3], ref[both, :3], atol=2e-5, err_msg=f"prim {int(p)}")
+
+
+def test_scan_extra_leaf_trees_match_oracle(zoo_engine):
+    """trees holding slab / infcylinder / disc leaves against the oracle (pinned leaf by leaf to
+    the reference's leaf functions)"""
+    eng, A, prims = zoo_engine
+    rays = scenes.scan_rays(1 << 15, seed=21, half=400.0)
+    for k in scenes.ZOO_EXTRA_PRIMS:
+        p = prims[k]
+        root = int(A["prim"].view(np.int32)[p, 0, 1])
+        ref, err = O.csg_scan(A["node"], A["itra"], root, rays, 0.0, plan=A["plan"])
+        assert err == 0
+        out = eng.scan(p, rays, 0.0)
+        hr, ho = ref[:, 3] > 0, out[:, 3] > 0
+        assert hr.sum() > 500, k
+        assert int((hr != ho).sum()) <= 3, k
+        both = hr & ho
+        np.testing.assert_allclose(out[both, 3], ref[both, 3], rtol=1e-4, atol=1e-4, err_msg=f"zoo prim {k}")
+        np.testing.assert_allclose(out[both, :3], ref[both, :3], atol=2e-5, err_msg=f"zoo prim {k}")

@@ -129,3 +129,82 @@ def test_oracle_physics_invariants_sphere_in_box():
 def test_oracle_reports_exhausted_uniform_stream():
     ph, seq, err = _c1_oracle(n=200, K=3)
     assert err & 2
+
+
+ZOO = os.path.join(ROOT, "tests", "golden", "csg_zoo_ref.npz")
+
+
+def one_leaf_node(q8, typecode):
+    """a one-node table holding leaf (q0, q1) with the given typecode, untransformed"""
+    node = np.zeros((1, 4, 4), np.float32)
+    node[0, :2] = np.asarray(q8, np.float32).reshape(2, 4)
+    node.view(np.uint32)[0, 3, 2] = typecode
+    return node
+
+
+def test_oracle_further_leaves_match_reference_golden_bit_exact():
+    g = np.load(ZOO)
+    fd, prims = scenes.csg_leaf_zoo()
+    A = fd.arrays()
+    np.testing.assert_array_equal(A["node"], g["node"])     # the fixture's geometry is the zoo's
+    np.testing.assert_array_equal(A["plan"], g["plan"])
+    for k, root in enumerate(g["roots"]):
+        out, err = O.csg_scan(g["node"], g["itra"], int(root), g["rays"], 0.0, plan=g["plan"])
+        ref = g["isect"][k]
+        assert err == 0
+        assert (ref[:, 3] > 0).sum() > 50, k
+        np.testing.assert_array_equal(out, ref, err_msg=f"zoo prim {int(g['prims'][k])}")
+
+
+def test_oracle_extra_leaves_match_reference_leaf_functions_bit_exact():
+    g = np.load(ZOO)
+    for k, tc in enumerate(g["extra_typecode"]):
+        out, err = O.csg_scan(one_leaf_node(g["extra_q"][k], int(tc)), None, 0, g["rays"], 0.0)
+        ref = g["extra_isect"][k]
+        assert err == 0
+        assert (ref[:, 3] > 0).sum() > 50, k
+        np.testing.assert_array_equal(out, ref, err_msg=f"typecode {int(tc)}")
+
+
+@pytest.mark.skipif(not O.have_ref_csg(), reason="reference CPU build absent")
+def test_oracle_further_leaves_match_live_reference_on_fresh_rays():
+    fd, prims = scenes.csg_leaf_zoo()
+    A = fd.arrays()
+    rays = scenes.scan_rays(20000, seed=5, half=400.0)
+    for k, p in enumerate(prims):
+        if k in scenes.ZOO_EXTRA_PRIMS:
+            continue
+        root = int(A["prim"].view(np.int32)[p, 0, 1])
+        ref = O.ref_csg_scan(A["node"], A["itra"], root, rays, 0.0, plan=A["plan"])
+        out, err = O.csg_scan(A["node"], A["itra"], root, rays, 0.0, plan=A["plan"])
+        assert err == 0
+        np.testing.assert_array_equal(out, ref, err_msg=f"zoo prim {k}")
+
+
+def test_convexpolyhedron_cube_equals_box():
+    # a convexpolyhedron of the six cube planes is the box leaf of the same size
+    cube = F.Foundry()
+    p0 = cube.add_prim(F.convexpolyhedron(F.cube_planes(150.0), (-150, -150, -150, 150, 150, 150)), 0)
+    p1 = cube.add_prim(F.box3(300.0, 300.0, 300.0), 0)
+    A = cube.arrays()
+    rays = scenes.scan_rays(5000, seed=17, half=400.0)
+    r0, r1 = (int(A["prim"].view(np.int32)[p, 0, 1]) for p in (p0, p1))
+    a, _ = O.csg_scan(A["node"], A["itra"], r0, rays, 0.0, plan=A["plan"])
+    b, _ = O.csg_scan(A["node"], A["itra"], r1, rays, 0.0, plan=A["plan"])
+    assert ((a[:, 3] > 0) != (b[:, 3] > 0)).sum() == 0
+    np.testing.assert_allclose(a[:, 3], b[:, 3], rtol=1e-5, atol=1e-3)
+
+
+def test_reference_driver_refuses_gensteps_it_cannot_generate():
+    # checked on the host before any launch: an engine-only torch type, a torch genstep without a
+    # wavelength and an unknown gencode are refused; reference torch types pass
+    ok = scenes.torch_genstep(10, type_=scenes.T_SPHERE)[None]
+    O.ref_genstep_check(ok)
+    for bad in (scenes.torch_genstep(10, type_=scenes.T_SPHERE_RANDPOL)[None],
+                scenes.torch_genstep(10, wavelength=0.0, type_=scenes.T_SPHERE)[None]):
+        with pytest.raises(ValueError):
+            O.ref_genstep_check(bad)
+    odd = ok.copy()
+    odd.view(np.int32)[0, 0, 0] = 99
+    with pytest.raises(ValueError):
+        O.ref_genstep_check(odd)
