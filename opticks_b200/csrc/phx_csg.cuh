@@ -514,7 +514,7 @@ PHX_COLD float4 leaf_convexpolyhedron(const float4 q0, const float4* __restrict_
     const float INF = __int_as_float(0x7f800000);
     float t0 = -INF, t1 = INF;
     float3 n0 = make_float3(0.f, 0.f, 0.f), n1 = make_float3(0.f, 0.f, 0.f);
-    for (unsigned i = 0; i < planeNum && i < 256u; i++) {
+    for (unsigned i = 0; i < planeNum; i++) {       // planeIdx + planeNum <= num_plan, checked at phx_create
         const float4 pl = __ldg(plan + planeIdx + i);
         const float3 n = make_float3(pl.x, pl.y, pl.z);
         const float nd = dot(n, d);
@@ -529,9 +529,14 @@ PHX_COLD float4 leaf_convexpolyhedron(const float4 q0, const float4* __restrict_
     if (t0 < t1) {
         if (t0 > t_min) isect = make_float4(n0.x, n0.y, n0.z, t0);
         else if (t1 > t_min) isect = make_float4(n1.x, n1.y, n1.z, t1);
+        else isect.w = -0.f;     // the reference reports this valid with isect unset: w = -0 carries that
     }
     return isect;
 }
+
+// a leaf's validity as the reference reports it: t > t_min, or the convexpolyhedron's valid
+// report with isect unset (w = -0).  Only the DISCONTIGUOUS list reads validity without t.
+PHX_D bool phx_leaf_valid(const float4& is, float t_min) { return is.w > t_min || __float_as_uint(is.w) == 0x80000000u; }
 
 // phi wedge between the half-planes at phi0 and phi1: q0 = (cos phi0, sin phi0, cos phi1, sin phi1);
 // a miss with an unbounded exit carries y = -0 (promoted to EXIT by the tree evaluator)
@@ -688,6 +693,7 @@ PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __res
         case PHX_CSG_DISC:     isect = leaf_disc(q0, q1, t_min, origin, direction); valid = isect.w > t_min; break;
         default: break;
     }
+    valid = valid || __float_as_uint(isect.w) == 0x80000000u;
     if (valid && q) {
         float3 n = xform_col(q, make_float3(isect.x, isect.y, isect.z), 0.f);
         isect.x = n.x; isect.y = n.y; isect.z = n.z;
@@ -711,6 +717,142 @@ PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min
 PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
 {
     return fabsf(ise.w) > tmin ? (ise.x * d.x + ise.y * d.y + ise.z * d.z < 0.f ? PHX_STATE_ENTER : PHX_STATE_EXIT) : PHX_STATE_MISS;
+}
+
+// ---------------------------------------------------------------- list nodes
+// CSG/csg_intersect_node.h:392-945.  A list header (typecode CONTIGUOUS, DISCONTIGUOUS or
+// OVERLAP; q0.u.x = subNum, q0.u.y = subOffset) names subNum leaves at root + subOffset + i,
+// root being the prim's first node (a list is a prim root, or a leaf of a boolean tree whose
+// sub-nodes follow the complete binary tree).  Ranges are checked at phx_create.
+#define PHX_LIST_MAX_ENTER 8
+
+// union of leaves that may touch or overlap: the farthest exit reachable through a chain of
+// overlapping constituents (CSG/csg_intersect_node.h:392-600)
+template <bool POLISH>
+PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
+                                     const float3& d, unsigned& err)
+{
+    float4 nearest_enter = make_float4(0.f, 0.f, 0.f, PHX_RT_MAX);
+    float4 farthest_exit = make_float4(0.f, 0.f, 0.f, t_min);
+    int exit_count = 0;
+    for (int i = 0; i < num_sub; i++) {
+        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        if (!phx_leaf_valid(s, t_min)) continue;
+        const int st = phx_classify(s, d, t_min);
+        if (st == PHX_STATE_ENTER) { if (s.w < nearest_enter.w) nearest_enter = s; }
+        else if (st == PHX_STATE_EXIT) exit_count += 1;
+    }
+    if (exit_count == 0) {
+        const bool valid = nearest_enter.w > t_min && nearest_enter.w < PHX_RT_MAX;
+        if (valid) isect = nearest_enter;
+        return valid;
+    }
+    int enter_count = 0;
+    float enter[PHX_LIST_MAX_ENTER];
+    int aux[PHX_LIST_MAX_ENTER];
+    for (int i = 0; i < num_sub; i++) {
+        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        if (!phx_leaf_valid(s, t_min)) continue;
+        const int st = phx_classify(s, d, t_min);
+        if (st == PHX_STATE_ENTER) {
+            // the reference's arrays hold 8 enters; more is undefined there: flag and drop
+            if (enter_count >= PHX_LIST_MAX_ENTER) { err |= PHX_STATUS_CSG_STACK; continue; }
+            aux[enter_count] = i;
+            enter[enter_count] = s.w;
+            enter_count += 1;
+        } else if (st == PHX_STATE_EXIT) {
+            exit_count += 1;
+            if (s.w > farthest_exit.w) farthest_exit = s;
+        }
+    }
+    // stable insertion sort of the enters by distance
+    for (int i = 1; i < enter_count; i++) {
+        const float ke = enter[i];
+        const int ka = aux[i];
+        int j = i - 1;
+        while (j >= 0 && enter[j] > ke) { enter[j + 1] = enter[j]; aux[j + 1] = aux[j]; j--; }
+        enter[j + 1] = ke;
+        aux[j + 1] = ka;
+    }
+    for (int i = 0; i < enter_count; i++) {
+        const float tminAdvanced = enter[i] + PHX_CSG_PROPAGATE_EPSILON;
+        if (tminAdvanced < farthest_exit.w) {
+            const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + aux[i], tminAdvanced, o, d);
+            if (phx_leaf_valid(s, tminAdvanced) && phx_classify(s, d, tminAdvanced) == PHX_STATE_EXIT) {
+                exit_count += 1;
+                if (s.w > farthest_exit.w) farthest_exit = s;
+            }
+        }
+    }
+    const bool valid = exit_count > 0 && farthest_exit.w > t_min;
+    if (valid) isect = farthest_exit;
+    return valid;
+}
+
+// union of disjoint leaves: the closest valid report (CSG/csg_intersect_node.h:654-700)
+template <bool POLISH>
+PHX_D bool intersect_list_discontiguous(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
+                                        const float3& d)
+{
+    float4 closest = make_float4(0.f, 0.f, 0.f, PHX_RT_MAX);
+    for (int i = 0; i < num_sub; i++) {
+        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        if (phx_leaf_valid(s, t_min) && s.w < closest.w) closest = s;
+    }
+    const bool valid = closest.w < PHX_RT_MAX;
+    if (valid) isect = closest;
+    return valid;
+}
+
+// intersection of leaves: farthest enter or nearest exit when every leaf is entered or exited
+// and the farthest enter precedes the nearest exit (CSG/csg_intersect_node.h:819-910)
+template <bool POLISH>
+PHX_D bool intersect_list_overlap(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
+                                  const float3& d)
+{
+    float4 farthest_enter = make_float4(0.f, 0.f, 0.f, t_min);
+    float4 nearest_exit = make_float4(0.f, 0.f, 0.f, PHX_RT_MAX);
+    int enter_count = 0, exit_count = 0;
+    for (int i = 0; i < num_sub; i++) {
+        float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        if (!phx_leaf_valid(s, t_min)) continue;
+        const int st = phx_classify(s, d, t_min);
+        if (st == PHX_STATE_ENTER) {
+            enter_count += 1;
+            if (s.w > farthest_enter.w) farthest_enter = s;
+            const float tminAdvanced = s.w + PHX_CSG_PROPAGATE_EPSILON;
+            s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, tminAdvanced, o, d);
+            if (phx_leaf_valid(s, tminAdvanced) && phx_classify(s, d, tminAdvanced) == PHX_STATE_EXIT) {
+                exit_count += 1;
+                if (s.w < nearest_exit.w) nearest_exit = s;
+            }
+        } else if (st == PHX_STATE_EXIT) {
+            exit_count += 1;
+            if (s.w < nearest_exit.w) nearest_exit = s;
+        }
+    }
+    const bool overlap_all = farthest_enter.w < nearest_exit.w && max(enter_count, exit_count) == num_sub;
+    if (overlap_all) {
+        if (farthest_enter.w > t_min && farthest_enter.w < PHX_RT_MAX) { isect = farthest_enter; return true; }
+        if (nearest_exit.w > t_min && nearest_exit.w < PHX_RT_MAX) { isect = nearest_exit; return true; }
+    }
+    return false;
+}
+
+// list header ni, sub-nodes relative to the prim root; isect is untouched on a miss
+template <bool POLISH>
+PHX_D bool intersect_list(float4& isect, const PhxCsgCtx& g, int ni, int root, unsigned typecode, float t_min, const float3& o,
+                          const float3& d, unsigned& err)
+{
+    const float4 q0 = __ldg(g.node + 4 * ni);
+    const int num_sub = (int)__float_as_uint(q0.x);
+    const int first = root + (int)__float_as_uint(q0.y);
+    switch (typecode) {
+        case PHX_CSG_CONTIGUOUS: return intersect_list_contiguous<POLISH>(isect, g, first, num_sub, t_min, o, d, err);
+        case PHX_CSG_DISCONTIGUOUS: return intersect_list_discontiguous<POLISH>(isect, g, first, num_sub, t_min, o, d);
+        case PHX_CSG_OVERLAP: return intersect_list_overlap<POLISH>(isect, g, first, num_sub, t_min, o, d);
+        default: return false;
+    }
 }
 
 #define PHX_POSTORDER_NEXT(i, elev) (((i) & 1u) ? (i) >> 1 : ((i) << (elev)) + (1u << (elev)))
@@ -765,7 +907,7 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
         const unsigned op = __float_as_uint(__ldg(g.node + 4 * root + 3).z);
         const unsigned tl = __float_as_uint(__ldg(g.node + 4 * (root + 1) + 3).z);
         const unsigned tr = __float_as_uint(__ldg(g.node + 4 * (root + 2) + 3).z);
-        if (op >= PHX_CSG_UNION && op <= PHX_CSG_DIFFERENCE && tl >= PHX_CSG_NODE && tr >= PHX_CSG_NODE)
+        if (op >= PHX_CSG_UNION && op <= PHX_CSG_DIFFERENCE && tl >= PHX_CSG_LEAF && tr >= PHX_CSG_LEAF)
             return intersect_tree3<POLISH>(isect, g, root, op, t_min, o, d, err);
     }
 #endif
@@ -792,8 +934,9 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
             const unsigned typecode = __float_as_uint(__ldg(g.node + 4 * ni + 3).z);
             if (typecode == PHX_CSG_ZERO) { nodeIdx = PHX_POSTORDER_NEXT(nodeIdx, elevation); continue; }
             if (typecode >= PHX_CSG_NODE) {
-                float4 nd_isect;
-                intersect_leaf<POLISH>(nd_isect, g, ni, tmin, o, d, err);
+                float4 nd_isect = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (typecode < PHX_CSG_LEAF) intersect_list<POLISH>(nd_isect, g, ni, root, typecode, tmin, o, d, err);
+                else intersect_leaf<POLISH>(nd_isect, g, ni, tmin, o, d, err);
                 nd_isect.w = copysignf(nd_isect.w, nodeIdx % 2u == 0u ? -1.f : 1.f);
                 if (sp >= PHX_CSG_STACK - 1) { ierr |= PHX_CSG_ERR_OVERFLOW; break; }
                 stk[++sp] = nd_isect;
@@ -855,7 +998,7 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
     return isect.w > 0.f;
 }
 
-// one prim: leaf at the root, or a boolean tree.  POLISH selects the FP64 root polish at
+// one prim: leaf at the root, a boolean tree, or a list.  POLISH selects the FP64 root polish at
 // compile time so the default path keeps the reference's FP32 expression structure.
 template <bool POLISH>
 PHX_D bool intersect_prim(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
@@ -864,5 +1007,5 @@ PHX_D bool intersect_prim(float4& isect, const PhxCsgCtx& g, int root, float t_m
     isect = make_float4(0.f, 0.f, 0.f, 0.f);
     if (typecode >= PHX_CSG_LEAF) return intersect_leaf<POLISH>(isect, g, root, t_min, o, d, err);
     if (typecode < PHX_CSG_NODE) return intersect_tree<POLISH>(isect, g, root, t_min, o, d, err);
-    return false;
+    return intersect_list<POLISH>(isect, g, root, root, typecode, t_min, o, d, err);
 }

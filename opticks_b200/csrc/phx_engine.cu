@@ -554,6 +554,63 @@ static PhxSph node_sphere(const phx_geometry* geo, int no, int i, int num)
     return s;
 }
 
+// Every node a prim's intersector can reach, checked on the host so that no device read leaves
+// the node, itra or plan tables: the tree's complete binary range (root subNum), list sub-node
+// ranges, leaf gtransformIdx and convexpolyhedron plane ranges.  Returns nullptr or the problem.
+static const char* check_leaf_node(const phx_geometry* geo, int ni)
+{
+    const float* q = geo->node + 16 * (size_t)ni;
+    uint32_t tc, tw;
+    memcpy(&tc, q + 14, 4);
+    memcpy(&tw, q + 15, 4);
+    const uint32_t g = tw & 0x7fffffffu;
+    if (g > 0 && ((int64_t)g > geo->num_itra || !geo->itra)) return "leaf gtransformIdx beyond the itra table";
+    if (tc == PHX_CSG_CONVEXPOLYHEDRON) {
+        uint32_t idx, num;
+        memcpy(&idx, q + 0, 4);
+        memcpy(&num, q + 1, 4);
+        if ((int64_t)idx + (int64_t)num > (int64_t)std::max(0, geo->num_plan) || (num > 0 && !geo->plan))
+            return "convexpolyhedron planes beyond the plan table";
+    }
+    return nullptr;
+}
+
+static const char* check_list_node(const phx_geometry* geo, int ni, int root)
+{
+    const float* q = geo->node + 16 * (size_t)ni;
+    uint32_t num, off;
+    memcpy(&num, q + 0, 4);
+    memcpy(&off, q + 1, 4);
+    if ((int64_t)root + (int64_t)off + (int64_t)num > geo->num_node) return "list sub-nodes beyond the node table";
+    for (uint32_t i = 0; i < num; i++) {
+        const char* m = check_leaf_node(geo, root + (int)(off + i));
+        if (m) return m;
+    }
+    return nullptr;
+}
+
+static const char* check_prim_nodes(const phx_geometry* geo, int root)
+{
+    uint32_t tc;
+    memcpy(&tc, geo->node + 16 * (size_t)root + 14, 4);
+    if (tc >= PHX_CSG_LEAF) return check_leaf_node(geo, root);
+    if (tc >= PHX_CSG_CONTIGUOUS && tc <= PHX_CSG_OVERLAP) return check_list_node(geo, root, root);
+    if (tc >= PHX_CSG_NODE) return nullptr;   // no intersector: always a miss
+    uint32_t num;
+    memcpy(&num, geo->node + 16 * (size_t)root, 4);    // subNum: complete binary tree size
+    if (num < 1 || num > 65535u || ((num + 1) & num) != 0) return "tree subNum is not 2^h - 1 (h 1..16)";
+    if ((int64_t)root + (int64_t)num > geo->num_node) return "tree nodes beyond the node table";
+    for (uint32_t i = 0; i < num; i++) {
+        const int ni = root + (int)i;
+        uint32_t t;
+        memcpy(&t, geo->node + 16 * (size_t)ni + 14, 4);
+        const char* m = t >= PHX_CSG_LEAF ? check_leaf_node(geo, ni)
+                      : t >= PHX_CSG_CONTIGUOUS && t <= PHX_CSG_OVERLAP ? check_list_node(geo, ni, root) : nullptr;
+        if (m) return m;
+    }
+    return nullptr;
+}
+
 // prim-frame sphere: the smaller of the box sphere and the tree sphere
 static PhxSph prim_sphere(const phx_geometry* geo, int p)
 {
@@ -735,6 +792,7 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
         int32_t nn;
         memcpy(&nn, geo->prim + 16 * p + 0, 4);
         if (no < 0 || no + std::max(nn, 1) > geo->num_node) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d node range out of bounds", p); }
+        if (const char* m = check_prim_nodes(geo, no)) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d: %s", p, m); }
     }
     std::vector<float> inv((size_t)std::max(1, geo->num_inst) * 16, 0.f);
     std::vector<PhxLeafInput> leaves;

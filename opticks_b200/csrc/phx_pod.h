@@ -68,6 +68,9 @@ enum {
     PHX_CSG_INTERSECTION = 2,
     PHX_CSG_DIFFERENCE = 3,
     PHX_CSG_NODE = 11,
+    PHX_CSG_CONTIGUOUS = 11,
+    PHX_CSG_DISCONTIGUOUS = 12,
+    PHX_CSG_OVERLAP = 13,
     PHX_CSG_LEAF = 101,
     PHX_CSG_SPHERE = 101,
     PHX_CSG_ZSPHERE = 103,

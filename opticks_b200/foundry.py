@@ -26,6 +26,9 @@ CSG_ZERO = 0
 CSG_UNION = 1
 CSG_INTERSECTION = 2
 CSG_DIFFERENCE = 3
+CSG_CONTIGUOUS = 11
+CSG_DISCONTIGUOUS = 12
+CSG_OVERLAP = 13
 CSG_SPHERE = 101
 CSG_ZSPHERE = 103
 CSG_CYLINDER = 105
@@ -42,6 +45,7 @@ CSG_HALFSPACE = 125
 UNBOUNDED = 1.0e9     # box half-extent given to unbounded leaves (halfspace, slab, phicut, infcylinder)
 
 OPS = {"union": CSG_UNION, "intersection": CSG_INTERSECTION, "difference": CSG_DIFFERENCE}
+LISTS = {"contiguous": CSG_CONTIGUOUS, "discontiguous": CSG_DISCONTIGUOUS, "overlap": CSG_OVERLAP}
 
 
 @dataclass
@@ -55,10 +59,15 @@ class Node:
     complement: bool = False
     bbox: tuple | None = None             # local (object frame) box of this leaf
     planes: np.ndarray | None = None      # convex polyhedron: (n,4) planes (unit normal, distance)
+    subs: list | None = None              # list node: its leaves
 
     @property
     def is_leaf(self) -> bool:
         return self.typecode >= 100
+
+    @property
+    def is_list(self) -> bool:
+        return CSG_CONTIGUOUS <= self.typecode <= CSG_OVERLAP
 
 
 def sphere(r, center=(0.0, 0.0, 0.0)):
@@ -144,6 +153,12 @@ def op(name, a: Node, b: Node) -> Node:
     return Node(OPS[name], left=a, right=b)
 
 
+def list_node(kind: str, leaves) -> Node:
+    """list node (CSGNode::ListHeader): "contiguous" (union of touching or overlapping leaves),
+    "discontiguous" (union of disjoint leaves) or "overlap" (intersection of the leaves)"""
+    return Node(LISTS[kind], subs=list(leaves))
+
+
 def translate(n: Node, tx, ty, tz) -> Node:
     m = np.eye(4)
     m[3, :3] = (tx, ty, tz)
@@ -152,7 +167,7 @@ def translate(n: Node, tx, ty, tz) -> Node:
 
 
 def _height(n: Node) -> int:
-    return 0 if n.is_leaf else 1 + max(_height(n.left), _height(n.right))
+    return 0 if n.is_leaf or n.is_list else 1 + max(_height(n.left), _height(n.right))
 
 
 def _bbox_transformed(bb, m):
@@ -167,6 +182,13 @@ def _tree_bbox(n: Node):
     """bbox of a subtree in the frame of its parent (the node's own transform applied)"""
     if n.is_leaf:
         return _bbox_transformed(n.bbox, n.transform)
+    if n.is_list:
+        bbs = [_tree_bbox(c) for c in n.subs]
+        if n.typecode == CSG_OVERLAP:
+            bb = tuple(max(b[k] for b in bbs) for k in range(3)) + tuple(min(b[k] for b in bbs) for k in range(3, 6))
+        else:
+            bb = tuple(min(b[k] for b in bbs) for k in range(3)) + tuple(max(b[k] for b in bbs) for k in range(3, 6))
+        return _bbox_transformed(bb, n.transform)
     a, b = _tree_bbox(n.left), _tree_bbox(n.right)
     if n.typecode == CSG_UNION:
         bb = tuple(min(a[k], b[k]) for k in range(3)) + tuple(max(a[k], b[k]) for k in range(3, 6))
@@ -200,8 +222,35 @@ class Foundry:
         self.itra.append(np.linalg.inv(np.asarray(m, dtype=np.float64)))
         return len(self.tran)   # 1-based gtransformIdx
 
+    def _node_row(self, n: Node | None, gm, boundary: int, index: int) -> np.ndarray:
+        q = np.zeros((4, 4), dtype=np.float32)
+        qu = q.view(np.uint32)
+        if n is None:
+            qu[3, 2] = CSG_ZERO
+        else:
+            if n.is_leaf:
+                q[0, :4] = n.param[:4]
+                q[1, :2] = n.param[4:6]
+                if n.planes is not None:       # convex polyhedron: planeIdx, planeNum (CSG/CSGNode.h:204-207)
+                    qu[0, 0] = len(self.plan)
+                    qu[0, 1] = len(n.planes)
+                    self.plan.extend(np.asarray(n.planes, np.float32))
+                bb = n.bbox
+            else:
+                bb = _tree_bbox(n)
+            q[2, 0:3] = bb[0:3]
+            q[2, 3] = bb[3]
+            q[3, 0:2] = bb[4:6]
+            qu[3, 2] = n.typecode
+            tidx = self._add_transform(gm) if (n.is_leaf and gm is not None) else 0
+            qu[3, 3] = (tidx & 0x7FFFFFFF) | (0x80000000 if n.complement else 0)
+        qu[1, 2] = boundary
+        qu[1, 3] = index
+        return q
+
     def add_prim(self, root: Node, boundary: int, mesh_idx: int = 0) -> int:
-        """Serialise a tree as a complete binary tree (level order, CSG_ZERO padding)."""
+        """Serialise a tree as a complete binary tree (level order, CSG_ZERO padding), the leaves
+        of its list nodes following it; a list at the root is its header then its leaves."""
         h = _height(root)
         num = (1 << (h + 1)) - 1
         slots: list[Node | None] = [None] * num
@@ -213,42 +262,36 @@ class Foundry:
         def place(n, i, parent_m):
             slots[i] = n
             gtran[i] = _compose(n.transform, parent_m)
-            if not n.is_leaf:
+            if not n.is_leaf and not n.is_list:
                 place(n.left, 2 * i + 1, gtran[i])
                 place(n.right, 2 * i + 2, gtran[i])
         place(root, 0, None)
         offset = len(self.node)
+        # list sub-nodes follow the tree; subOffset counts from the prim's first node
+        # (CSG/CSGMaker.cc:800-860, CSG/csg_intersect_node.h:392-945)
+        subs, cursor = [], num
         for i, n in enumerate(slots):
-            q = np.zeros((4, 4), dtype=np.float32)
-            qu = q.view(np.uint32)
-            if n is None:
-                qu[3, 2] = CSG_ZERO
-            else:
-                if n.is_leaf:
-                    q[0, :4] = n.param[:4]
-                    q[1, :2] = n.param[4:6]
-                    if n.planes is not None:       # convex polyhedron: planeIdx, planeNum (CSG/CSGNode.h:204-207)
-                        qu[0, 0] = len(self.plan)
-                        qu[0, 1] = len(n.planes)
-                        self.plan.extend(np.asarray(n.planes, np.float32))
-                    bb = n.bbox
-                else:
-                    bb = _tree_bbox(n)
-                q[2, 0:3] = bb[0:3]
-                q[2, 3] = bb[3]
-                q[3, 0:2] = bb[4:6]
-                qu[3, 2] = n.typecode
-                tidx = self._add_transform(gtran[i]) if (n.is_leaf and gtran[i] is not None) else 0
-                qu[3, 3] = (tidx & 0x7FFFFFFF) | (0x80000000 if n.complement else 0)
-            qu[1, 2] = boundary
-            qu[1, 3] = i
+            if n is not None and n.is_list:
+                subs.append((i, cursor))
+                cursor += len(n.subs)
+        for i, n in enumerate(slots):
+            q = self._node_row(n, gtran[i], boundary, i)
+            if n is not None and n.is_list:
+                qu = q.view(np.uint32)
+                qu[0, 0] = len(n.subs)
+                qu[0, 1] = dict(subs)[i]
             self.node.append(q)
-        if not root.is_leaf:
-            self.node[offset].view(np.uint32)[0, 0] = num      # subNum
+        for i, first in subs:
+            for k, leaf in enumerate(slots[i].subs):
+                if not leaf.is_leaf:
+                    raise ValueError("list nodes hold leaves only")
+                self.node.append(self._node_row(leaf, _compose(leaf.transform, gtran[i]), boundary, first + k))
+        if not root.is_leaf and not root.is_list:
+            self.node[offset].view(np.uint32)[0, 0] = num      # subNum: complete binary tree size
         bb = _tree_bbox(root)
         p = np.zeros((4, 4), dtype=np.float32)
         pi = p.view(np.int32)
-        pi[0, 0] = num
+        pi[0, 0] = cursor
         pi[0, 1] = offset
         pi[1, 1] = mesh_idx
         pi[1, 3] = len(self.prim)

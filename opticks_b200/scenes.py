@@ -157,6 +157,39 @@ def csg_leaf_zoo():
     return fd, prims
 
 
+def csg_list_zoo():
+    """(foundry, prim indices) of list nodes: contiguous, discontiguous and overlap lists of
+    spheres, boxes, cylinders and a convexpolyhedron (translated leaves), and lists as leaves of
+    boolean trees.  No contiguous list puts more than 8 enters on one ray."""
+    def sph(r, x, y, z=0.0):
+        return F.translate(F.sphere(r), x, y, z)
+    s2 = 100.0 * math.sqrt(2.0)
+    three = lambda r: [sph(r, 100.0, 100.0), sph(r, -100.0, 100.0), sph(r, 0.0, -s2)]
+    cube = F.convexpolyhedron(F.cube_planes(60.0), (-60, -60, -60, 60, 60, 60))
+    chain = [F.translate(F.cylinder(40.0, -60.0, 60.0), 0.0, 0.0, z) for z in (-200.0, -100.0, 0.0, 100.0, 200.0)]
+    trees = [
+        F.list_node("contiguous", three(150.0)),
+        F.list_node("discontiguous", three(80.0)),
+        F.list_node("overlap", [F.box3(300.0, 300.0, 300.0), F.sphere(200.0)]),
+        F.list_node("overlap", three(260.0)),
+        F.list_node("contiguous", [F.box3(300.0, 300.0, 300.0), F.sphere(200.0)]),
+        F.list_node("discontiguous", [sph(60.0, -50.0, 0.0), sph(60.0, 50.0, 0.0),
+                                      F.translate(F.box3(80.0, 80.0, 80.0), 0.0, 200.0, 0.0),
+                                      F.translate(F.box3(80.0, 80.0, 80.0), 0.0, -200.0, 0.0)]),
+        F.op("union", F.box3(200.0, 200.0, 200.0), F.list_node("contiguous", three(120.0))),
+        F.op("difference", F.list_node("contiguous", three(150.0)), F.sphere(120.0)),
+        F.list_node("discontiguous", [F.translate(cube, 150.0, 0.0, 0.0), sph(70.0, -150.0, 0.0)]),
+        F.list_node("contiguous", chain),
+        F.op("intersection", F.list_node("overlap", [F.box3(300.0, 300.0, 300.0), F.sphere(200.0)]),
+             F.list_node("discontiguous", [sph(90.0, 0.0, 120.0), sph(90.0, 0.0, -120.0)])),
+    ]
+    fd = F.Foundry()
+    prims = [fd.add_prim(t, 0) for t in trees]
+    fd.add_solid("lists", prims)
+    fd.add_inst(np.eye(4), 0)
+    return fd, prims
+
+
 def leaf_zoo_detector(num_photon: int = 100_000):
     """photons from the centre of a water-filled box whose walls detect, through acrylic bodies
     made of the further leaves: a cone, a hyperboloid, an octahedral convexpolyhedron, a sphere cut
@@ -183,6 +216,38 @@ def leaf_zoo_detector(num_photon: int = 100_000):
     fd = F.Foundry()
     prims = [fd.add_prim(F.box3(3000.0, 3000.0, 3000.0), b_box)] + [fd.add_prim(b, b_acr) for b in bodies]
     s0 = fd.add_solid("zoo", prims)
+    fd.add_inst(np.eye(4), s0)
+    gs = torch_genstep(num_photon, wavelength=440.0, radius=0.0, type_=T_SPHERE, distance=0.25)[None]
+    return fd, lib, None, gs
+
+
+def list_zoo_detector(num_photon: int = 100_000):
+    """photons from the centre of a water-filled box whose walls detect, through acrylic bodies
+    that are list nodes (contiguous, discontiguous, overlap) and trees holding lists"""
+    lib = M.BoundaryLib()
+    lib.mat(VACUUM)
+    lib.mat(M.Material("Rock", rindex=1.5, absorption_length=1.0, scattering_length=1e9))
+    lib.mat(WATER_C1)
+    lib.mat(M.Material("Acrylic", rindex=1.49, absorption_length=1e6, scattering_length=1e6))
+    lib.sur(M.Surface("Detector", detect=1.0, absorb=0.0))
+    b_box = lib.add("Rock", "", "Detector", "Water")
+    b_acr = lib.add("Water", "", "", "Acrylic")
+
+    def sph(r, x, y, z=0.0):
+        return F.translate(F.sphere(r), x, y, z)
+    s2 = 100.0 * math.sqrt(2.0)
+    three = lambda r: [sph(r, 100.0, 100.0), sph(r, -100.0, 100.0), sph(r, 0.0, -s2)]
+    bodies = [
+        F.translate(F.list_node("contiguous", three(150.0)), 900.0, 0.0, 0.0),
+        F.translate(F.list_node("discontiguous", three(80.0)), -900.0, 0.0, 0.0),
+        F.translate(F.list_node("overlap", [F.box3(300.0, 300.0, 300.0), F.sphere(200.0)]), 0.0, 900.0, 0.0),
+        F.translate(F.list_node("contiguous", [F.box3(300.0, 300.0, 300.0), F.sphere(200.0)]), 0.0, -900.0, 0.0),
+        F.translate(F.op("union", F.box3(200.0, 200.0, 200.0), F.list_node("contiguous", three(120.0))), 0.0, 0.0, 900.0),
+        F.translate(F.op("difference", F.list_node("contiguous", three(150.0)), F.sphere(120.0)), 0.0, 0.0, -900.0),
+    ]
+    fd = F.Foundry()
+    prims = [fd.add_prim(F.box3(3000.0, 3000.0, 3000.0), b_box)] + [fd.add_prim(b, b_acr) for b in bodies]
+    s0 = fd.add_solid("lists", prims)
     fd.add_inst(np.eye(4), s0)
     gs = torch_genstep(num_photon, wavelength=440.0, radius=0.0, type_=T_SPHERE, distance=0.25)[None]
     return fd, lib, None, gs

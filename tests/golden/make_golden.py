@@ -8,6 +8,9 @@ csg_zoo_ref.npz  : the same for the further leaves (scenes.csg_leaf_zoo: cone, h
                    convexpolyhedron with its plan table, phicut, halfspace) through the reference's
                    tree intersector, and the slab / infcylinder / disc leaves one at a time through
                    the reference's own leaf functions (compiled there only under CSG_EXTRA).
+csg_list_ref.npz : list nodes (scenes.csg_list_zoo: contiguous, discontiguous, overlap, and lists
+                   inside boolean trees) through the reference's tree / list intersectors
+                   (built WITH_CONTIGUOUS as its CSG library is).
 
 Run from the repository root where the reference checkout is present:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -64,6 +67,19 @@ def main():
     np.savez_compressed(os.path.join(ROOT, "tests", "golden", "csg_scan_ref.npz"), **out)
     print({k: getattr(v, "shape", v) for k, v in out.items()})
     zoo()
+    lists()
+
+
+def lists():
+    fd, prims = scenes.csg_list_zoo()
+    A = fd.arrays()
+    rays = scenes.scan_rays(2000, seed=19, half=400.0)
+    roots = np.array([int(A["prim"].view(np.int32)[p, 0, 1]) for p in prims], np.int32)
+    out = {"node": A["node"], "itra": A["itra"], "plan": A["plan"], "prims": np.array(prims, np.int32),
+           "roots": roots, "rays": rays}
+    out["isect"] = np.stack([O.ref_csg_scan(A["node"], A["itra"], int(r), rays, 0.0, plan=A["plan"]) for r in roots])
+    np.savez_compressed(os.path.join(ROOT, "tests", "golden", "csg_list_ref.npz"), **out)
+    print({k: getattr(v, "shape", v) for k, v in out.items()})
 
 
 EXTRA_LEAVES = (F.slab((0.6, 0.8, 0.0), -100.0, 150.0), F.infcylinder(120.0),

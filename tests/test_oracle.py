@@ -208,3 +208,64 @@ def test_reference_driver_refuses_gensteps_it_cannot_generate():
     odd.view(np.int32)[0, 0, 0] = 99
     with pytest.raises(ValueError):
         O.ref_genstep_check(odd)
+
+
+LISTS = os.path.join(ROOT, "tests", "golden", "csg_list_ref.npz")
+
+
+def test_oracle_list_nodes_match_reference_golden_bit_exact():
+    g = np.load(LISTS)
+    fd, prims = scenes.csg_list_zoo()
+    A = fd.arrays()
+    np.testing.assert_array_equal(A["node"], g["node"])
+    for k, root in enumerate(g["roots"]):
+        out, err = O.csg_scan(g["node"], g["itra"], int(root), g["rays"], 0.0, plan=g["plan"])
+        ref = g["isect"][k]
+        assert err == 0
+        assert (ref[:, 3] > 0).sum() > 30, k
+        np.testing.assert_array_equal(out, ref, err_msg=f"list prim {k}")
+
+
+@pytest.mark.skipif(not O.have_ref_csg(), reason="reference CPU build absent")
+def test_oracle_list_nodes_match_live_reference_on_fresh_rays():
+    fd, prims = scenes.csg_list_zoo()
+    A = fd.arrays()
+    rays = scenes.scan_rays(20000, seed=23, half=400.0)
+    for k, p in enumerate(prims):
+        root = int(A["prim"].view(np.int32)[p, 0, 1])
+        ref = O.ref_csg_scan(A["node"], A["itra"], root, rays, 0.0, plan=A["plan"])
+        out, err = O.csg_scan(A["node"], A["itra"], root, rays, 0.0, plan=A["plan"])
+        np.testing.assert_array_equal(out, ref, err_msg=f"list prim {k}")
+
+
+def test_list_layout_follows_the_reference():
+    # a list at the root: header (subNum, subOffset 1) then its leaves; inside a tree the leaves
+    # follow the complete binary tree and subOffset counts from the tree's root
+    fd = F.Foundry()
+    l1 = F.list_node("discontiguous", [F.sphere(10.0), F.translate(F.sphere(10.0), 30.0, 0.0, 0.0)])
+    p0 = fd.add_prim(l1, 0)
+    p1 = fd.add_prim(F.op("union", F.box3(50.0, 50.0, 50.0), F.list_node("overlap", [F.sphere(20.0), F.box3(30.0, 30.0, 30.0)])), 0)
+    A = fd.arrays()
+    nu, pi = A["node"].view(np.uint32), A["prim"].view(np.int32)
+    assert tuple(pi[p0, 0, :2]) == (3, 0)
+    assert (nu[0, 3, 2], nu[0, 0, 0], nu[0, 0, 1]) == (F.CSG_DISCONTIGUOUS, 2, 1)
+    assert nu[2, 3, 3] == 1                                  # the second sphere's transform
+    assert tuple(pi[p1, 0, :2]) == (5, 3)
+    assert nu[3, 0, 0] == 3                                  # tree root subNum: 3 tree nodes
+    assert (nu[5, 3, 2], nu[5, 0, 0], nu[5, 0, 1]) == (F.CSG_OVERLAP, 2, 3)
+    assert (nu[6, 3, 2], nu[7, 3, 2]) == (F.CSG_SPHERE, F.CSG_BOX3)
+
+
+def test_contiguous_list_flags_more_than_eight_enters():
+    # the reference keeps 8 enters per contiguous list (CSG/csg_intersect_node.h:460-470, undefined
+    # beyond); the restatement drops the rest and raises the evaluator error flag
+    fd = F.Foundry()
+    chain = [F.translate(F.sphere(30.0), 0.0, 0.0, z) for z in np.arange(10) * 50.0]
+    fd.add_prim(F.list_node("contiguous", chain), 0)
+    A = fd.arrays()
+    rays = np.array([[0.0], [0.0], [0.0], [0.0], [0.0], [1.0]], np.float32)       # inside the first: 9 enters
+    out, err = O.csg_scan(A["node"], A["itra"], 0, rays, 0.0)
+    assert err & 1
+    rays = np.array([[0.0], [-100.0], [0.0], [0.0], [1.0], [0.0]], np.float32)     # across: 1 enter
+    out, err = O.csg_scan(A["node"], A["itra"], 0, rays, 0.0)
+    assert err == 0 and abs(out[0, 3] - 70.0) < 1e-3
