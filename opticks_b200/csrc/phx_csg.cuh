@@ -87,6 +87,21 @@ struct PhxCsgCtx {
     const float4* plan;   // (Nl) float4 : planes of convex polyhedra (n, w)
 };
 
+// CSG evaluator variant, the template argument of the trace chain: bit 0 the FP64 root polish,
+// bit 1 the full evaluator (the leaves beyond sphere, zsphere, cylinder, box3 and torus, and list
+// nodes).  The host launches the full variant only for geometries that use it: in the base
+// variant the leaf dispatch and tree walk keep the registers and code size of those five leaves.
+#define PHX_CV_POLISH 1
+#define PHX_CV_FULL 2
+#define PHX_CV_P(cv) (((cv) & PHX_CV_POLISH) != 0)
+#define PHX_CV_F(cv) (((cv) & PHX_CV_FULL) != 0)
+
+// typecodes the base variant evaluates (operators, CSG_ZERO and the five leaves)
+__host__ __device__ inline bool phx_csg_base_typecode(unsigned tc)
+{
+    return tc <= 3u || tc == 101u || tc == 103u || tc == 105u || tc == 110u || tc == 116u;
+}
+
 PHX_D unsigned nd_u(const float4& q, int k) { return __float_as_uint(k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w); }
 
 // ---------------------------------------------------------------- quadratic roots
@@ -655,28 +670,63 @@ PHX_COLD float4 leaf_disc(const float4 q0, const float4 q1, const float t_min, c
 // One out-of-line copy of the leaf intersector, shared by the tree evaluator and leaf-rooted
 // prims; arguments and result by value so nothing goes through the stack.  A miss returns w=0
 // (with x=-0 for a complemented leaf), a hit has w = t > t_min.
-template <bool POLISH>
-PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __restrict__ itra, const float4* __restrict__ plan,
-                            const int ni, const float t_min, const float3 ray_o, const float3 ray_d)
-{
-    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 q0 = __ldg(node + 4 * ni + 0);
-    const float4 q1 = __ldg(node + 4 * ni + 1);
-    const float4 q3 = __ldg(node + 4 * ni + 3);
-    const unsigned typecode = __float_as_uint(q3.z);
-    const unsigned tc_w = __float_as_uint(q3.w);
-    const unsigned gtransformIdx = tc_w & 0x7fffffffu;
-    const bool complement = (tc_w & 0x80000000u) != 0u;
-    float4 t4[4];
-    const float4* q = nullptr;
-    if (gtransformIdx > 0) {
-        const float4* src = itra + 4 * (gtransformIdx - 1);
-        t4[0] = __ldg(src + 0); t4[1] = __ldg(src + 1); t4[2] = __ldg(src + 2); t4[3] = __ldg(src + 3);
-        q = t4;
-    }
-    float3 origin = q ? xform_row(q, ray_o, 1.f) : ray_o;
-    float3 direction = q ? xform_row(q, ray_d, 0.f) : ray_d;
+// transform of the ray into the leaf frame and of the normal back, and the complement, around
+// one leaf intersector (CSG/csg_intersect_leaf.h:174-300)
+#define PHX_LEAF_PROLOGUE                                                                        \
+    float4 isect = make_float4(0.f, 0.f, 0.f, 0.f);                                              \
+    const float4 q0 = __ldg(node + 4 * ni + 0);                                                  \
+    const float4 q1 = __ldg(node + 4 * ni + 1);                                                  \
+    const float4 q3 = __ldg(node + 4 * ni + 3);                                                  \
+    const unsigned typecode = __float_as_uint(q3.z);                                             \
+    const unsigned tc_w = __float_as_uint(q3.w);                                                 \
+    const unsigned gtransformIdx = tc_w & 0x7fffffffu;                                           \
+    const bool complement = (tc_w & 0x80000000u) != 0u;                                          \
+    float4 t4[4];                                                                                \
+    const float4* q = nullptr;                                                                   \
+    if (gtransformIdx > 0) {                                                                     \
+        const float4* src = itra + 4 * (gtransformIdx - 1);                                      \
+        t4[0] = __ldg(src + 0); t4[1] = __ldg(src + 1); t4[2] = __ldg(src + 2); t4[3] = __ldg(src + 3); \
+        q = t4;                                                                                  \
+    }                                                                                            \
+    float3 origin = q ? xform_row(q, ray_o, 1.f) : ray_o;                                        \
+    float3 direction = q ? xform_row(q, ray_d, 0.f) : ray_d;                                     \
     bool valid = false;
+
+#define PHX_LEAF_EPILOGUE                                                                        \
+    if (valid && q) {                                                                            \
+        float3 n = xform_col(q, make_float3(isect.x, isect.y, isect.z), 0.f);                    \
+        isect.x = n.x; isect.y = n.y; isect.z = n.z;                                             \
+    }                                                                                            \
+    if (complement) {                                                                            \
+        isect.x = valid ? -isect.x : -0.f;                                                       \
+        isect.y = valid ? -isect.y : isect.y;                                                    \
+        isect.z = valid ? -isect.z : isect.z;                                                    \
+    }                                                                                            \
+    return isect;
+
+// the five base leaves
+template <bool POLISH>
+PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __restrict__ itra, const int ni, const float t_min,
+                            const float3 ray_o, const float3 ray_d)
+{
+    PHX_LEAF_PROLOGUE
+    switch (typecode) {
+        case PHX_CSG_SPHERE:   valid = leaf_sphere<POLISH>(isect, q0, t_min, origin, direction); break;
+        case PHX_CSG_ZSPHERE:  valid = leaf_zsphere<POLISH>(isect, q0, q1, t_min, origin, direction); break;
+        case PHX_CSG_CYLINDER: valid = leaf_cylinder<POLISH>(isect, q0, q1, t_min, origin, direction); break;
+        case PHX_CSG_BOX3:     isect = leaf_box3(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        case PHX_CSG_TORUS:    isect = leaf_torus(q0, t_min, origin, direction); valid = isect.w > t_min; break;
+        default: break;
+    }
+    PHX_LEAF_EPILOGUE
+}
+
+// every leaf (the full variant)
+template <bool POLISH>
+PHX_LEAFFN float4 leaf_eval_full(const float4* __restrict__ node, const float4* __restrict__ itra, const float4* __restrict__ plan,
+                                 const int ni, const float t_min, const float3 ray_o, const float3 ray_d)
+{
+    PHX_LEAF_PROLOGUE
     switch (typecode) {
         case PHX_CSG_SPHERE:   valid = leaf_sphere<POLISH>(isect, q0, t_min, origin, direction); break;
         case PHX_CSG_ZSPHERE:  valid = leaf_zsphere<POLISH>(isect, q0, q1, t_min, origin, direction); break;
@@ -693,24 +743,24 @@ PHX_LEAFFN float4 leaf_eval(const float4* __restrict__ node, const float4* __res
         case PHX_CSG_DISC:     isect = leaf_disc(q0, q1, t_min, origin, direction); valid = isect.w > t_min; break;
         default: break;
     }
+    // w = -0: the convexpolyhedron's valid report with isect unset, kept valid as the reference does
     valid = valid || __float_as_uint(isect.w) == 0x80000000u;
-    if (valid && q) {
-        float3 n = xform_col(q, make_float3(isect.x, isect.y, isect.z), 0.f);
-        isect.x = n.x; isect.y = n.y; isect.z = n.z;
-    }
-    if (complement) {
-        isect.x = valid ? -isect.x : -0.f;
-        isect.y = valid ? -isect.y : isect.y;
-        isect.z = valid ? -isect.z : isect.z;
-    }
-    return isect;
+    PHX_LEAF_EPILOGUE
 }
 
-template <bool POLISH>
+// one leaf through the evaluator of the variant
+template <int CV>
+PHX_D float4 leaf_call(const PhxCsgCtx& g, int ni, float t_min, const float3& o, const float3& d)
+{
+    if constexpr (PHX_CV_F(CV)) return leaf_eval_full<PHX_CV_P(CV)>(g.node, g.itra, g.plan, ni, t_min, o, d);
+    else return leaf_eval<PHX_CV_P(CV)>(g.node, g.itra, ni, t_min, o, d);
+}
+
+template <int CV>
 PHX_D bool intersect_leaf(float4& isect, const PhxCsgCtx& g, int ni, float t_min, const float3& ray_o, const float3& ray_d, unsigned& err)
 {
     (void)err;
-    isect = leaf_eval<POLISH>(g.node, g.itra, g.plan, ni, t_min, ray_o, ray_d);
+    isect = leaf_call<CV>(g, ni, t_min, ray_o, ray_d);
     return isect.w > t_min;
 }
 
@@ -728,7 +778,7 @@ PHX_D int phx_classify(const float4& ise, const float3& d, float tmin)
 
 // union of leaves that may touch or overlap: the farthest exit reachable through a chain of
 // overlapping constituents (CSG/csg_intersect_node.h:392-600)
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
                                      const float3& d, unsigned& err)
 {
@@ -736,7 +786,7 @@ PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int firs
     float4 farthest_exit = make_float4(0.f, 0.f, 0.f, t_min);
     int exit_count = 0;
     for (int i = 0; i < num_sub; i++) {
-        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        const float4 s = leaf_call<CV>(g, first + i, t_min, o, d);
         if (!phx_leaf_valid(s, t_min)) continue;
         const int st = phx_classify(s, d, t_min);
         if (st == PHX_STATE_ENTER) { if (s.w < nearest_enter.w) nearest_enter = s; }
@@ -751,7 +801,7 @@ PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int firs
     float enter[PHX_LIST_MAX_ENTER];
     int aux[PHX_LIST_MAX_ENTER];
     for (int i = 0; i < num_sub; i++) {
-        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        const float4 s = leaf_call<CV>(g, first + i, t_min, o, d);
         if (!phx_leaf_valid(s, t_min)) continue;
         const int st = phx_classify(s, d, t_min);
         if (st == PHX_STATE_ENTER) {
@@ -777,7 +827,7 @@ PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int firs
     for (int i = 0; i < enter_count; i++) {
         const float tminAdvanced = enter[i] + PHX_CSG_PROPAGATE_EPSILON;
         if (tminAdvanced < farthest_exit.w) {
-            const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + aux[i], tminAdvanced, o, d);
+            const float4 s = leaf_call<CV>(g, first + aux[i], tminAdvanced, o, d);
             if (phx_leaf_valid(s, tminAdvanced) && phx_classify(s, d, tminAdvanced) == PHX_STATE_EXIT) {
                 exit_count += 1;
                 if (s.w > farthest_exit.w) farthest_exit = s;
@@ -790,13 +840,13 @@ PHX_D bool intersect_list_contiguous(float4& isect, const PhxCsgCtx& g, int firs
 }
 
 // union of disjoint leaves: the closest valid report (CSG/csg_intersect_node.h:654-700)
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_list_discontiguous(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
                                         const float3& d)
 {
     float4 closest = make_float4(0.f, 0.f, 0.f, PHX_RT_MAX);
     for (int i = 0; i < num_sub; i++) {
-        const float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        const float4 s = leaf_call<CV>(g, first + i, t_min, o, d);
         if (phx_leaf_valid(s, t_min) && s.w < closest.w) closest = s;
     }
     const bool valid = closest.w < PHX_RT_MAX;
@@ -806,7 +856,7 @@ PHX_D bool intersect_list_discontiguous(float4& isect, const PhxCsgCtx& g, int f
 
 // intersection of leaves: farthest enter or nearest exit when every leaf is entered or exited
 // and the farthest enter precedes the nearest exit (CSG/csg_intersect_node.h:819-910)
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_list_overlap(float4& isect, const PhxCsgCtx& g, int first, int num_sub, float t_min, const float3& o,
                                   const float3& d)
 {
@@ -814,14 +864,14 @@ PHX_D bool intersect_list_overlap(float4& isect, const PhxCsgCtx& g, int first, 
     float4 nearest_exit = make_float4(0.f, 0.f, 0.f, PHX_RT_MAX);
     int enter_count = 0, exit_count = 0;
     for (int i = 0; i < num_sub; i++) {
-        float4 s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, t_min, o, d);
+        float4 s = leaf_call<CV>(g, first + i, t_min, o, d);
         if (!phx_leaf_valid(s, t_min)) continue;
         const int st = phx_classify(s, d, t_min);
         if (st == PHX_STATE_ENTER) {
             enter_count += 1;
             if (s.w > farthest_enter.w) farthest_enter = s;
             const float tminAdvanced = s.w + PHX_CSG_PROPAGATE_EPSILON;
-            s = leaf_eval<POLISH>(g.node, g.itra, g.plan, first + i, tminAdvanced, o, d);
+            s = leaf_call<CV>(g, first + i, tminAdvanced, o, d);
             if (phx_leaf_valid(s, tminAdvanced) && phx_classify(s, d, tminAdvanced) == PHX_STATE_EXIT) {
                 exit_count += 1;
                 if (s.w < nearest_exit.w) nearest_exit = s;
@@ -840,7 +890,7 @@ PHX_D bool intersect_list_overlap(float4& isect, const PhxCsgCtx& g, int first, 
 }
 
 // list header ni, sub-nodes relative to the prim root; isect is untouched on a miss
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_list(float4& isect, const PhxCsgCtx& g, int ni, int root, unsigned typecode, float t_min, const float3& o,
                           const float3& d, unsigned& err)
 {
@@ -848,9 +898,9 @@ PHX_D bool intersect_list(float4& isect, const PhxCsgCtx& g, int ni, int root, u
     const int num_sub = (int)__float_as_uint(q0.x);
     const int first = root + (int)__float_as_uint(q0.y);
     switch (typecode) {
-        case PHX_CSG_CONTIGUOUS: return intersect_list_contiguous<POLISH>(isect, g, first, num_sub, t_min, o, d, err);
-        case PHX_CSG_DISCONTIGUOUS: return intersect_list_discontiguous<POLISH>(isect, g, first, num_sub, t_min, o, d);
-        case PHX_CSG_OVERLAP: return intersect_list_overlap<POLISH>(isect, g, first, num_sub, t_min, o, d);
+        case PHX_CSG_CONTIGUOUS: return intersect_list_contiguous<CV>(isect, g, first, num_sub, t_min, o, d, err);
+        case PHX_CSG_DISCONTIGUOUS: return intersect_list_discontiguous<CV>(isect, g, first, num_sub, t_min, o, d);
+        case PHX_CSG_OVERLAP: return intersect_list_overlap<CV>(isect, g, first, num_sub, t_min, o, d);
         default: return false;
     }
 }
@@ -868,11 +918,11 @@ PHX_D bool intersect_list(float4& isect, const PhxCsgCtx& g, int ni, int root, u
 #endif
 #define PHX_TREE3_LOOP_CAP 64
 
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned op, float t_min, const float3& o, const float3& d, unsigned& err)
 {
-    float4 L = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 1, t_min, o, d);
-    float4 R = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 2, t_min, o, d);
+    float4 L = leaf_call<CV>(g, root + 1, t_min, o, d);
+    float4 R = leaf_call<CV>(g, root + 2, t_min, o, d);
     for (int it = 0; it < PHX_TREE3_LOOP_CAP; it++) {
         int l_state = phx_classify(L, d, t_min);
         int r_state = phx_classify(R, d, t_min);
@@ -889,8 +939,8 @@ PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned
             isect = result;
             return isect.w > 0.f;
         }
-        if (ctrl == PHX_CTRL_LOOP_A) L = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 1, fabsf(L.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
-        else R = leaf_eval<POLISH>(g.node, g.itra, g.plan, root + 2, fabsf(R.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+        if (ctrl == PHX_CTRL_LOOP_A) L = leaf_call<CV>(g, root + 1, fabsf(L.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
+        else R = leaf_call<CV>(g, root + 2, fabsf(R.w) + PHX_CSG_PROPAGATE_EPSILON, o, d);
     }
     err |= PHX_STATUS_CSG_STACK;
     isect = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -898,7 +948,7 @@ PHX_D bool intersect_tree3(float4& isect, const PhxCsgCtx& g, int root, unsigned
 }
 
 // ---------------------------------------------------------------- tree
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
 {
     const unsigned numNode = __float_as_uint(__ldg(g.node + 4 * root).x);   // subNum
@@ -908,7 +958,7 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
         const unsigned tl = __float_as_uint(__ldg(g.node + 4 * (root + 1) + 3).z);
         const unsigned tr = __float_as_uint(__ldg(g.node + 4 * (root + 2) + 3).z);
         if (op >= PHX_CSG_UNION && op <= PHX_CSG_DIFFERENCE && tl >= PHX_CSG_LEAF && tr >= PHX_CSG_LEAF)
-            return intersect_tree3<POLISH>(isect, g, root, op, t_min, o, d, err);
+            return intersect_tree3<CV>(isect, g, root, op, t_min, o, d, err);
     }
 #endif
     const unsigned height = (unsigned)(__ffs((int)numNode + 1) - 2);
@@ -935,8 +985,12 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
             if (typecode == PHX_CSG_ZERO) { nodeIdx = PHX_POSTORDER_NEXT(nodeIdx, elevation); continue; }
             if (typecode >= PHX_CSG_NODE) {
                 float4 nd_isect = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (typecode < PHX_CSG_LEAF) intersect_list<POLISH>(nd_isect, g, ni, root, typecode, tmin, o, d, err);
-                else intersect_leaf<POLISH>(nd_isect, g, ni, tmin, o, d, err);
+                if constexpr (PHX_CV_F(CV)) {
+                    if (typecode < PHX_CSG_LEAF) intersect_list<CV>(nd_isect, g, ni, root, typecode, tmin, o, d, err);
+                    else intersect_leaf<CV>(nd_isect, g, ni, tmin, o, d, err);
+                } else {
+                    intersect_leaf<CV>(nd_isect, g, ni, tmin, o, d, err);   // lists launch the full variant
+                }
                 nd_isect.w = copysignf(nd_isect.w, nodeIdx % 2u == 0u ? -1.f : 1.f);
                 if (sp >= PHX_CSG_STACK - 1) { ierr |= PHX_CSG_ERR_OVERFLOW; break; }
                 stk[++sp] = nd_isect;
@@ -998,14 +1052,15 @@ PHX_D bool intersect_tree(float4& isect, const PhxCsgCtx& g, int root, float t_m
     return isect.w > 0.f;
 }
 
-// one prim: leaf at the root, a boolean tree, or a list.  POLISH selects the FP64 root polish at
+// one prim: leaf at the root, a boolean tree, or a list.  CV selects the FP64 root polish at
 // compile time so the default path keeps the reference's FP32 expression structure.
-template <bool POLISH>
+template <int CV>
 PHX_D bool intersect_prim(float4& isect, const PhxCsgCtx& g, int root, float t_min, const float3& o, const float3& d, unsigned& err)
 {
     const unsigned typecode = __float_as_uint(__ldg(g.node + 4 * root + 3).z);
     isect = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (typecode >= PHX_CSG_LEAF) return intersect_leaf<POLISH>(isect, g, root, t_min, o, d, err);
-    if (typecode < PHX_CSG_NODE) return intersect_tree<POLISH>(isect, g, root, t_min, o, d, err);
-    return intersect_list<POLISH>(isect, g, root, root, typecode, t_min, o, d, err);
+    if (typecode >= PHX_CSG_LEAF) return intersect_leaf<CV>(isect, g, root, t_min, o, d, err);
+    if (typecode < PHX_CSG_NODE) return intersect_tree<CV>(isect, g, root, t_min, o, d, err);
+    if constexpr (PHX_CV_F(CV)) return intersect_list<CV>(isect, g, root, root, typecode, t_min, o, d, err);
+    return false;
 }

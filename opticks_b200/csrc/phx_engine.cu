@@ -90,12 +90,14 @@ struct phx_engine {
     cudaStream_t stream = nullptr;
     // geometry
     DevBuf<float4> node, itra, plan, inst_inv;
+    PhxCsgCtx csg = { nullptr, nullptr, nullptr };
     DevBuf<phx_bvh4_node> bvh;
     DevBuf<phx_leaf> leaves, globals;
     DevBuf<float4> leaf_sph, global_sph;   // world bounding sphere per leaf (centre, radius)
     int num_global = 0;
     float cull[4] = { 0.f, 0.f, 0.f, 0.f };
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
+    bool has_full = false;    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
     std::vector<int> prim_node_offset;
     // physics
     cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr;
@@ -147,9 +149,7 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.bvh = e->bvh.p;
     S.leaves = e->leaves.p;
     S.inst_inv = e->inst_inv.p;
-    S.csg.node = e->node.p;
-    S.csg.itra = e->itra.p;
-    S.csg.plan = e->plan.p;
+    S.csg = e->csg;
     (void)polish;
     S.globals = e->globals.p;
     S.leaf_sph = e->leaf_sph.p;
@@ -265,7 +265,7 @@ struct SimArgs {
 #ifndef PHX_SIM_MINB
 #define PHX_SIM_MINB 8
 #endif
-template <bool POLISH>
+template <int CV>
 __global__ void __launch_bounds__(PHX_SIM_BLOCK, PHX_SIM_MINB) k_simulate(SimArgs a)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(PHX_SIM_BLOCK, PHX_SIM_MINB) k_simulate(SimArg
         memset(&p, 0, sizeof(p));
         generate_photon(p, rng, g, (unsigned long long)photon_idx, a.P, status);
         unsigned long long seqhis[2] = { 0ull, 0ull }, seqbnd[2] = { 0ull, 0ull };
-        phx_bounce_loop<POLISH>(p, rng, a.S, a.P, a.C, seqhis, seqbnd, status);
+        phx_bounce_loop<CV>(p, rng, a.S, a.P, a.C, seqhis, seqbnd, status);
         if (a.photon) phx_store_photon(a.photon + idx, p);
         if (a.seq) {
             ulonglong2* s = reinterpret_cast<ulonglong2*>(a.seq + idx);
@@ -385,7 +385,7 @@ __global__ void k_compact(const phx_photon* photon, long long N, const uint32_t*
 }
 
 // CSGScan : one thread per ray, SoA rays
-template <bool POLISH>
+template <int CV>
 __global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* rays, long long n, float4* out, unsigned* status)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -394,7 +394,7 @@ __global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* ra
     const float3 d = make_float3(__ldg(rays + 3 * n + i), __ldg(rays + 4 * n + i), __ldg(rays + 5 * n + i));
     unsigned st = 0;
     float4 is;
-    const bool valid = intersect_prim<POLISH>(is, csg, root, t_min, o, d, st);
+    const bool valid = intersect_prim<CV>(is, csg, root, t_min, o, d, st);
     out[i] = valid ? is : make_float4(0.f, 0.f, 0.f, 0.f);
     if (st) atomicOr(status, st);
 }
@@ -783,6 +783,9 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     if (geo->num_itra > 0) PHX_TRYCU(cudaMemcpy(e->itra.p, geo->itra, (size_t)geo->num_itra * 64, cudaMemcpyHostToDevice));
     PHX_TRYCU(e->plan.ensure((size_t)std::max(1, geo->num_plan)));
     if (geo->num_plan > 0) PHX_TRYCU(cudaMemcpy(e->plan.p, geo->plan, (size_t)geo->num_plan * 16, cudaMemcpyHostToDevice));
+    e->csg.node = e->node.p;
+    e->csg.itra = e->itra.p;
+    e->csg.plan = e->plan.p;
 
     e->prim_node_offset.resize(geo->num_prim);
     for (int p = 0; p < geo->num_prim; p++) {
@@ -793,6 +796,11 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
         memcpy(&nn, geo->prim + 16 * p + 0, 4);
         if (no < 0 || no + std::max(nn, 1) > geo->num_node) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d node range out of bounds", p); }
         if (const char* m = check_prim_nodes(geo, no)) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d: %s", p, m); }
+    }
+    for (int i = 0; i < geo->num_node && !e->has_full; i++) {
+        uint32_t tc;
+        memcpy(&tc, geo->node + 16 * (size_t)i + 14, 4);
+        e->has_full = !phx_csg_base_typecode(tc);
     }
     std::vector<float> inv((size_t)std::max(1, geo->num_inst) * 16, 0.f);
     std::vector<PhxLeafInput> leaves;
@@ -916,7 +924,7 @@ static PersistArgs persist_args_from(const phx_engine* e, const SimArgs& a)
 }
 
 // grid = SMs x resident blocks of the chosen block size (one wave of persistent blocks)
-template <bool POLISH, int BLOCK, bool ADJ = false>
+template <int CV, int BLOCK, bool ADJ = false>
 static int launch_persistent_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
     // occupancy is queried once per (device, kernel) so graph capture sees only the launch
@@ -926,27 +934,49 @@ static int launch_persistent_t(phx_engine* e, const PersistArgs& A, cudaStream_t
     if (!cached_sms[dev]) {
         int sms = 0, per_sm = 0;
         PHX_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sim_persistent<POLISH, BLOCK, ADJ>, BLOCK, 0));
+        PHX_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sim_persistent<CV, BLOCK, ADJ>, BLOCK, 0));
         cached_per_sm[dev] = per_sm;
         cached_sms[dev] = sms;
     }
     const int sms = cached_sms[dev], per_sm = cached_per_sm[dev];
     const long long want = (A.N + BLOCK - 1) / BLOCK;
     const long long grid = std::max<long long>(1, std::min<long long>((long long)sms * std::max(1, per_sm), want));
-    k_sim_persistent<POLISH, BLOCK, ADJ><<<(unsigned)grid, BLOCK, 0, st>>>(A);
+    k_sim_persistent<CV, BLOCK, ADJ><<<(unsigned)grid, BLOCK, 0, st>>>(A);
     PHX_CU(cudaGetLastError());
     return 0;
 }
 
+// the CSG variant (PHX_CV_*) of an engine: root polish from the config, the full set of leaves
+// and list nodes when the geometry uses any of them
+static int cv_of(const phx_engine* e, bool polish)
+{
+    return (polish ? PHX_CV_POLISH : 0) | (e->has_full ? PHX_CV_FULL : 0);
+}
+
+// `return EXPR` with the compile-time constant CVK set to the runtime variant cv
+#define PHX_CV_RETURN(cv, EXPR)                               \
+    switch (cv) {                                             \
+        case 1: { constexpr int CVK = 1; return EXPR; }       \
+        case 2: { constexpr int CVK = 2; return EXPR; }       \
+        case 3: { constexpr int CVK = 3; return EXPR; }       \
+        default: { constexpr int CVK = 0; return EXPR; }      \
+    }
+
+template <int BLOCK, bool ADJ = false>
+static int launch_persistent_b(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st)
+{
+    PHX_CV_RETURN(cv, (launch_persistent_t<CVK, BLOCK, ADJ>(e, A, st)));
+}
+
 static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cudaStream_t st)
 {
-    const bool pol = e->cfg.root_polish != 0;
+    const int cv = cv_of(e, e->cfg.root_polish != 0);
     switch (block) {
-        case 32:  return pol ? launch_persistent_t<true, 32>(e, A, st) : launch_persistent_t<false, 32>(e, A, st);
-        case 64:  return pol ? launch_persistent_t<true, 64>(e, A, st) : launch_persistent_t<false, 64>(e, A, st);
-        case 256: return pol ? launch_persistent_t<true, 256>(e, A, st) : launch_persistent_t<false, 256>(e, A, st);
+        case 32:  return launch_persistent_b<32>(e, A, cv, st);
+        case 64:  return launch_persistent_b<64>(e, A, cv, st);
+        case 256: return launch_persistent_b<256>(e, A, cv, st);
         case 128:
-        default:  return pol ? launch_persistent_t<true, 128>(e, A, st) : launch_persistent_t<false, 128>(e, A, st);
+        default:  return launch_persistent_b<128>(e, A, cv, st);
     }
 }
 
@@ -977,17 +1007,17 @@ static int wave_grid(K kernel, int dev, int* cache)
     return 0;
 }
 
-template <bool POLISH, bool ADJ = false>
+template <int CV, bool ADJ = false>
 static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
     static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {};
     const int dev = e->device;
     if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
     int rc;
-    if ((rc = wave_grid(k_wave_init<POLISH, ADJ>, dev, g_init))) return rc;
-    if ((rc = wave_grid(k_wave_trace<POLISH>, dev, g_trace))) return rc;
-    if ((rc = wave_grid(k_wave_shade<POLISH, ADJ>, dev, g_shade))) return rc;
-    if ((rc = wave_grid(k_wave_fill<POLISH, ADJ>, dev, g_fill))) return rc;
+    if ((rc = wave_grid(k_wave_init<CV, ADJ>, dev, g_init))) return rc;
+    if ((rc = wave_grid(k_wave_trace<CV>, dev, g_trace))) return rc;
+    if ((rc = wave_grid(k_wave_shade<CV, ADJ>, dev, g_shade))) return rc;
+    if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
     const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
@@ -1006,7 +1036,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     W.n_free = e->wcnt.p + 2;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
-    k_wave_init<POLISH, ADJ><<<gi, 128, 0, st>>>(W);
+    k_wave_init<CV, ADJ><<<gi, 128, 0, st>>>(W);
     PHX_CU(cudaGetLastError());
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
     e->last_rounds = 0;
@@ -1015,9 +1045,9 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     for (long long r = 0; r < max_rounds && !done;) {
         for (int k = 0; k < PHX_WAVE_ROUNDS; k++, r++) {
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
-            k_wave_trace<POLISH><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
-            k_wave_shade<POLISH, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
-            if (refill) k_wave_fill<POLISH, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
+            k_wave_trace<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+            k_wave_shade<CV, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
+            if (refill) k_wave_fill<CV, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
             cur = 1 - cur;
         }
         PHX_CU(cudaGetLastError());
@@ -1030,9 +1060,35 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     return 0;
 }
 
+template <bool ADJ = false>
+static int launch_wave_cv(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st)
+{
+    PHX_CV_RETURN(cv, (launch_wave_t<CVK, ADJ>(e, A, st)));
+}
+
 static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
-    return e->cfg.root_polish ? launch_wave_t<true>(e, A, st) : launch_wave_t<false>(e, A, st);
+    return launch_wave_cv(e, A, cv_of(e, e->cfg.root_polish != 0), st);
+}
+
+template <int CV>
+static void launch_simulate_t(const SimArgs& a, long long N, cudaStream_t st)
+{
+    const int B = PHX_SIM_BLOCK;
+    k_simulate<CV><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+}
+
+static int launch_simulate(phx_engine* e, const SimArgs& a, long long N, cudaStream_t st)
+{
+    PHX_CV_RETURN(cv_of(e, e->cfg.root_polish != 0), (launch_simulate_t<CVK>(a, N, st), 0));
+}
+
+template <int CV>
+static void launch_scan_t(const PhxCsgCtx& csg, int root, float t_min, const float* d_rays, long long n, float4* out, unsigned* status,
+                          cudaStream_t st)
+{
+    const int B = 128;
+    k_csg_scan<CV><<<(unsigned)((n + B - 1) / B), B, 0, st>>>(csg, root, t_min, d_rays, n, out, status);
 }
 
 extern "C" {
@@ -1104,9 +1160,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (A.ev_rng ? 1 : 0) +
                            (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
-        const int B = PHX_SIM_BLOCK;
-        if (e->cfg.root_polish) k_simulate<true><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
-        else k_simulate<false><<<(unsigned)((N + B - 1) / B), B, 0, st>>>(a);
+        launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());
         e->last_rounds = 0;
         e->last_launches = 1 + (event_index > 0 ? 1 : 0) + 1 + (want_hits ? 3 : 0);
@@ -1212,15 +1266,16 @@ int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d
     PHX_CU(cudaSetDevice(e->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
     PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
-    PhxCsgCtx csg;
-    csg.node = e->node.p;
-    csg.itra = e->itra.p;
-    csg.plan = e->plan.p;
+    const PhxCsgCtx csg = e->csg;
     if (n > 0) {
-        const int B = 128;
-        const unsigned grid = (unsigned)((n + B - 1) / B);
-        if (polish) k_csg_scan<true><<<grid, B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
-        else k_csg_scan<false><<<grid, B, 0, st>>>(csg, e->prim_node_offset[prim], t_min, d_rays, n, reinterpret_cast<float4*>(d_isect), e->status.p);
+        float4* out = reinterpret_cast<float4*>(d_isect);
+        const int root = e->prim_node_offset[prim];
+        switch (cv_of(e, polish != 0)) {
+            case 1: launch_scan_t<1>(csg, root, t_min, d_rays, n, out, e->status.p, st); break;
+            case 2: launch_scan_t<2>(csg, root, t_min, d_rays, n, out, e->status.p, st); break;
+            case 3: launch_scan_t<3>(csg, root, t_min, d_rays, n, out, e->status.p, st); break;
+            default: launch_scan_t<0>(csg, root, t_min, d_rays, n, out, e->status.p, st); break;
+        }
         PHX_CU(cudaGetLastError());
     }
     return 0;
@@ -1503,7 +1558,8 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     A.adj_wl_lo = wl_lo;
     A.adj_binw = binw;
     if (N > 0) {
-        rc = e->cfg.kernel_mode == 2 ? launch_wave_t<false, true>(e, A, st) : launch_persistent_t<false, 64, true>(e, A, st);
+        const int cv = cv_of(e, false);
+        rc = e->cfg.kernel_mode == 2 ? launch_wave_cv<true>(e, A, cv, st) : launch_persistent_b<64, true>(e, A, cv, st);
         if (rc) return rc;
     }
     PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));

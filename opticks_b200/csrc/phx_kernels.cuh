@@ -48,7 +48,7 @@ PHX_D bool phx_ball_overlaps(const float4 b, const float3& o, const float3& d, f
     return tc + h >= tmin && tc - h <= tmax;
 }
 
-template <bool POLISH>
+template <int CV>
 PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, const float3& o, const float3& d, float tmin, PhxBest& B,
                          unsigned& status)
 {
@@ -58,7 +58,7 @@ PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, con
     const float3 lo = xform_row(m, o, 1.f);
     const float3 ld = xform_row(m, d, 0.f);
     float4 is;
-    const bool valid = intersect_prim<POLISH>(is, S.csg, L.y, tmin, lo, ld, status);
+    const bool valid = intersect_prim<CV>(is, S.csg, L.y, tmin, lo, ld, status);
     // OptiX's interval rule: a report outside [tmin, tmax] is ignored (a convexpolyhedron wholly
     // behind the ray reports valid with t = 0, CSG/csg_intersect_leaf_convexpolyhedron.h:85-101)
     if (valid && is.w >= tmin && is.w < B.t) {
@@ -76,7 +76,7 @@ PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, con
 // The global leaves are tested first, then the hierarchy is traversed unless the segment
 // [tmin, closest so far] lies inside the ball no hierarchy leaf reaches.
 // Returns false for a miss (prd boundary 0xffff).
-template <bool POLISH>
+template <int CV>
 PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float tmin, float tmax, PhxPRD& prd, unsigned& status)
 {
     prd.gp_bd = 0xffffffffu;
@@ -91,7 +91,7 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
     B.isect = make_float4(0.f, 0.f, 0.f, 0.f);
     B.lposcost = 0.f;
     for (int g = 0; g < S.num_global; g++)
-        phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B, status);
+        phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B, status);
     bool traverse = !S.bvh_empty;
     if (traverse && S.cull.w > 0.f) {
         const float3 c = make_float3(S.cull.x, S.cull.y, S.cull.z);
@@ -129,7 +129,7 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                 const int first = enc >> 3;
                 const int count = (enc & 7) + 1;
                 for (int li = first; li < first + count; li++)
-                    phx_test_leaf<POLISH>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin,
+                    phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin,
                                           B, status);
                 continue;
             }
@@ -203,7 +203,7 @@ PHX_D void seq_add_nibble(unsigned long long* seqhis, unsigned long long* seqbnd
 
 // The bounce loop of CSGOptiX/CSGOptiX7.cu:432-530 with sctx::point/end seq recording
 // (sysrap/sctx.h:134-185, sysrap/sseq.h:174-184) always on.
-template <bool POLISH>
+template <int CV>
 PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene& S, const PhxProps& P, const PhxLoopCfg& C,
                            unsigned long long* seqhis, unsigned long long* seqbnd, unsigned& status)
 {
@@ -212,7 +212,7 @@ PHX_D void phx_bounce_loop(PhxPhoton& p, curandStateXORWOW& rng, const PhxScene&
     while (bounce < C.max_bounce && p.time < C.max_time) {
         const float tmin = (p.obf & C.eps0_mask) ? C.tmin0 : C.tmin;
         PhxPRD prd;
-        phx_trace<POLISH>(S, p.pos, p.mom, tmin, C.tmax, prd, status);
+        phx_trace<CV>(S, p.pos, p.mom, tmin, C.tmax, prd, status);
         if (prd.boundary() == 0xffffu) break;
         prd.normal = normalize(prd.normal);
         const int command = propagate(p, rng, prd, P, status);

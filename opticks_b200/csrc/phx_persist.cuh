@@ -79,12 +79,12 @@ PHX_D unsigned long long phx_globaltimer()
 #define PHX_STEPFN_P __device__ __forceinline__
 #endif
 
-template <bool POLISH>
+template <int CV>
 PHX_STEPFN_T PhxPRD phx_trace_step(const PhxScene S, const float3 o, const float3 d, const float tmin, const float tmax,
                                  unsigned& status)
 {
     PhxPRD prd;
-    phx_trace<POLISH>(S, o, d, tmin, tmax, prd, status);
+    phx_trace<CV>(S, o, d, tmin, tmax, prd, status);
     return prd;
 }
 
@@ -120,7 +120,7 @@ PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, lon
     }
 }
 
-template <bool POLISH, bool ADJ>
+template <int CV, bool ADJ>
 PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status, PhxScore* sc)
 {
     if (ADJ) {
@@ -154,7 +154,7 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
     L.ev = (int)ev;
 }
 
-template <bool POLISH, bool ADJ>
+template <int CV, bool ADJ>
 PHX_D void persist_finish(PhxLane& L, const PersistArgs& A, const PhxScore* sc)
 {
     const long long idx = L.idx;
@@ -182,14 +182,14 @@ PHX_D void persist_finish(PhxLane& L, const PersistArgs& A, const PhxScore* sc)
 }
 
 // one bounce of CSGOptiX/CSGOptiX7.cu:477-509; returns true when the photon is finished
-template <bool POLISH, bool ADJ>
+template <int CV, bool ADJ>
 PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status, PhxScore* sc)
 {
     if (!(L.bounce < A.C.max_bounce && L.p.time < A.C.max_time)) return true;
     const float tmin = (L.p.obf & A.C.eps0_mask) ? A.C.tmin0 : A.C.tmin;
     PhxPRD prd;
-    if (ADJ) phx_trace<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
-    else prd = phx_trace_step<POLISH>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, status);
+    if (ADJ) phx_trace<CV>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, prd, status);
+    else prd = phx_trace_step<CV>(A.S, L.p.pos, L.p.mom, tmin, A.C.tmax, status);
     if (prd.boundary() == 0xffffu) return true;
     int command;
     if (ADJ) {
@@ -210,7 +210,7 @@ PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status, PhxS
 #endif
 #define PHX_PERSIST_MINB(BLOCK) ((PHX_PERSIST_MIN_WARPS * 32 / (BLOCK)) > 0 ? (PHX_PERSIST_MIN_WARPS * 32 / (BLOCK)) : 1)
 
-template <bool POLISH, int BLOCK, bool ADJ = false>
+template <int CV, int BLOCK, bool ADJ = false>
 __global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persistent(PersistArgs A)
 {
     PhxScore score;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persiste
                 take = t;
             }
             if ((take >> lane) & 1u) {
-                persist_start<POLISH, ADJ>(L, A, wnext + __popc(take & lanes_below), status, sc);
+                persist_start<CV, ADJ>(L, A, wnext + __popc(take & lanes_below), status, sc);
                 active = true;
             }
             wnext += __popc(take);
@@ -257,8 +257,8 @@ __global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persiste
         }
         if (!__any_sync(FULL, active)) break;
         for (int k = 0; k < regroup; k++) {
-            if (active && persist_step<POLISH, ADJ>(L, A, status, sc)) {
-                persist_finish<POLISH, ADJ>(L, A, sc);
+            if (active && persist_step<CV, ADJ>(L, A, status, sc)) {
+                persist_finish<CV, ADJ>(L, A, sc);
                 active = false;
             }
         }

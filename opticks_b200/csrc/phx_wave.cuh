@@ -134,7 +134,7 @@ PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s) { wave_push(W.a
 // Lanes in `need` take new photons from the queue until each has a path that can be traced
 // (photons that cannot take a first bounce are finished at once) or the queue is empty.
 // Returns true in the lanes that hold a live path.  Warp-collective.
-template <bool POLISH, bool ADJ = false>
+template <int CV, bool ADJ = false>
 PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status, PhxScore* sc = nullptr)
 {
     const unsigned FULL = 0xffffffffu;
@@ -152,9 +152,9 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
             if (idx >= A.N) {
                 need = false;
             } else {
-                persist_start<POLISH, ADJ>(L, A, idx, status, sc);
+                persist_start<CV, ADJ>(L, A, idx, status, sc);
                 if (wave_can_trace(L, A)) { live = true; need = false; }
-                else persist_finish<POLISH, ADJ>(L, A, sc);
+                else persist_finish<CV, ADJ>(L, A, sc);
             }
         }
     }
@@ -162,7 +162,7 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
 }
 
 // fill the pool: every slot takes photons until it holds a live path or the queue is empty
-template <bool POLISH, bool ADJ = false>
+template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
 {
     unsigned status = 0;
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < W.pool; base += stride) {
         const long long s = base + (threadIdx.x & 31);
-        const bool live = wave_refill<POLISH, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
+        const bool live = wave_refill<CV, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
         if (live) {
             wave_store(W, (uint32_t)s, L);
             if (ADJ) wave_store_score(W, (uint32_t)s, &score);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
 #define PHX_WAVE_TRACE_MINB 3
 #endif
 
-template <bool POLISH>
+template <int CV>
 __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArgs W)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) { *W.n_out = 0u; *W.n_free = 0u; }   // the launches after this one append
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
         const float4 q0 = o->q0, q1 = o->q1;
         const unsigned obf = __float_as_uint(o->q3.x);
         const float tmin = (obf & W.A.C.eps0_mask) ? W.A.C.tmin0 : W.A.C.tmin;
-        const PhxPRD prd = phx_trace_step<POLISH>(W.A.S, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z), tmin,
+        const PhxPRD prd = phx_trace_step<CV>(W.A.S, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z), tmin,
                                                   W.A.C.tmax, status);
         W.prd[s].nd = make_float4(prd.normal.x, prd.normal.y, prd.normal.z, prd.distance);
         W.prd[s].lgi = make_uint4(__float_as_uint(prd.lposcost), prd.gp_bd, prd.ii_id, 0u);
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
 #define PHX_WAVE_SHADE_MINB 1
 #endif
 
-template <bool POLISH, bool ADJ = false>
+template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
     const unsigned n = *W.n_in;
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
                 seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
                 done = command == PHX_BREAK || !wave_can_trace(L, W.A);
             }
-            if (done) persist_finish<POLISH, ADJ>(L, W.A, ADJ ? &score : nullptr);
+            if (done) persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
             live = !done;
         }
         if (live) {
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
 }
 
 // new photons from the queue into the slots freed this round (warp-coherent generation)
-template <bool POLISH, bool ADJ = false>
+template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
 {
     const unsigned n = *W.n_free;
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
         const long long i = base + (threadIdx.x & 31);
         const bool valid = i < (long long)n;
         const uint32_t s = valid ? W.free_list[i] : 0u;
-        const bool live = wave_refill<POLISH, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
+        const bool live = wave_refill<CV, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
         if (live) {
             wave_store(W, s, L);
             if (ADJ) wave_store_score(W, s, &score);
