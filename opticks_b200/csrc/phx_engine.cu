@@ -155,6 +155,7 @@ static PhxScene scene_of(const phx_engine* e, int polish)
     S.leaf_sph = e->leaf_sph.p;
     S.global_sph = e->global_sph.p;
     S.num_global = e->num_global;
+    S.num_leaf = e->num_leaf;
     S.cull = make_float4(e->cull[0], e->cull[1], e->cull[2], e->cull[3]);
     S.bvh_empty = e->num_leaf == 0;
     S.empty = e->num_leaf == 0 && e->num_global == 0;
@@ -1015,17 +1016,21 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
     int rc;
     if ((rc = wave_grid(k_wave_init<CV, ADJ>, dev, g_init))) return rc;
+#if PHX_WAVE_TRACE_DF
+    if ((rc = wave_grid(k_wave_trace_df<CV>, dev, g_trace))) return rc;
+#else
     if ((rc = wave_grid(k_wave_trace<CV>, dev, g_trace))) return rc;
+#endif
     if ((rc = wave_grid(k_wave_shade<CV, ADJ>, dev, g_shade))) return rc;
     if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
     const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
-    PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(3));
+    PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
     const bool refill = N > pool;
     PHX_CU(e->wfree.ensure((size_t)pool));
     if (ADJ) PHX_CU(e->wscore.ensure((size_t)pool * 8));
-    PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 3 * sizeof(unsigned), st));
+    PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 4 * sizeof(unsigned), st));
     WaveArgs W;
     W.A = A;
     W.slot = e->wslot.p; W.prd = e->wprd.p; W.sidx = e->wsidx.p; W.pool = pool;
@@ -1034,6 +1039,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     W.free_list = e->wfree.p;
     W.score = ADJ ? e->wscore.p : nullptr;
     W.n_free = e->wcnt.p + 2;
+    W.trace_ctr = e->wcnt.p + 3;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
     k_wave_init<CV, ADJ><<<gi, 128, 0, st>>>(W);
@@ -1045,7 +1051,11 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     for (long long r = 0; r < max_rounds && !done;) {
         for (int k = 0; k < PHX_WAVE_ROUNDS; k++, r++) {
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
+#if PHX_WAVE_TRACE_DF
+            k_wave_trace_df<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+#else
             k_wave_trace<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+#endif
             k_wave_shade<CV, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
             if (refill) k_wave_fill<CV, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
             cur = 1 - cur;

@@ -22,6 +22,7 @@ struct PhxScene {
     PhxCsgCtx csg;
     float4 cull;                // ball no hierarchy leaf reaches: centre xyz, radius^2 (0: none)
     int num_global;
+    int num_leaf;               // hierarchy leaves (stack ranges from here on address the global leaves)
     int bvh_empty;              // no hierarchy leaves
     int empty;                  // no leaves at all
 };
@@ -70,6 +71,89 @@ PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, con
     }
 }
 
+// Visit BVH4 node ni: slab-test its four children against [tmin, tmax] and push the hit ones
+// (inner nodes and leaf ranges) far-to-near, so that the nearest is taken next.
+PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const float3& oi, float tmin, float tmax, int* stk, float* stt,
+                          int& sp, unsigned& status)
+{
+    const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
+    const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
+    const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(nf + 6));
+    const float lxa[4] = { lx.x, lx.y, lx.z, lx.w }, hxa[4] = { hx.x, hx.y, hx.z, hx.w };
+    const float lya[4] = { ly.x, ly.y, ly.z, ly.w }, hya[4] = { hy.x, hy.y, hy.z, hy.w };
+    const float lza[4] = { lz.x, lz.y, lz.z, lz.w }, hza[4] = { hz.x, hz.y, hz.z, hz.w };
+    const int cha[4] = { ch.x, ch.y, ch.z, ch.w };
+    float tn[4];
+    int hitmask = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float tx0 = fmaf(lxa[c], inv.x, oi.x), tx1 = fmaf(hxa[c], inv.x, oi.x);
+        const float ty0 = fmaf(lya[c], inv.y, oi.y), ty1 = fmaf(hya[c], inv.y, oi.y);
+        const float tz0 = fmaf(lza[c], inv.z, oi.z), tz1 = fmaf(hza[c], inv.z, oi.z);
+        const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+        const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+        // slab arithmetic slack: boxes are padded on the host, and a relative slack here
+        tn[c] = tnear;
+        if (cha[c] != 0 && tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
+    }
+    int order[4] = { 0, 1, 2, 3 };
+#pragma unroll
+    for (int i = 1; i < 4; i++)
+#pragma unroll
+        for (int j = i; j > 0; j--) {
+            if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
+        }
+#pragma unroll
+    for (int k = 3; k >= 0; k--) {
+        const int c = order[k];
+        if (!(hitmask & (1 << c))) continue;
+        if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
+        stk[sp] = cha[c]; stt[sp] = tn[c]; sp++;
+    }
+}
+
+// ray set-up shared by both traversal loops: reciprocal direction (zero components nudged) and
+// the slab offsets
+PHX_D void phx_ray_slabs(const float3& o, const float3& d, float3& inv, float3& oi)
+{
+    const float3 dd = make_float3(fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x,
+                                  fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y,
+                                  fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
+    inv = make_float3(1.f / dd.x, 1.f / dd.y, 1.f / dd.z);
+    oi = make_float3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
+}
+
+// The segment [tmin, t] lies inside the ball no hierarchy leaf reaches: skip the hierarchy.
+PHX_D bool phx_culled(const PhxScene& S, const float3& o, const float3& d, float tmin, float t)
+{
+    if (!(S.cull.w > 0.f)) return false;
+    const float3 c = make_float3(S.cull.x, S.cull.y, S.cull.z);
+    const float3 p0 = o + tmin * d - c;
+    const float3 p1 = o + t * d - c;
+    return dot(p0, p0) < S.cull.w && dot(p1, p1) < S.cull.w;
+}
+
+// PRD of a closest hit (CH program CSGOptiX/CSGOptiX7.cu:776-874), or of a miss
+PHX_D void phx_best_prd(const PhxScene& S, const PhxBest& B, PhxPRD& prd)
+{
+    if (B.L.x < 0) {
+        prd.gp_bd = 0xffffffffu;
+        prd.ii_id = 0xffffffffu;
+        prd.normal = make_float3(0.f, 0.f, 0.f);
+        prd.distance = 0.f;
+        prd.lposcost = 0.f;
+        return;
+    }
+    const float4* q = S.inst_inv + 4 * B.L.x;
+    float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
+    prd.normal = xform_col(m, make_float3(B.isect.x, B.isect.y, B.isect.z), 0.f);
+    prd.distance = B.t;
+    prd.lposcost = B.lposcost;
+    prd.gp_bd = (unsigned)B.L.z;
+    prd.ii_id = (unsigned)B.L.w;
+}
+
 // Closest hit over all (instance, prim) leaves: restates optixTrace over the IAS with the
 // IS program CSGOptiX/CSGOptiX7.cu:896-967 (object-frame intersect_prim, lposcost) and the
 // CH program :776-874 (object->world normal, iindex<<16|identity, globalPrimIdx<<16|boundary).
@@ -92,19 +176,9 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
     B.lposcost = 0.f;
     for (int g = 0; g < S.num_global; g++)
         phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B, status);
-    bool traverse = !S.bvh_empty;
-    if (traverse && S.cull.w > 0.f) {
-        const float3 c = make_float3(S.cull.x, S.cull.y, S.cull.z);
-        const float3 p0 = o + tmin * d - c;
-        const float3 p1 = o + B.t * d - c;
-        traverse = !(dot(p0, p0) < S.cull.w && dot(p1, p1) < S.cull.w);
-    }
-    if (traverse) {
-        const float3 dd = make_float3(fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x,
-                                      fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y,
-                                      fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
-        const float3 inv = make_float3(1.f / dd.x, 1.f / dd.y, 1.f / dd.z);
-        const float3 oi = make_float3(-o.x * inv.x, -o.y * inv.y, -o.z * inv.z);
+    if (!S.bvh_empty && !phx_culled(S, o, d, tmin, B.t)) {
+        float3 inv, oi;
+        phx_ray_slabs(o, d, inv, oi);
         int stk[PHX_BVH_STACK];
         float stt[PHX_BVH_STACK];
         int sp = 0;
@@ -133,53 +207,11 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                                           B, status);
                 continue;
             }
-            const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
-            const float4 lx = __ldg(nf + 0), hx = __ldg(nf + 1), ly = __ldg(nf + 2), hy = __ldg(nf + 3);
-            const float4 lz = __ldg(nf + 4), hz = __ldg(nf + 5);
-            const int4 ch = __ldg(reinterpret_cast<const int4*>(nf + 6));
-            const float lxa[4] = { lx.x, lx.y, lx.z, lx.w }, hxa[4] = { hx.x, hx.y, hx.z, hx.w };
-            const float lya[4] = { ly.x, ly.y, ly.z, ly.w }, hya[4] = { hy.x, hy.y, hy.z, hy.w };
-            const float lza[4] = { lz.x, lz.y, lz.z, lz.w }, hza[4] = { hz.x, hz.y, hz.z, hz.w };
-            const int cha[4] = { ch.x, ch.y, ch.z, ch.w };
-            float tn[4];
-            int hitmask = 0;
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const float tx0 = fmaf(lxa[c], inv.x, oi.x), tx1 = fmaf(hxa[c], inv.x, oi.x);
-                const float ty0 = fmaf(lya[c], inv.y, oi.y), ty1 = fmaf(hya[c], inv.y, oi.y);
-                const float tz0 = fmaf(lza[c], inv.z, oi.z), tz1 = fmaf(hza[c], inv.z, oi.z);
-                const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
-                const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), B.t));
-                // slab arithmetic slack: boxes are padded on the host, and a relative slack here
-                tn[c] = tnear;
-                if (cha[c] != 0 && tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
-            }
-            // push the hit children (inner nodes and leaf ranges) far-to-near: the nearest is next
-            int order[4] = { 0, 1, 2, 3 };
-#pragma unroll
-            for (int i = 1; i < 4; i++)
-#pragma unroll
-                for (int j = i; j > 0; j--) {
-                    if (tn[order[j]] < tn[order[j - 1]]) { int t = order[j]; order[j] = order[j - 1]; order[j - 1] = t; }
-                }
-#pragma unroll
-            for (int k = 3; k >= 0; k--) {
-                const int c = order[k];
-                if (!(hitmask & (1 << c))) continue;
-                if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
-                stk[sp] = cha[c]; stt[sp] = tn[c]; sp++;
-            }
+            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, stt, sp, status);
         }
     }
-    if (B.L.x < 0) return false;
-    const float4* q = S.inst_inv + 4 * B.L.x;
-    float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
-    prd.normal = xform_col(m, make_float3(B.isect.x, B.isect.y, B.isect.z), 0.f);
-    prd.distance = B.t;
-    prd.lposcost = B.lposcost;
-    prd.gp_bd = (unsigned)B.L.z;
-    prd.ii_id = (unsigned)B.L.w;
-    return true;
+    phx_best_prd(S, B, prd);
+    return B.L.x >= 0;
 }
 
 struct PhxLoopCfg {

@@ -47,6 +47,7 @@ struct WaveArgs {
     float4* score;            // ADJ: 8 float4 (the 32 score terms) per slot
     uint32_t* free_list;      // slots freed by this round's physics (refilled by k_wave_fill)
     unsigned* n_free;
+    unsigned* trace_ctr;      // rays of this round handed to warps (k_wave_trace_df); zeroed by the kernel before
     long long pool;           // slots (init only)
 };
 
@@ -210,6 +211,113 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
     if (status) atomicOr(W.A.status, status);
 }
 
+// The closest-hit round with persistent warps that refill finished lanes: each warp takes the
+// round's rays 32 indices at a time (one atomic per 32 rays), and whenever lanes of the warp have
+// finished their ray they start the next ones of the window, so the warp keeps stepping with
+// most lanes busy instead of waiting for its slowest ray.  A ray starts by testing the global
+// leaves, then (unless the cull ball holds the whole segment) walks the hierarchy from its own
+// stack, in the same order and with the same arithmetic as phx_trace: the PRDs are the same as
+// the plain kernel's.
+#ifndef PHX_WAVE_TRACE_DF
+#define PHX_WAVE_TRACE_DF 1
+#endif
+// idle lanes a warp waits for before it takes new rays (32: refill only when the whole warp is done)
+#ifndef PHX_WAVE_TRACE_REFILL
+#define PHX_WAVE_TRACE_REFILL 12
+#endif
+template <int CV>
+__global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(WaveArgs W)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *W.n_out = 0u; *W.n_free = 0u; }   // the launches after this one append
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned n = *W.n_in;
+    const PhxScene& S = W.A.S;
+    unsigned status = 0;
+    unsigned wnext = 0u, wend = 0u;       // this warp's unassigned ray indices [wnext, wend)
+    bool drained = false;                 // the round's rays are all handed out
+    bool has = false;                     // this lane holds a ray
+    uint32_t s = 0u;
+    float3 o = make_float3(0.f, 0.f, 0.f), d = o, inv = o, oi = o;
+    float tmin = 0.f;
+    PhxBest B;
+    B.t = 0.f; B.L = make_int4(-1, 0, 0, 0); B.isect = make_float4(0.f, 0.f, 0.f, 0.f); B.lposcost = 0.f;
+    int stk[PHX_BVH_STACK];
+    float stt[PHX_BVH_STACK];
+    int sp = 0;
+    for (;;) {
+        // hand new rays to the idle lanes (at most a window and a fresh window per step)
+        unsigned idle = __ballot_sync(FULL, !has);
+        if (__popc(idle) < PHX_WAVE_TRACE_REFILL) idle = 0u;
+        for (int pass = 0; pass < 2 && idle != 0u && !drained; pass++) {
+            if (wnext >= wend) {
+                unsigned b = 0u;
+                if (lane == 0u) b = atomicAdd(W.trace_ctr, 32u);
+                b = __shfl_sync(FULL, b, 0);
+                if (b >= n) { drained = true; break; }
+                wnext = b;
+                wend = min(b + 32u, n);
+            }
+            const unsigned take = min((unsigned)__popc(idle), wend - wnext);
+            const unsigned rank = __popc(idle & below);
+            if (!has && rank < take) {
+                s = W.act_in[wnext + rank];
+                const PhxWaveSlot* ps = W.slot + s;
+                const float4 q0 = ps->q0, q1 = ps->q1;
+                const unsigned obf = __float_as_uint(ps->q3.x);
+                tmin = (obf & W.A.C.eps0_mask) ? W.A.C.tmin0 : W.A.C.tmin;
+                o = make_float3(q0.x, q0.y, q0.z);
+                d = make_float3(q1.x, q1.y, q1.z);
+                phx_ray_slabs(o, d, inv, oi);
+                B.t = W.A.C.tmax; B.L = make_int4(-1, 0, 0, 0); B.isect = make_float4(0.f, 0.f, 0.f, 0.f); B.lposcost = 0.f;
+                sp = 0;
+                // the global leaves first, then the hierarchy unless the cull ball holds the segment
+                for (int g = 0; g < S.num_global; g++)
+                    phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B,
+                                      status);
+                if (!S.bvh_empty && !phx_culled(S, o, d, tmin, B.t)) { stk[0] = 0; stt[0] = tmin; sp = 1; }
+                has = true;
+            }
+            wnext += take;
+            idle = __ballot_sync(FULL, !has);
+        }
+        // finish the rays whose stacks are empty
+        if (has) {
+            while (sp > 0 && stt[sp - 1] > B.t) sp--;
+            if (sp == 0) {
+                PhxPRD prd;
+                phx_best_prd(S, B, prd);
+                W.prd[s].nd = make_float4(prd.normal.x, prd.normal.y, prd.normal.z, prd.distance);
+                W.prd[s].lgi = make_uint4(__float_as_uint(prd.lposcost), prd.gp_bd, prd.ii_id, 0u);
+                has = false;
+            }
+        }
+        const bool leaf_top = has && stk[sp - 1] < 0;
+        const unsigned want_leaf = __ballot_sync(FULL, leaf_top);
+        const unsigned want_node = __ballot_sync(FULL, has && !leaf_top);
+        if (!(want_leaf | want_node)) {
+            if (drained) break;
+            continue;
+        }
+        // one step: the lanes whose next entry is a leaf range, or those whose next entry is a node
+        const bool leaf_step = want_node == 0u || __popc(want_leaf) * PHX_TRACE_LEAF_WEIGHT >= __popc(want_node);
+        if (!has || leaf_top != leaf_step) continue;
+        sp--;
+        const int ni = stk[sp];
+        if (leaf_step) {
+            const int enc = -ni - 1;
+            const int first = enc >> 3;
+            const int count = (enc & 7) + 1;
+            for (int li = first; li < first + count; li++)
+                phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin, B, status);
+        } else {
+            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, stt, sp, status);
+        }
+    }
+    if (status) atomicOr(W.A.status, status);
+}
+
 // physics of every live path after its closest hit (CSGOptiX/CSGOptiX7.cu:491-509), finishing
 // and refilling slots; live slots go to the next round's list
 // resident 128-thread blocks per SM asked for the physics kernel (its loads of path state are
@@ -221,6 +329,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
 template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && W.trace_ctr) *W.trace_ctr = 0u;   // for the next round's closest-hit kernel
     const unsigned n = *W.n_in;
     unsigned status = 0;
     PhxLane L;
