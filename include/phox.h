@@ -85,7 +85,10 @@ typedef struct {
     uint32_t* sensor_hits;  /* (num_sensor) hits per sensor (identity-1), or NULL */
     int64_t   num_photon;   /* out */
     int64_t   num_hit;      /* out : hits selected (may exceed hit_capacity; then status has HIT_OVERFLOW) */
-    uint32_t  status;       /* out : PHX_STATUS_* bits */
+    uint32_t  status;       /* out : status bits: 0x1 CSG evaluator stack error, 0x2 traversal stack
+                               overflow, 0x4 rejection-loop cap, 0x8 hit overflow, 0x10 photon index
+                               beyond the prepared RNG states, 0x20 queue watchdog, 0x40 input photon
+                               index beyond the input photon array */
 } phx_outputs;
 
 void        phx_config_default(phx_config* cfg);
@@ -179,6 +182,16 @@ int phx_merge_hits_device(phx_engine* e, const void* d_in, int64_t num_in, int32
 /* host arrays in and out; same semantics */
 int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, uint32_t select_flagmask, float time_window,
                    void* out, int64_t out_capacity, int64_t* num_out);
+
+/* Input photons (SEvt::setInputPhoton sysrap/SEvt.cc:602-640, uploaded as in qudarap/QEvt.cc:540-560):
+ * a genstep of gencode 19 (OpticksGenstep_INPUT_PHOTON, numphoton N) makes each of its photons a
+ * copy of photon[photon index] (sphoton rows, (num_photon,4,4) float32) with the TORCH flag set
+ * (qudarap/qsim.h:2557); the photon index is the absolute one of phx_simulate_device.  An index
+ * beyond num_photon leaves the photon zero and sets PHX_STATUS_INPUT_RANGE.  The host form copies
+ * the array to the device; the device form uses the caller's buffer (16-byte aligned, kept alive
+ * and unchanged while calls use it).  num_photon 0 clears.  Gencode 14 (CARRIER) needs no input. */
+int phx_set_input_photon(phx_engine* e, const float* photon, int64_t num_photon);
+int phx_set_input_photon_device(phx_engine* e, const float* d_photon, int64_t num_photon);
 
 /* Diagnostics of the last phx_simulate / phx_simulate_device call on this engine (no reference
  * counterpart): kernels it launched and, in kernel_mode 2, wavefront rounds (one closest-hit and

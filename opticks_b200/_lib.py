@@ -78,6 +78,8 @@ SIGNATURES = {
     "phx_merge_hits": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint32, C.c_float, C.c_void_p, C.c_int64,
                                  C.POINTER(C.c_int64)]),
     "phx_last_call_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "phx_set_input_photon": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "phx_set_input_photon_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
 }
 
 

@@ -103,6 +103,9 @@ struct phx_engine {
     cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr;
     cudaTextureObject_t bnd_tex = 0, icdf_tex = 0;
     DevBuf<uint4> optical;
+    DevBuf<float4> input_own;              // input photons copied from the host
+    const float4* input_photon = nullptr;  // the input photons in use (input_own or a caller's buffer)
+    long long num_input_photon = 0;
     float nm0 = 60.f, nms = 1.f;
     unsigned nx = 0, ny = 0, hd_factor = 20;
     int num_bnd = 0;
@@ -173,6 +176,8 @@ static PhxProps props_of(const phx_engine* e)
     P.ny = e->ny;
     P.icdf_tex = e->icdf_tex;
     P.hd_factor = e->hd_factor;
+    P.input_photon = e->input_photon;
+    P.num_input_photon = e->num_input_photon;
     return P;
 }
 
@@ -1816,6 +1821,34 @@ int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, 
         PHX_CU(cudaMemcpyAsync(out, w.hout.p, (size_t)no * rb, cudaMemcpyDeviceToHost, st));
     }
     PHX_CU(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// SEvt::setInputPhoton (sysrap/SEvt.cc:602-640) with QEvt's upload of the input photons
+// (qudarap/QEvt.cc:540-560): INPUT_PHOTON gensteps copy photon[photon index] and set TORCH.
+int phx_set_input_photon(phx_engine* e, const float* photon, int64_t num_photon)
+{
+    if (!e) return phx_fail(-1, "phx_set_input_photon: null engine");
+    if (num_photon < 0 || (num_photon > 0 && !photon)) return phx_fail(-1, "phx_set_input_photon: bad array");
+    PHX_CU(cudaSetDevice(e->device));
+    e->input_photon = nullptr;
+    e->num_input_photon = 0;
+    if (num_photon == 0) { e->input_own.release(); return 0; }
+    PHX_CU(e->input_own.ensure((size_t)num_photon * 4));
+    PHX_CU(cudaMemcpy(e->input_own.p, photon, (size_t)num_photon * 64, cudaMemcpyHostToDevice));
+    e->input_photon = e->input_own.p;
+    e->num_input_photon = num_photon;
+    return 0;
+}
+
+int phx_set_input_photon_device(phx_engine* e, const float* d_photon, int64_t num_photon)
+{
+    if (!e) return phx_fail(-1, "phx_set_input_photon_device: null engine");
+    if (num_photon < 0 || (num_photon > 0 && !d_photon)) return phx_fail(-1, "phx_set_input_photon_device: bad array");
+    if (((uintptr_t)d_photon & 15u) != 0u) return phx_fail(-1, "phx_set_input_photon_device: array not 16-byte aligned");
+    e->input_own.release();
+    e->input_photon = num_photon > 0 ? reinterpret_cast<const float4*>(d_photon) : nullptr;
+    e->num_input_photon = num_photon;
     return 0;
 }
 

@@ -118,6 +118,8 @@ struct PhxProps {
     unsigned nx, ny;                // texture width/height
     cudaTextureObject_t icdf_tex;   // 4096 x 3 float, linear, normalized, wrap
     unsigned hd_factor;
+    const float4* input_photon;     // (num_input_photon*4) sphoton rows for INPUT_PHOTON gensteps, or null
+    long long num_input_photon;
 };
 
 PHX_D float phx_uniform(curandStateXORWOW& r) { return curand_uniform(&r); }
@@ -386,6 +388,28 @@ PHX_D void generate_cerenkov(PhxPhoton& p, curandStateXORWOW& rng, const float4*
     p.set_flag(PHX_CERENKOV);
 }
 
+// scarrier::generate sysrap/scarrier.h: the photon is the genstep's rows 2-5, moved 10 mm in y per photon
+PHX_D void generate_carrier(PhxPhoton& p, const float4* g, unsigned long long photon_id)
+{
+    p.pos = make_float3(g[2].x, g[2].y + float(photon_id) * 10.f, g[2].z); p.time = g[2].w;
+    p.mom = make_float3(g[3].x, g[3].y, g[3].z); p.hitcount_iindex = __float_as_uint(g[3].w);
+    p.pol = make_float3(g[4].x, g[4].y, g[4].z); p.wavelength = g[4].w;
+    p.obf = __float_as_uint(g[5].x); p.identity = __float_as_uint(g[5].y);
+    p.index = __float_as_uint(g[5].z); p.flagmask = __float_as_uint(g[5].w);
+    p.set_flag(PHX_TORCH);
+}
+
+// an sphoton (4 float4 rows) as given: an input photon (qudarap/qsim.h:2557, evt->photon[photon_id])
+PHX_D void phx_load_sphoton(PhxPhoton& p, const float4* r)
+{
+    const float4 q0 = __ldg(r + 0), q1 = __ldg(r + 1), q2 = __ldg(r + 2), q3 = __ldg(r + 3);
+    p.pos = make_float3(q0.x, q0.y, q0.z); p.time = q0.w;
+    p.mom = make_float3(q1.x, q1.y, q1.z); p.hitcount_iindex = __float_as_uint(q1.w);
+    p.pol = make_float3(q2.x, q2.y, q2.z); p.wavelength = q2.w;
+    p.obf = __float_as_uint(q3.x); p.identity = __float_as_uint(q3.y);
+    p.index = __float_as_uint(q3.z); p.flagmask = __float_as_uint(q3.w);
+}
+
 // qsim::generate_photon qudarap/qsim.h:2532-2561
 PHX_COLD void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
 {
@@ -396,6 +420,12 @@ PHX_COLD void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4
         case PHX_GS_CERENKOV: generate_cerenkov(p, rng, g, P, status); break;
         case PHX_GS_DsG4Scintillation_r4695:
         case PHX_GS_SCINTILLATION: generate_scint(p, rng, g, P); break;
+        case PHX_GS_CARRIER: generate_carrier(p, g, photon_id); break;
+        case PHX_GS_INPUT_PHOTON:
+            if (P.input_photon && (long long)photon_id < P.num_input_photon) phx_load_sphoton(p, P.input_photon + 4 * photon_id);
+            else status |= PHX_STATUS_INPUT_RANGE;
+            p.set_flag(PHX_TORCH);
+            break;
         default: break;
     }
     p.set_index(photon_id);

@@ -41,9 +41,11 @@ enum {
     PHX_GS_G4Scintillation_1042    = 2,
     PHX_GS_DsG4Scintillation_r4695 = 5,
     PHX_GS_TORCH                   = 6,
+    PHX_GS_CARRIER                 = 14,
     PHX_GS_CERENKOV                = 15,
     PHX_GS_SCINTILLATION           = 16,
-    PHX_GS_G4Cerenkov_modified     = 18
+    PHX_GS_G4Cerenkov_modified     = 18,
+    PHX_GS_INPUT_PHOTON            = 19
 };
 
 // ---- torch source shapes (storch q5.u.w) ----
@@ -104,7 +106,8 @@ enum {
     PHX_STATUS_LOOP_CAP         = 0x1 << 2,  // a rejection loop hit its iteration cap
     PHX_STATUS_HIT_OVERFLOW     = 0x1 << 3,  // more hits than the hit buffer holds
     PHX_STATUS_RNG_RANGE        = 0x1 << 4,  // photon index beyond the prepared RNG states
-    PHX_STATUS_QUEUE_WATCHDOG   = 0x1 << 5   // persistent queue gave up
+    PHX_STATUS_QUEUE_WATCHDOG   = 0x1 << 5,  // persistent queue gave up
+    PHX_STATUS_INPUT_RANGE      = 0x1 << 6   // INPUT_PHOTON genstep beyond the input photon array (photon left zero)
 };
 
 #define PHX_NSEQ 2

@@ -21,6 +21,7 @@ from ._lib import PhxConfig, PhxGeometry, PhxOutputs, PhxPhysics
 # status bits (phx_pod.h)
 STATUS_NAMES = {
     0x1: "CSG_STACK", 0x2: "BVH_STACK", 0x4: "LOOP_CAP", 0x8: "HIT_OVERFLOW", 0x10: "RNG_RANGE", 0x20: "QUEUE_WATCHDOG",
+    0x40: "INPUT_RANGE",
 }
 
 FLAG = dict(CK=0x1, SI=0x2, TO=0x4, AB=0x8, RE=0x10, SC=0x20, SD=0x40, SA=0x80, DR=0x100, SR=0x200, BR=0x400, BT=0x800)
@@ -200,6 +201,24 @@ class Engine:
         _lib.check(_lib.lib().phx_rng_sequence(self._h, int(eventID), int(photon_offset), int(num_photon),
                                                int(num_per_photon), _ptr(out)), "phx_rng_sequence")
         return out
+
+    def set_input_photon(self, photon) -> None:
+        """SEvt::setInputPhoton: (N,4,4) float32 sphoton rows that INPUT_PHOTON gensteps (gencode 19)
+        copy; a torch tensor on the engine's device is used in place (kept alive here), anything
+        else is copied to the device; None clears"""
+        if photon is None:
+            self._input = None
+            _lib.check(_lib.lib().phx_set_input_photon(self._h, None, 0), "phx_set_input_photon")
+            return
+        if hasattr(photon, "data_ptr") and getattr(photon, "is_cuda", False):
+            assert photon.dtype.itemsize == 4 and photon.is_contiguous() and photon.shape[1:] == (4, 4)
+            self._input = photon
+            _lib.check(_lib.lib().phx_set_input_photon_device(self._h, C.c_void_p(photon.data_ptr()), int(photon.shape[0])),
+                       "phx_set_input_photon_device")
+            return
+        a = np.ascontiguousarray(photon, dtype=np.float32).reshape(-1, 4, 4)
+        self._input = None
+        _lib.check(_lib.lib().phx_set_input_photon(self._h, _ptr(a), len(a)), "phx_set_input_photon")
 
     def last_call_stats(self) -> dict:
         """kernel launches and wavefront rounds of the last simulate call"""

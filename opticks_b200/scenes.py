@@ -22,6 +22,8 @@ from . import material as M
 GS_TORCH = 6
 GS_SCINTILLATION = 16
 GS_CERENKOV = 15
+GS_CARRIER = 14
+GS_INPUT_PHOTON = 19
 T_SPHERE = 7
 T_SPHERE_RANDPOL = 64    # T_SPHERE with a random linear polarisation (one extra uniform)
 T_POINT = 3
@@ -48,6 +50,41 @@ def torch_genstep(numphoton: int, pos=(0.0, 0.0, 0.0), wavelength=440.0, radius=
     gi[5, 2] = 0
     gi[5, 3] = type_
     return g
+
+
+def input_photon_genstep(num_photon: int) -> np.ndarray:
+    """SEvent::MakeInputPhotonGenstep (sysrap/SEvent.cc:120-133): gencode INPUT_PHOTON and the photon
+    count; the photons themselves are set on the engine (Engine.set_input_photon)"""
+    g = np.zeros((6, 4), dtype=np.float32)
+    g.view(np.int32)[0] = (GS_INPUT_PHOTON, 0, 0, num_photon)
+    return g
+
+
+def carrier_genstep(numphoton: int, pos=(0.0, 0.0, 0.0), time=0.0, mom=(1.0, 0.0, 0.0), pol=(0.0, 1.0, 0.0),
+                    wavelength=500.0) -> np.ndarray:
+    """scarrier (sysrap/scarrier.h): rows 2-5 are the photon itself (moved 10 mm in y per photon)"""
+    g = np.zeros((6, 4), dtype=np.float32)
+    g.view(np.int32)[0] = (GS_CARRIER, 0, 0, numphoton)
+    g[2] = (*pos, time)
+    g[3, :3] = mom
+    g[4] = (*pol, wavelength)
+    return g
+
+
+def input_photons(n: int, seed: int = 0, radius: float = 100.0, wavelength: float = 440.0) -> np.ndarray:
+    """(n,4,4) sphoton rows: positions in a ball, isotropic directions, transverse polarisations"""
+    rng = np.random.default_rng(seed)
+    p = np.zeros((n, 4, 4), np.float32)
+    p[:, 0, :3] = uniform_ball(n, radius, rng)
+    p[:, 0, 3] = rng.uniform(0.0, 1.0, n)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = np.cross(d, rng.normal(size=(n, 3)))
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    p[:, 1, :3] = d
+    p[:, 2, :3] = t
+    p[:, 2, 3] = wavelength
+    return p
 
 
 def scint_genstep(numphoton: int, pos, matline: int, time=0.0, delta=(0.0, 0.0, 1.0), step_length=1.0,

@@ -217,6 +217,8 @@ typedef struct {
     int polish;
     const float* pair_bbox;     /* (Np,6) padded world boxes, or NULL for no culling */
     const float* plan;          /* (Nl,4) convex polyhedron planes, or NULL */
+    const float* input_photon;  /* (num_input,4,4) sphoton rows for INPUT_PHOTON gensteps, or NULL */
+    long long num_input;
 } oracle_scene;
 
 typedef struct { const float* u; int n; int k; int over; } ustream;
@@ -325,6 +327,16 @@ static void gen_torch(photon_t* p, ustream* r, const float* g, unsigned long lon
         p->pol = V(0.f, -1.f, 0.f); rotate_uz(&p->pol, p->mom);
     }
     zero_flags(p);
+    set_flag(p, 0x4);
+}
+
+/* scarrier::generate sysrap/scarrier.h: genstep rows 2-5, moved 10 mm in y per photon index */
+static void gen_carrier(photon_t* p, const float* g, unsigned long long pid)
+{
+    p->pos.x = g[8]; p->pos.y = g[9] + (float)pid * 10.f; p->pos.z = g[10]; p->time = g[11];
+    p->mom.x = g[12]; p->mom.y = g[13]; p->mom.z = g[14]; memcpy(&p->hitcount_iindex, g + 15, 4);
+    p->pol.x = g[16]; p->pol.y = g[17]; p->pol.z = g[18]; p->wavelength = g[19];
+    memcpy(&p->obf, g + 20, 4); memcpy(&p->identity, g + 21, 4); memcpy(&p->index, g + 22, 4); memcpy(&p->flagmask, g + 23, 4);
     set_flag(p, 0x4);
 }
 
@@ -700,6 +712,12 @@ static int run_photons(const oracle_scene* S, const float* gs, int G, long long 
         if (code == 6) gen_torch(&p, &r, g, (unsigned long long)idx);
         else if (code == 16 || code == 5) gen_scint(&p, &r, g, S);
         else if (code == 15 || code == 18) gen_cerenkov(&p, &r, g, S);
+        else if (code == 14) gen_carrier(&p, g, (unsigned long long)idx);
+        else if (code == 19) {
+            /* qudarap/qsim.h:2557: the input photon as given, TORCH flag set */
+            if (S->input_photon && idx < S->num_input) memcpy(&p, S->input_photon + 16 * (size_t)idx, sizeof(p));
+            set_flag(&p, 0x4);
+        }
         p.index = (unsigned)(idx & 0xffffffffu);
         p.identity = ((unsigned)((idx >> 32) & 0xff) << 24) | (p.identity & 0xffffffu);
         uint64_t his[2] = { 0, 0 }, bn[2] = { 0, 0 };

@@ -40,7 +40,7 @@ class OracleScene(C.Structure):
         ("optical", C.c_void_p), ("icdf", C.c_void_p), ("icdf_w", C.c_int), ("icdf_h", C.c_int), ("hd_factor", C.c_int),
         ("max_bounce", C.c_int), ("max_time", C.c_float), ("tmin", C.c_float), ("tmin0", C.c_float),
         ("eps0_mask", C.c_uint), ("hit_mask", C.c_uint), ("polish", C.c_int),
-        ("pair_bbox", C.c_void_p), ("plan", C.c_void_p),
+        ("pair_bbox", C.c_void_p), ("plan", C.c_void_p), ("input_photon", C.c_void_p), ("num_input", C.c_longlong),
     ]
 
 
@@ -136,7 +136,7 @@ class Scene:
     """keeps the arrays alive behind an OracleScene"""
 
     def __init__(self, geom: dict, phys: dict, max_bounce=31, max_time=1e27, tmin=0.05, tmin0=0.05,
-                 eps0_mask=0x4 | 0x1 | 0x2 | 0x20 | 0x10, hit_mask=0x40, polish=0, cull=True):
+                 eps0_mask=0x4 | 0x1 | 0x2 | 0x20 | 0x10, hit_mask=0x40, polish=0, cull=True, input_photon=None):
         self.node = np.ascontiguousarray(geom["node"], np.float32)
         itra = geom.get("itra")
         self.itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
@@ -153,7 +153,13 @@ class Scene:
             len(self.pin), _p(self.bnd), nwl, nb * 8, float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)),
             _p(self.optical), _p(self.icdf), 0 if self.icdf is None else self.icdf.shape[1],
             0 if self.icdf is None else self.icdf.shape[0], int(phys.get("hd_factor", 20)),
-            max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox), _p(self.plan))
+            max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox), _p(self.plan),
+            None, 0)
+        self.input_photon = None
+        if input_photon is not None:
+            self.input_photon = np.ascontiguousarray(input_photon, np.float32).reshape(-1, 4, 4)
+            self.s.input_photon = _p(self.input_photon)
+            self.s.num_input = len(self.input_photon)
 
     def simulate(self, gs: np.ndarray, uniforms: np.ndarray, first: int = 0):
         gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
@@ -287,14 +293,14 @@ def ref_scan_gpu(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, pla
 
 
 # gencodes the driver gives the reference's qsim::generate_photon everything for
-# (qudarap/qsim.h:2532-2561): torch, Cerenkov and scintillation
-REF_GENCODES = (6, 15, 16)
+# (qudarap/qsim.h:2532-2561): torch, carrier, Cerenkov, scintillation, and input photons when given
+REF_GENCODES = (6, 14, 15, 16, 19)
 # torch types the reference's storch::generate fills a photon for (sysrap/storchtype.h:8-18,
 # sysrap/storch.h:207-470): disc, line, point, circle, rectangle, sphere_marsaglia, sphere
 REF_TORCH_TYPES = range(1, 8)
 
 
-def ref_genstep_check(gs: np.ndarray) -> None:
+def ref_genstep_check(gs: np.ndarray, have_input: bool = False) -> None:
     """refuse gensteps the reference's device code is not given the means to generate: a torch
     genstep of another type, or without a wavelength, leaves the photon's wavelength at zero, and
     qsim::generate_photon then samples the Planck texture (qudarap/qsim.h:2541-2544), which this
@@ -304,13 +310,15 @@ def ref_genstep_check(gs: np.ndarray) -> None:
         code = int(gi[k, 0, 0])
         if code not in REF_GENCODES:
             raise ValueError(f"genstep {k}: gencode {code} is not one the reference driver generates")
+        if code == 19 and not have_input:
+            raise ValueError(f"genstep {k}: INPUT_PHOTON genstep without input photons")
         if code == 6 and (int(gi[k, 5, 3]) not in REF_TORCH_TYPES or not gs[k, 3, 3] > 0.0):
             raise ValueError(f"genstep {k}: torch type {int(gi[k, 5, 3])} / wavelength {gs[k, 3, 3]} is not a reference torch genstep")
 
 
 def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 0, seed: int = 0, skip: int = 100000,
                      max_bounce: int = 31, max_time: float = 1e27, tmin: float = 0.05, tmin0: float = 0.05,
-                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10, record: bool = False):
+                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10, record: bool = False, input_photon=None):
     """run the reference's qsim on the GPU through ref_sim.cu; returns photon (N,4,4), seq (N,2,2)
     and, with ``record``, the per-point sphoton records (N,max_bounce+1,4,4) and per-trace prd
     (N,max_bounce+1,2,4) that the reference's sctx::point / sctx::trace write"""
@@ -324,7 +332,7 @@ def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 
                   C.c_ulonglong, C.c_ulonglong, C.c_int,
                   C.c_void_p, C.c_int, C.c_longlong,
                   C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint,
-                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]
     node = np.ascontiguousarray(geom["node"], np.float32)
     itra = geom.get("itra")
     itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
@@ -334,7 +342,8 @@ def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 
     icdf = phys.get("icdf")
     icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
     gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
-    ref_genstep_check(gs)
+    inp = None if input_photon is None else np.ascontiguousarray(input_photon, np.float32).reshape(-1, 4, 4)
+    ref_genstep_check(gs, inp is not None)
     N = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
     photon = np.zeros((N, 4, 4), np.float32)
     seq = np.zeros((N, 2, 2), np.uint64)
@@ -347,7 +356,7 @@ def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 
            _p(bnd), bnd.shape[0], bnd.shape[3], float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)), _p(optical),
            _p(icdf), 0 if icdf is None else icdf.shape[1], 0 if icdf is None else icdf.shape[0], int(phys.get("hd_factor", 20)),
            seed, skip, event_index, _p(gs), len(gs), N, max_bounce, max_time, tmin, tmin0, eps0_mask, _p(photon), _p(seq),
-           _p(rec) if record else None, _p(prd) if record else None, max_record)
+           _p(rec) if record else None, _p(prd) if record else None, max_record, _p(inp), 0 if inp is None else len(inp))
     if rc != 0:
         raise RuntimeError(f"ref_sim_run failed {rc}")
     return (photon, seq, rec, prd) if record else (photon, seq)

@@ -181,7 +181,8 @@ extern "C" int ref_sim_run(
     unsigned long long seed, unsigned long long skip, int event_index,
     const float* gs, int G, long long N,
     int max_bounce, float max_time, float tmin, float tmin0, unsigned eps0mask,
-    float* photon_out, unsigned long long* seq_out, float* record_out, float* prd_out, int max_record)
+    float* photon_out, unsigned long long* seq_out, float* record_out, float* prd_out, int max_record,
+    const float* input_photon, long long num_input)
 {
     // record_out (N, max_record, 4, 4) sphoton per point and prd_out (N, max_record, 2, 4) quad2 per
     // trace, as the reference's sctx::point / sctx::trace write them; max_record >= max_bounce + 1
@@ -250,6 +251,11 @@ extern "C" int ref_sim_run(
     ev_h.genstep = up((const quad6*)gs, (size_t)G);
     ev_h.seed = up(seed_h.data(), (size_t)N);
     cudaMalloc(&ev_h.photon, sizeof(sphoton) * (N > 0 ? N : 1));
+    // input photons: generate_photon copies evt->photon[photon_id] (qudarap/qsim.h:2557), as QEvt
+    // uploads them before the launch (qudarap/QEvt.cc:540-560)
+    cudaMemset(ev_h.photon, 0, sizeof(sphoton) * (N > 0 ? N : 1));
+    if (input_photon && num_input > 0 && N > 0)
+        cudaMemcpy(ev_h.photon, input_photon, sizeof(sphoton) * (size_t)(num_input < N ? num_input : N), cudaMemcpyHostToDevice);
     cudaMalloc(&ev_h.seq, sizeof(sseq) * (N > 0 ? N : 1));
     cudaMemset(ev_h.seq, 0, sizeof(sseq) * (N > 0 ? N : 1));
     const size_t nrec = record_out && N > 0 ? (size_t)N * (size_t)max_record : 0;
