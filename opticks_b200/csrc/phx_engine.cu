@@ -129,6 +129,7 @@ struct phx_engine {
     DevBuf<long long> ev_start;
     DevBuf<unsigned> ev_left;
     DevBuf<uint32_t> jump_pow, jump_tab;   // P_k = T^(skip 2^k) and per-call event jump matrices
+    DevBuf<uint32_t> jump4;                // 4-bit group tables of a single-event jump matrix
     DevBuf<uint32_t> ev_rng;               // per-call event-advanced XORWOW states (k_rng_event)
     cudaGraphExec_t batch_exec = nullptr;   // cached batched launch sequence (use_graph)
     PhxBatchCall batch_call;
@@ -257,6 +258,7 @@ struct SimArgs {
     const uint32_t* rng;
     long long rng_slots;
     const uint32_t* jump;      // event jump matrix (phx_rngjump.h) or null for cuRAND skipahead
+    const uint32_t* jump4;     // its 4-bit group tables, or null
     phx_photon* photon;
     phx_seq* seq;
     uint32_t* hitword;
@@ -291,7 +293,8 @@ __global__ void __launch_bounds__(PHX_SIM_BLOCK, PHX_SIM_MINB) k_simulate(SimArg
             curand_init(0ull, (unsigned long long)photon_idx, 0ull, &rng);
         }
         if (a.event_index > 0ull) {
-            if (a.jump) phx_rng_jump(rng, a.jump, a.skip * a.event_index);
+            if (a.jump4) phx_rng_jump4(rng, a.jump4, a.skip * a.event_index);
+            else if (a.jump) phx_rng_jump(rng, a.jump, a.skip * a.event_index);
             else skipahead(a.skip * a.event_index, &rng);
         }
         PhxPhoton p;
@@ -751,7 +754,7 @@ int phx_destroy(phx_engine* e)
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
     e->counters.release(); e->status.release(); e->ev_start.release(); e->ev_left.release();
-    e->jump_pow.release(); e->jump_tab.release(); e->ev_rng.release();
+    e->jump_pow.release(); e->jump_tab.release(); e->jump4.release(); e->ev_rng.release();
     e->merge.release();
     e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wfree.release(); e->wscore.release(); e->wcnt.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
@@ -923,7 +926,7 @@ static PersistArgs persist_args_from(const phx_engine* e, const SimArgs& a)
     A.gs = a.gs; A.gs_off = a.gs_off; A.G = a.G; A.N = a.N;
     A.photon_offset = a.photon_offset; A.event_index = a.event_index;
     A.gs_event = nullptr; A.ev_start = nullptr;
-    A.skip = a.skip; A.rng = a.rng; A.rng_slots = a.rng_slots; A.jump = a.jump;
+    A.skip = a.skip; A.rng = a.rng; A.rng_slots = a.rng_slots; A.jump = a.jump; A.jump4 = a.jump4;
     A.photon = a.photon; A.seq = a.seq; A.hitword = a.hitword; A.hit_mask = a.hit_mask; A.status = a.status;
     A.regroup = 1; A.chunk = 1;
     return A;
@@ -1117,6 +1120,7 @@ struct PhxPlainBufs {
     long long* counters;   // [0] num_hit, [1] queue head
     unsigned* status;
     uint32_t* jump;        // one event jump matrix (PHX_JUMP_MATW words)
+    uint32_t* jump4;       // its 4-bit group tables (PHX_JUMP_NIBW words), or null to use the matrix
 };
 
 // every device operation of one plain simulate call on st, then the D2H of num_hit/status
@@ -1130,6 +1134,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
     PHX_CU(cudaMemsetAsync(b.counters, 0, 2 * sizeof(long long), st));
     k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gs), G, b.gs_off);
     if (event_index > 0) k_jump_build<<<1, 160, 0, st>>>(nullptr, (unsigned long long)event_index, e->jump_pow.p, b.jump);
+    if (event_index > 0 && b.jump4) k_jump_nibbles<<<(PHX_JUMP_BITS / 4 * 16 + 127) / 128, 128, 0, st>>>(b.jump, b.jump4);
     PHX_CU(cudaGetLastError());
     SimArgs a;
     a.S = scene_of(e, e->cfg.root_polish);
@@ -1145,6 +1150,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
     a.jump = event_index > 0 ? b.jump : nullptr;
+    a.jump4 = event_index > 0 ? b.jump4 : nullptr;
     a.photon = photon;
     a.seq = seq;
     a.hitword = want_hits ? b.hitword : nullptr;
@@ -1172,13 +1178,13 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         e->last_rounds = 0;
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
-        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + (A.ev_rng ? 1 : 0) +
+        e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + (A.ev_rng ? 1 : 0) +
                            (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());
         e->last_rounds = 0;
-        e->last_launches = 1 + (event_index > 0 ? 1 : 0) + 1 + (want_hits ? 3 : 0);
+        e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + 1 + (want_hits ? 3 : 0);
     }
     if (sensor) PHX_CU(cudaMemsetAsync(sensor, 0, sizeof(uint32_t) * std::max(0, e->cfg.num_sensor), st));
     if (want_hits && N > 0) {
@@ -1214,7 +1220,8 @@ static int simulate_device_impl(phx_engine* e, const float* d_gs, int G, long lo
     PHX_CU(e->wordoff.ensure((size_t)std::max<long long>(1, nword)));
     PHX_CU(e->blocksum.ensure((size_t)std::max<long long>(1, (nword + 255) / 256)));
     PHX_CU(e->jump_tab.ensure(PHX_JUMP_MATW));
-    PhxPlainBufs b = { e->gs_off.p, e->hitword.p, e->wordoff.p, e->blocksum.p, e->counters.p, e->status.p, e->jump_tab.p };
+    PHX_CU(e->jump4.ensure(PHX_JUMP_NIBW));
+    PhxPlainBufs b = { e->gs_off.p, e->hitword.p, e->wordoff.p, e->blocksum.p, e->counters.p, e->status.p, e->jump_tab.p, e->jump4.p };
     rc = plain_enqueue(e, b, d_gs, G, N, event_index, photon_offset, photon, d_seq, d_hit, hit_capacity, d_sensor, want_hits, st,
                        true);
     if (rc) return rc;
@@ -1376,6 +1383,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
     a.jump = e->jump_tab.p;
+    a.jump4 = nullptr;
     a.photon = photon;
     a.seq = reinterpret_cast<phx_seq*>(c.seq);
     a.hitword = want_hits ? e->hitword.p : nullptr;
@@ -1555,6 +1563,7 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
     a.jump = event_index > 0 ? e->jump_tab.p : nullptr;
+    a.jump4 = nullptr;
     a.photon = nullptr;
     a.seq = nullptr;
     a.hitword = nullptr;

@@ -287,6 +287,44 @@ PHX_D void phx_rng_jump(curandStateXORWOW& s, const uint32_t* __restrict__ M, un
     s.d += (unsigned int)((362437ull * n) & 0xffffffffull);
 }
 
+// v <- M v through the 4-bit group tables of M (k_jump_nibbles): 40 lookups instead of 160 column
+// steps, the same XOR of the same columns, so the same state as phx_rng_jump and skipahead(n)
+PHX_D void phx_rng_jump4(curandStateXORWOW& s, const uint32_t* __restrict__ T, unsigned long long n)
+{
+    uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u, o4 = 0u;
+    const uint32_t in[5] = { s.v[0], s.v[1], s.v[2], s.v[3], s.v[4] };
+#pragma unroll 1
+    for (int w = 0; w < 5; w++) {
+        const uint32_t x = in[w];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const uint32_t* e = T + (size_t)((8 * w + q) * 16 + ((x >> (4 * q)) & 15u)) * PHX_JUMP_COLW;
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(e));
+            const uint32_t e4 = __ldg(e + 4);
+            o0 ^= a.x; o1 ^= a.y; o2 ^= a.z; o3 ^= a.w; o4 ^= e4;
+        }
+    }
+    s.v[0] = o0; s.v[1] = o1; s.v[2] = o2; s.v[3] = o3; s.v[4] = o4;
+    s.d += (unsigned int)((362437ull * n) & 0xffffffffull);
+}
+
+// the 4-bit group tables of one jump matrix M: thread t builds entry (t / 16, t % 16)
+__global__ void k_jump_nibbles(const uint32_t* __restrict__ M, uint32_t* T)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= PHX_JUMP_BITS / 4 * 16) return;
+    const int g = t >> 4, k = t & 15;
+    uint32_t o[5] = { 0u, 0u, 0u, 0u, 0u };
+    for (int b = 0; b < 4; b++) {
+        if (!((k >> b) & 1)) continue;
+        const uint32_t* col = M + (size_t)(4 * g + b) * PHX_JUMP_COLW;
+        for (int q = 0; q < 5; q++) o[q] ^= col[q];
+    }
+    uint32_t* dst = T + (size_t)t * PHX_JUMP_COLW;
+    for (int q = 0; q < 5; q++) dst[q] = o[q];
+    dst[5] = dst[6] = dst[7] = 0u;
+}
+
 // one event jump matrix per entry: entry i uses event ev[i] (or `single` when ev is null);
 // thread c composes column c of prod_k P_k^(bit k of event)
 __global__ void k_jump_build(const int* ev, unsigned long long single, const uint32_t* __restrict__ P, uint32_t* out)

@@ -63,6 +63,14 @@ enum {
     PHX_T_SPHERE_RANDPOL = 64
 };
 
+// ---- event jump matrices of the XORWOW streams (phx_rngjump.h) ----
+#define PHX_JUMP_BITS 160
+#define PHX_JUMP_COLW 8                          // words per stored column (5 used)
+#define PHX_JUMP_MATW (PHX_JUMP_BITS * PHX_JUMP_COLW)
+// the same jump as XOR tables over 4-bit groups of the state: entry (g, k) = XOR of the columns
+// 4g+b for the bits b set in k (40 groups x 16 patterns x PHX_JUMP_COLW words)
+#define PHX_JUMP_NIBW (PHX_JUMP_BITS / 4 * 16 * PHX_JUMP_COLW)
+
 // ---- CSG typecodes ----
 enum {
     PHX_CSG_ZERO = 0,

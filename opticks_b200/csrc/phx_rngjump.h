@@ -8,15 +8,15 @@
 // counter advances by 362437 n.  The host builds T from the recurrence, the powers
 // P_k = T^(skip * 2^k) by repeated squaring, and the device composes M_e = prod_k P_k^(bit k of e)
 // once per event (one thread per matrix column).  A photon then applies M_e to its 160-bit state:
-// 160 predicated XORs of 32-byte columns instead of a multi-stage skipahead per photon.
+// 160 predicated XORs of 32-byte columns instead of a multi-stage skipahead per photon, or, for a
+// single event, 40 lookups in tables of M_e over 4-bit groups of the state (the "four Russians"
+// grouping of a GF(2) matrix-vector product), built once per call.
 // Matrices are stored column-major, one column = the image of one state bit, padded to 8 words.
 #pragma once
 #include <stdint.h>
 #include <vector>
 
-#define PHX_JUMP_BITS 160
-#define PHX_JUMP_COLW 8                          // words per stored column (5 used)
-#define PHX_JUMP_MATW (PHX_JUMP_BITS * PHX_JUMP_COLW)
+#include "phx_pod.h"                        // PHX_JUMP_BITS, PHX_JUMP_COLW, PHX_JUMP_MATW
 #define PHX_JUMP_POWERS 32                       // events < 2^32
 
 struct PhxV5 { uint32_t w[5]; };
