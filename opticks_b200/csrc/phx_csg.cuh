@@ -292,7 +292,6 @@ PHX_COLD float4 leaf_box3(const float4 q0, const float t_min, const float3 o, co
     else if (along_y) has = in_x && in_z;
     else if (along_z) has = in_x && in_y;
     else has = (t_far > t_near && t_far > 0.f);
-    bool valid = false;
     if (has) {
         float t_cand = t_min < t_near ? t_near : (t_min < t_far ? t_far : t_min);
         float3 p = o + t_cand * dir;
@@ -301,12 +300,10 @@ PHX_COLD float4 leaf_box3(const float4 q0, const float t_min, const float3 o, co
         if (pa.x >= pa.y && pa.x >= pa.z) n.x = copysignf(1.f, p.x);
         else if (pa.y >= pa.x && pa.y >= pa.z) n.y = copysignf(1.f, p.y);
         else if (pa.z >= pa.x && pa.z >= pa.y) n.z = copysignf(1.f, p.z);
-        if (t_cand > t_min) {
-            valid = true;
+        if (t_cand > t_min) {   // valid: w > t_min
             isect.x = n.x; isect.y = n.y; isect.z = n.z; isect.w = t_cand;
         }
     }
-    (void)valid;
     return isect;
 }
 
