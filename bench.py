@@ -515,7 +515,7 @@ def main():
                 "hit_fraction": f_hit,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "traffic": None, "kernel_ms": k_ms,
-                             "kernel": ("k_wave_init + k_wave_trace/k_wave_shade rounds (whole simulate launch sequence)"
+                             "kernel": ("k_wave_init + k_wave_trace_df/k_wave_shade rounds (whole simulate launch sequence)"
                                         if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
                              "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},
