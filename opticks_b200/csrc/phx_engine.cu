@@ -97,7 +97,8 @@ struct phx_engine {
     int num_global = 0;
     float cull[4] = { 0.f, 0.f, 0.f, 0.f };
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
-    bool has_full = false;    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
+    bool has_full = false;
+    int last_tail = 0;        // the last wavefront call finished its paths in one tail kernel    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
     std::vector<int> prim_node_offset;
     // physics
     cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr;
@@ -1054,6 +1055,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     PHX_CU(cudaGetLastError());
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
     e->last_rounds = 0;
+    e->last_tail = 0;
     int cur = 0;
     bool done = false;
     for (long long r = 0; r < max_rounds && !done;) {
@@ -1071,8 +1073,17 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
         PHX_CU(cudaGetLastError());
         PHX_CU(cudaMemcpyAsync(e->h_pinned + 40, cnt[cur], sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         PHX_CU(cudaStreamSynchronize(st));
-        done = e->h_pinned[40] == 0u;
+        const unsigned live = e->h_pinned[40];
+        done = live == 0u;
         e->last_rounds = r;
+        if (!done && !refill && live <= (unsigned)PHX_WAVE_TAIL) {
+            // few paths left and none queued: finish them in one kernel
+            W.act_in = act[cur]; W.n_in = cnt[cur];
+            k_wave_tail<CV, ADJ><<<(unsigned)((live + 127) / 128), 128, 0, st>>>(W);
+            PHX_CU(cudaGetLastError());
+            e->last_tail = 1;
+            done = true;
+        }
     }
     if (!done) return phx_fail(-5, "wavefront loop did not drain within %lld rounds", max_rounds);
     return 0;
@@ -1179,7 +1190,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
         e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + (A.ev_rng ? 1 : 0) +
-                           (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds : 1) + (want_hits ? 3 : 0);
+                           (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());

@@ -318,6 +318,33 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
     if (status) atomicOr(W.A.status, status);
 }
 
+// The last live paths of a call, once few remain and no photons wait in the queue: each thread
+// takes one path and runs its remaining bounces to the end with the one-kernel loop's step
+// (persist_step: the shared closest-hit and physics code), so a long chain no longer costs two
+// launches per bounce.  Photons, seq and hits are the same as the rounds would give.
+#ifndef PHX_WAVE_TAIL
+#define PHX_WAVE_TAIL (1 << 18)
+#endif
+template <int CV, bool ADJ = false>
+__global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
+{
+    const unsigned n = *W.n_in;
+    unsigned status = 0;
+    PhxLane L;
+    PhxScore score;
+    if (ADJ) wave_score_setup(score, W.A);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)n; i += stride) {
+        const uint32_t s = W.act_in[i];
+        wave_load(W, s, L);
+        if (ADJ) wave_load_score(W, s, &score);
+        for (int b = 0; b <= W.A.C.max_bounce + 1; b++)        // persist_step ends the path within max_bounce
+            if (persist_step<CV, ADJ>(L, W.A, status, ADJ ? &score : nullptr)) break;
+        persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
+    }
+    if (status) atomicOr(W.A.status, status);
+}
+
 // physics of every live path after its closest hit (CSGOptiX/CSGOptiX7.cu:491-509), finishing
 // and refilling slots; live slots go to the next round's list
 // resident 128-thread blocks per SM asked for the physics kernel (its loads of path state are
