@@ -1557,7 +1557,11 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     PHX_CU(cudaMemsetAsync(d_hits, 0, sizeof(double) * (size_t)e->cfg.num_sensor, st));
     PHX_CU(cudaMemsetAsync(d_grad, 0, sizeof(double) * (size_t)e->cfg.num_sensor * 32, st));
     k_genstep_offsets<<<1, 1024, 0, st>>>(reinterpret_cast<const float4*>(d_gensteps), G, e->gs_off.p);
-    if (event_index > 0) k_jump_build<<<1, 160, 0, st>>>(nullptr, (unsigned long long)event_index, e->jump_pow.p, e->jump_tab.p);
+    PHX_CU(e->jump4.ensure(PHX_JUMP_NIBW));
+    if (event_index > 0) {
+        k_jump_build<<<1, 160, 0, st>>>(nullptr, (unsigned long long)event_index, e->jump_pow.p, e->jump_tab.p);
+        k_jump_nibbles<<<(PHX_JUMP_BITS / 4 * 16 + 127) / 128, 128, 0, st>>>(e->jump_tab.p, e->jump4.p);
+    }
     PHX_CU(cudaGetLastError());
     SimArgs a;
     a.S = scene_of(e, 0);
@@ -1574,7 +1578,7 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
     a.jump = event_index > 0 ? e->jump_tab.p : nullptr;
-    a.jump4 = nullptr;
+    a.jump4 = event_index > 0 ? e->jump4.p : nullptr;
     a.photon = nullptr;
     a.seq = nullptr;
     a.hitword = nullptr;
