@@ -282,9 +282,7 @@ __global__ void __launch_bounds__(PHX_SIM_BLOCK, PHX_SIM_MINB) k_simulate(SimArg
     bool is_hit = false;
     if (idx < a.N) {
         const int gi = phx_find_genstep(a.gs_off, a.G, idx);
-        float4 g[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) g[k] = __ldg(a.gs + 6 * gi + k);
+        const float4* g = a.gs + 6 * gi;
         const long long photon_idx = a.photon_offset + idx;
         curandStateXORWOW rng;
         if (photon_idx < a.rng_slots) {

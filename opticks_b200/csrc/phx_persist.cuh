@@ -130,9 +130,7 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
         for (int k = 0; k < 32; k++) sc->g[k] = 0.f;
     }
     const int gi = phx_find_genstep(A.gs_off, A.G, idx);
-    float4 g[6];
-#pragma unroll
-    for (int k = 0; k < 6; k++) g[k] = __ldg(A.gs + 6 * gi + k);
+    const float4* g = A.gs + 6 * gi;     // read in place: a local copy would live in local memory
     long long slot;
     unsigned long long ev;
     if (A.gs_event) {
