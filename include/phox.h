@@ -193,6 +193,11 @@ int phx_merge_hits(phx_engine* e, const void* in, int64_t num_in, int32_t lite, 
 int phx_set_input_photon(phx_engine* e, const float* photon, int64_t num_photon);
 int phx_set_input_photon_device(phx_engine* e, const float* d_photon, int64_t num_photon);
 
+/* The black-body wavelength table (4096 floats, nm) that torch photons without a wavelength
+ * sample (qudarap/qsim.h:2541-2544, QPlanck: 6500 K over 80-800 nm, qudarap/QPlanck.cc:36-48).
+ * Host-only, no engine needed. */
+int phx_planck_icdf(float* out, int n);
+
 /* Diagnostics of the last phx_simulate / phx_simulate_device call on this engine (no reference
  * counterpart): kernels it launched and, in kernel_mode 2, wavefront rounds (one closest-hit and
  * one physics launch each). */

@@ -79,6 +79,7 @@ SIGNATURES = {
                                  C.POINTER(C.c_int64)]),
     "phx_last_call_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "phx_set_input_photon": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    "phx_planck_icdf": (C.c_int, [C.c_void_p, C.c_int]),
     "phx_set_input_photon_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
 }
 

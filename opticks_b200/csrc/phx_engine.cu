@@ -97,12 +97,12 @@ struct phx_engine {
     int num_global = 0;
     float cull[4] = { 0.f, 0.f, 0.f, 0.f };
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
-    bool has_full = false;
-    int last_tail = 0;        // the last wavefront call finished its paths in one tail kernel    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
+    bool has_full = false;    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
+    int last_tail = 0;        // the last wavefront call finished its paths in one tail kernel
     std::vector<int> prim_node_offset;
     // physics
-    cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr;
-    cudaTextureObject_t bnd_tex = 0, icdf_tex = 0;
+    cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr, planck_arr = nullptr;
+    cudaTextureObject_t bnd_tex = 0, icdf_tex = 0, planck_tex = 0;
     DevBuf<uint4> optical;
     DevBuf<float4> input_own;              // input photons copied from the host
     const float4* input_photon = nullptr;  // the input photons in use (input_own or a caller's buffer)
@@ -178,6 +178,7 @@ static PhxProps props_of(const phx_engine* e)
     P.ny = e->ny;
     P.icdf_tex = e->icdf_tex;
     P.hd_factor = e->hd_factor;
+    P.planck_tex = e->planck_tex;
     P.input_photon = e->input_photon;
     P.num_input_photon = e->num_input_photon;
     return P;
@@ -638,6 +639,49 @@ static PhxSph prim_sphere(const phx_geometry* geo, int p)
     return t.r < b.r ? t : b;
 }
 
+// QPlanck's table (qudarap/QPlanck.cc:36-48): sblackbody<double>(4096, 4096, 6500 K, 80 nm, 800 nm)
+// narrowed to float.  Planck's law sampled at 4096 wavelengths (sysrap/sblackbody.h:77-116), its
+// trapezoid integral normalised by the last value (NP::trapz, NP::divide_by_last), inverted at
+// y = j / 4096 by the first bin with y0 <= y < y1 and linear interpolation (NP::MakeICDF with
+// hd_factor 0, NP::pdomain), in double as the reference does.
+extern "C" int phx_planck_icdf(float* out, int n)
+{
+    if (!out || n < PHX_PLANCK_N) return phx_fail(-1, "phx_planck_icdf: need %d floats", PHX_PLANCK_N);
+    const int ni = 4096, nu = PHX_PLANCK_N;
+    const double temp_K = 6500.0, nm0 = 80.0, nm1 = 800.0;
+    const double h = 6.62606957e-34, c = 299792458.0, k = 1.3806488e-23;
+    const double a = 2.0 * h * c * c, b = h * c / k;
+    std::vector<double> x((size_t)ni), y((size_t)ni);
+    for (int i = 0; i < ni; i++) {
+        x[i] = nm0 + (nm1 - nm0) * double(i) / double(ni - 1);
+        const double wlm = x[i] * 1e-9;
+        y[i] = (a * std::pow(wlm, -5.0)) / (std::exp(b / (wlm * temp_K)) - 1.0);
+    }
+    std::vector<double> cdf((size_t)ni);
+    cdf[0] = 0.0;
+    for (int i = 0; i < ni - 1; i++) cdf[i + 1] = cdf[i] + (x[i + 1] - x[i]) * (y[i] + y[i + 1]) * 0.5;
+    const double last = cdf[ni - 1];
+    if (last != 0.0) for (int i = 0; i < ni; i++) cdf[i] /= last;
+    for (int j = 0; j < nu; j++) {
+        const double yv = double(j) / double(nu);
+        double xv = x[0];
+        if (yv <= cdf[0]) xv = x[0];
+        else if (yv >= cdf[ni - 1]) xv = x[ni - 1];
+        else {
+            for (int i = 0; i < ni - 1; i++) {
+                const double y0 = cdf[i], y1 = cdf[i + 1], dy = y1 - y0;
+                if (y0 <= yv && yv < y1) {
+                    xv = x[i];
+                    if (dy > 0.0) xv += (yv - y0) * (x[i + 1] - x[i]) / dy;
+                    break;
+                }
+            }
+        }
+        out[j] = static_cast<float>(xv);
+    }
+    return 0;
+}
+
 static int make_texture_f4(cudaArray_t& arr, cudaTextureObject_t& tex, const float* data, int width, int height)
 {
     cudaChannelFormatDesc ch = cudaCreateChannelDesc<float4>();
@@ -748,6 +792,8 @@ int phx_destroy(phx_engine* e)
     if (e->icdf_tex) cudaDestroyTextureObject(e->icdf_tex);
     if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
+    if (e->planck_tex) cudaDestroyTextureObject(e->planck_tex);
+    if (e->planck_arr) cudaFreeArray(e->planck_arr);
     e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release();
     e->bvh.release(); e->leaves.release(); e->globals.release(); e->leaf_sph.release(); e->global_sph.release(); e->optical.release(); e->rng.release();
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
@@ -895,6 +941,12 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
         e->hd_factor = 0xffffffffu;  // no scintillator table : reemission wavelength 0
         float dummy[4] = { 0.f, 0.f, 0.f, 0.f };
         PHX_TRY(make_texture_f1(e->icdf_arr, e->icdf_tex, dummy, 2, 2));
+    }
+    {
+        // black-body wavelengths for torch photons without a wavelength (QPlanck)
+        float table[PHX_PLANCK_N];
+        phx_planck_icdf(table, PHX_PLANCK_N);
+        PHX_TRY(make_texture_f1(e->planck_arr, e->planck_tex, table, PHX_PLANCK_N, 1));
     }
     // ---- rng + small buffers
     {

@@ -118,6 +118,7 @@ struct PhxProps {
     unsigned nx, ny;                // texture width/height
     cudaTextureObject_t icdf_tex;   // 4096 x 3 float, linear, normalized, wrap
     unsigned hd_factor;
+    cudaTextureObject_t planck_tex; // PHX_PLANCK_N x 1 float black-body wavelength ICDF, linear, normalized, wrap
     const float4* input_photon;     // (num_input_photon*4) sphoton rows for INPUT_PHOTON gensteps, or null
     long long num_input_photon;
 };
@@ -415,7 +416,10 @@ PHX_COLD void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4
 {
     const int gencode = __float_as_int(g[0].x);
     switch (gencode) {
-        case PHX_GS_TORCH: generate_torch(p, rng, g, photon_id); break;
+        case PHX_GS_TORCH:
+            generate_torch(p, rng, g, photon_id);
+            if (p.wavelength <= 0.f) p.wavelength = tex2D<float>(P.planck_tex, curand_uniform(&rng), 0.5f);   // qplanck::wavelength
+            break;
         case PHX_GS_G4Cerenkov_modified:
         case PHX_GS_CERENKOV: generate_cerenkov(p, rng, g, P, status); break;
         case PHX_GS_DsG4Scintillation_r4695:

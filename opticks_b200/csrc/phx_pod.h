@@ -71,6 +71,8 @@ enum {
 // 4g+b for the bits b set in k (40 groups x 16 patterns x PHX_JUMP_COLW words)
 #define PHX_JUMP_NIBW (PHX_JUMP_BITS / 4 * 16 * PHX_JUMP_COLW)
 
+#define PHX_PLANCK_N 4096                        // black-body wavelength ICDF entries (QPlanck)
+
 // ---- CSG typecodes ----
 enum {
     PHX_CSG_ZERO = 0,

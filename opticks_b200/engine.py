@@ -68,6 +68,13 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def planck_icdf() -> np.ndarray:
+    """the black-body wavelength ICDF (4096 float32, nm) torch photons without a wavelength sample"""
+    out = np.zeros(4096, np.float32)
+    _lib.check(_lib.lib().phx_planck_icdf(_ptr(out), 4096), "phx_planck_icdf")
+    return out
+
+
 class Engine:
     def __init__(self, geometry: dict, physics: dict, config: PhxConfig | dict | None = None, device: int = 0):
         L = _lib.lib()

@@ -195,6 +195,41 @@ static float tex2d_f1(const float* data, int W, int H, float x, float y)
          + (1 - ax) * ay * data[(size_t)y1 * W + x0] + ax * ay * data[(size_t)y1 * W + x1];
 }
 
+/* QPlanck's table (qudarap/QPlanck.cc:36-48): Planck's law at 4096 wavelengths over 80-800 nm at
+   6500 K (sysrap/sblackbody.h:77-116), trapezoid integral / last (NP::trapz, NP::divide_by_last),
+   inverted at y = j/4096 by the first bin with y0 <= y < y1 and linear interpolation
+   (NP::MakeICDF hd_factor 0, NP::pdomain), in double, narrowed to float. */
+int oracle_planck_icdf(float* out, int n)
+{
+    enum { NI = 4096, NU = 4096 };
+    if (!out || n < NU) return -1;
+    static double x[NI], y[NI], cdf[NI];
+    const double T = 6500.0, nm0 = 80.0, nm1 = 800.0;
+    const double h = 6.62606957e-34, c = 299792458.0, k = 1.3806488e-23;
+    const double a = 2.0 * h * c * c, b = h * c / k;
+    for (int i = 0; i < NI; i++) {
+        x[i] = nm0 + (nm1 - nm0) * (double)i / (double)(NI - 1);
+        double wlm = x[i] * 1e-9;
+        y[i] = (a * pow(wlm, -5.0)) / (exp(b / (wlm * T)) - 1.0);
+    }
+    cdf[0] = 0.0;
+    for (int i = 0; i < NI - 1; i++) cdf[i + 1] = cdf[i] + (x[i + 1] - x[i]) * (y[i] + y[i + 1]) * 0.5;
+    double last = cdf[NI - 1];
+    if (last != 0.0) for (int i = 0; i < NI; i++) cdf[i] /= last;
+    for (int j = 0; j < NU; j++) {
+        double yv = (double)j / (double)NU, xv = x[0];
+        if (yv <= cdf[0]) xv = x[0];
+        else if (yv >= cdf[NI - 1]) xv = x[NI - 1];
+        else
+            for (int i = 0; i < NI - 1; i++) {
+                double y0 = cdf[i], y1 = cdf[i + 1], dy = y1 - y0;
+                if (y0 <= yv && yv < y1) { xv = x[i]; if (dy > 0.0) xv += (yv - y0) * (x[i + 1] - x[i]) / dy; break; }
+            }
+        out[j] = (float)xv;
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ scene */
 typedef struct {
     const float* node;          /* (Nn,4,4) */
@@ -219,6 +254,7 @@ typedef struct {
     const float* plan;          /* (Nl,4) convex polyhedron planes, or NULL */
     const float* input_photon;  /* (num_input,4,4) sphoton rows for INPUT_PHOTON gensteps, or NULL */
     long long num_input;
+    const float* planck;        /* (4096) black-body wavelength ICDF, or NULL */
 } oracle_scene;
 
 typedef struct { const float* u; int n; int k; int over; } ustream;
@@ -709,7 +745,11 @@ static int run_photons(const oracle_scene* S, const float* gs, int G, long long 
         memset(&p, 0, sizeof(p));
         int32_t code;
         memcpy(&code, g, 4);
-        if (code == 6) gen_torch(&p, &r, g, (unsigned long long)idx);
+        if (code == 6) {
+            gen_torch(&p, &r, g, (unsigned long long)idx);
+            /* qudarap/qsim.h:2541-2544: no wavelength given, a black-body one (qplanck::wavelength) */
+            if (p.wavelength <= 0.f && S->planck) { float u = U(&r); p.wavelength = tex2d_f1(S->planck, 4096, 1, u, 0.5f); }
+        }
         else if (code == 16 || code == 5) gen_scint(&p, &r, g, S);
         else if (code == 15 || code == 18) gen_cerenkov(&p, &r, g, S);
         else if (code == 14) gen_carrier(&p, g, (unsigned long long)idx);

@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_CSG = os.path.join(HERE, "_ref", "libref_csg.so")
 REF_SIM = os.path.join(HERE, "_ref", "libref_sim.so")
+REF_PLANCK = os.path.join(HERE, "_ref", "libref_planck.so")
 REF_SPM = os.path.join(HERE, "_ref", "libref_spm.so")
 
 
@@ -41,6 +42,7 @@ class OracleScene(C.Structure):
         ("max_bounce", C.c_int), ("max_time", C.c_float), ("tmin", C.c_float), ("tmin0", C.c_float),
         ("eps0_mask", C.c_uint), ("hit_mask", C.c_uint), ("polish", C.c_int),
         ("pair_bbox", C.c_void_p), ("plan", C.c_void_p), ("input_photon", C.c_void_p), ("num_input", C.c_longlong),
+        ("planck", C.c_void_p),
     ]
 
 
@@ -132,6 +134,32 @@ def pair_world_boxes(geom: dict, pin, pnode) -> np.ndarray:
     return out
 
 
+def planck_icdf() -> np.ndarray:
+    """the oracle's restatement of QPlanck's black-body wavelength ICDF (4096 float32)"""
+    out = np.zeros(4096, np.float32)
+    L = lib()
+    L.oracle_planck_icdf.restype = C.c_int
+    L.oracle_planck_icdf.argtypes = [C.c_void_p, C.c_int]
+    if L.oracle_planck_icdf(_p(out), 4096) != 0:
+        raise RuntimeError("oracle_planck_icdf failed")
+    return out
+
+
+def have_ref_planck() -> bool:
+    return os.path.exists(REF_PLANCK)
+
+
+def ref_planck_icdf() -> np.ndarray:
+    """the reference's own table (sysrap/sblackbody.h compiled on the CPU)"""
+    L = C.CDLL(REF_PLANCK)
+    L.ref_planck_icdf.restype = C.c_int
+    L.ref_planck_icdf.argtypes = [C.c_void_p, C.c_int]
+    out = np.zeros(4096, np.float32)
+    if L.ref_planck_icdf(_p(out), 4096) != 0:
+        raise RuntimeError("ref_planck_icdf failed")
+    return out
+
+
 class Scene:
     """keeps the arrays alive behind an OracleScene"""
 
@@ -154,7 +182,9 @@ class Scene:
             _p(self.optical), _p(self.icdf), 0 if self.icdf is None else self.icdf.shape[1],
             0 if self.icdf is None else self.icdf.shape[0], int(phys.get("hd_factor", 20)),
             max_bounce, max_time, tmin, tmin0, eps0_mask, hit_mask, polish, _p(self.pair_bbox), _p(self.plan),
-            None, 0)
+            None, 0, None)
+        self.planck = planck_icdf()
+        self.s.planck = _p(self.planck)
         self.input_photon = None
         if input_photon is not None:
             self.input_photon = np.ascontiguousarray(input_photon, np.float32).reshape(-1, 4, 4)
@@ -302,9 +332,9 @@ REF_TORCH_TYPES = range(1, 8)
 
 def ref_genstep_check(gs: np.ndarray, have_input: bool = False) -> None:
     """refuse gensteps the reference's device code is not given the means to generate: a torch
-    genstep of another type, or without a wavelength, leaves the photon's wavelength at zero, and
-    qsim::generate_photon then samples the Planck texture (qudarap/qsim.h:2541-2544), which this
-    driver does not set up"""
+    genstep of a type storch::generate does not fill leaves the photon unset (zero wavelength
+    then samples the Planck texture, qudarap/qsim.h:2541-2544, which this driver sets up as
+    QPlanck does); input photons need the input array"""
     gi = gs.view(np.int32)
     for k in range(len(gs)):
         code = int(gi[k, 0, 0])
@@ -312,8 +342,8 @@ def ref_genstep_check(gs: np.ndarray, have_input: bool = False) -> None:
             raise ValueError(f"genstep {k}: gencode {code} is not one the reference driver generates")
         if code == 19 and not have_input:
             raise ValueError(f"genstep {k}: INPUT_PHOTON genstep without input photons")
-        if code == 6 and (int(gi[k, 5, 3]) not in REF_TORCH_TYPES or not gs[k, 3, 3] > 0.0):
-            raise ValueError(f"genstep {k}: torch type {int(gi[k, 5, 3])} / wavelength {gs[k, 3, 3]} is not a reference torch genstep")
+        if code == 6 and int(gi[k, 5, 3]) not in REF_TORCH_TYPES:
+            raise ValueError(f"genstep {k}: torch type {int(gi[k, 5, 3])} is not a reference torch type")
 
 
 def ref_simulate_gpu(geom: dict, phys: dict, gs: np.ndarray, event_index: int = 0, seed: int = 0, skip: int = 100000,

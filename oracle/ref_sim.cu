@@ -27,6 +27,8 @@
 #include <curand_kernel.h>
 #include "qrng.h"
 #include "qsim.h"
+#include "qplanck.h"
+#include "sblackbody.h"
 #include "csg_intersect_leaf.h"
 #include "csg_intersect_node.h"
 #include "csg_intersect_tree.h"
@@ -227,6 +229,19 @@ extern "C" int ref_sim_run(
     sc_h.hd_factor = (unsigned)hd_factor;
     qscint* sc_d = up(&sc_h, 1);
 
+    // the Planck wavelength texture QPlanck builds (qudarap/QPlanck.cc:36-48): sblackbody<double>
+    // narrowed to float, 4096 x 1, linear, normalized coordinates, wrap
+    std::vector<float> planck_h(4096);
+    {
+        sblackbody<double> bb(4096, 4096, 6500., 80., 800., 1000);
+        const double* v = bb.icdf->cvalues<double>();
+        for (int i = 0; i < 4096; i++) planck_h[i] = static_cast<float>(v[i]);
+    }
+    cudaArray_t a_planck = nullptr;
+    qplanck pl_h;
+    pl_h.tex = tex_f1(planck_h.data(), 4096, 1, &a_planck);
+    qplanck* pl_d = up(&pl_h, 1);
+
     qbase base_h; base_h.pidx = 0xffffffffffffffffull;
     qbase* base_d = up(&base_h, 1);
 
@@ -271,7 +286,7 @@ extern "C" int ref_sim_run(
 
     qsim sim_h; memset(&sim_h, 0, sizeof(sim_h));
     sim_h.base = base_d; sim_h.evt = ev_d; sim_h.rng = rng_d; sim_h.bnd = bnd_d;
-    sim_h.cerenkov = ck_d; sim_h.scint = sc_d;
+    sim_h.cerenkov = ck_d; sim_h.scint = sc_d; sim_h.planck = pl_d;
     qsim* sim_d = up(&sim_h, 1);
 
     if (N > 0) ref_simulate_k<<<(unsigned)((N + 127) / 128), 128>>>(sim_d, ev_d, S, tmin, tmin0, eps0mask, max_time);
@@ -285,8 +300,8 @@ extern "C" int ref_sim_run(
         }
     }
     if (nrec) { cudaFree(ev_h.record); cudaFree(ev_h.prd); }
-    cudaDestroyTextureObject(t_bnd); cudaDestroyTextureObject(t_icdf);
-    cudaFreeArray(a_bnd); cudaFreeArray(a_icdf);
+    cudaDestroyTextureObject(t_bnd); cudaDestroyTextureObject(t_icdf); cudaDestroyTextureObject(pl_h.tex);
+    cudaFreeArray(a_bnd); cudaFreeArray(a_icdf); cudaFreeArray(a_planck); cudaFree(pl_d);
     cudaFree((void*)S.node); if (S.plan) cudaFree((void*)S.plan); cudaFree((void*)S.itra); cudaFree((void*)S.inst_inv); cudaFree((void*)S.pair_inst);
     cudaFree((void*)S.pair_node); cudaFree((void*)S.pair_gpbd); cudaFree((void*)S.pair_iiid);
     cudaFree(meta_d); cudaFree(bnd_h.optical); cudaFree(bnd_d); cudaFree(sc_d); cudaFree(base_d); cudaFree(ck_d);

@@ -11,6 +11,8 @@ csg_zoo_ref.npz  : the same for the further leaves (scenes.csg_leaf_zoo: cone, h
 csg_list_ref.npz : list nodes (scenes.csg_list_zoo: contiguous, discontiguous, overlap, and lists
                    inside boolean trees) through the reference's tree / list intersectors
                    (built WITH_CONTIGUOUS as its CSG library is).
+planck_icdf_ref.npy : the black-body wavelength table QPlanck builds from sysrap/sblackbody.h
+                   (oracle/_ref/libref_planck.so), 4096 float32.
 
 Run from the repository root where the reference checkout is present:
     make -C oracle ref && python tests/golden/make_golden.py
@@ -68,6 +70,7 @@ def main():
     print({k: getattr(v, "shape", v) for k, v in out.items()})
     zoo()
     lists()
+    np.save(os.path.join(ROOT, "tests", "golden", "planck_icdf_ref.npy"), O.ref_planck_icdf())
 
 
 def lists():

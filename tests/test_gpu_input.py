@@ -91,3 +91,26 @@ def test_carrier_genstep_matches_reference(cuda):
     assert seq_match(r["seq"], sq) >= 0.95
     same = np.all(r["seq"][:, 0, :] == sq[:, 0, :], axis=1)
     assert frac_close(r["photon"], ph, same, TOL) >= 0.95
+
+
+@pytest.mark.skipif(not O.have_ref_sim(), reason="reference GPU build absent")
+def test_torch_without_wavelength_matches_reference(cuda):
+    """torch photons without a wavelength take one from the black-body texture (qsim.h:2541-2544)"""
+    from opticks_b200 import engine as E
+    fd, lib, _, _ = scenes.sphere_in_box(1)
+    n = 50_000
+    gs = scenes.torch_genstep(n, wavelength=0.0, type_=scenes.T_SPHERE, distance=0.25)[None]
+    eng = E.Engine(fd.arrays(), lib.arrays(), E.default_config(max_photon=n))
+    r = eng.simulate(gs, 0)
+    eng.close()
+    assert r["status"] == 0
+    wl = r["photon"][:, 2, 3]
+    assert np.all((wl > 80.0) & (wl < 800.0))
+    ph, sq = O.ref_simulate_gpu(fd.arrays(), lib.arrays(), gs)
+    m = seq_match(r["seq"], sq)
+    same = np.all(r["seq"][:, 0, :] == sq[:, 0, :], axis=1)
+    fc = frac_close(r["photon"], ph, same, TOL)
+    wl_exact = float(np.mean(r["photon"][:, 2, 3] == ph[:, 2, 3]))
+    print(f"black-body torch vs reference: seqhis {m:.6f} close {fc:.6f} wavelength bit-exact {wl_exact:.6f}")
+    assert m >= SEQ_BAR
+    assert fc >= SEQ_BAR

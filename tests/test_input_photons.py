@@ -59,3 +59,27 @@ def test_reference_driver_needs_the_input_photons():
     with pytest.raises(ValueError):
         O.ref_genstep_check(gs)
     O.ref_genstep_check(gs, have_input=True)
+
+
+def test_planck_table_matches_reference_golden():
+    # QPlanck's black-body wavelength ICDF: the engine's and the oracle's restatements against the
+    # reference's own sblackbody table
+    import os
+    from tests.conftest import ROOT
+    from opticks_b200 import engine as E
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "planck_icdf_ref.npy"))
+    np.testing.assert_array_equal(O.planck_icdf(), ref)
+    np.testing.assert_array_equal(E.planck_icdf(), ref)
+    assert ref[0] == 80.0 and np.all(np.diff(ref) >= 0.0) and ref[-1] < 800.0
+
+
+def test_oracle_torch_without_wavelength_samples_black_body():
+    geo, phys = _box()
+    n = 400
+    gs = scenes.torch_genstep(n, wavelength=0.0, type_=scenes.T_SPHERE)[None]
+    S = O.Scene(geo, phys, max_bounce=0)
+    u = np.random.default_rng(5).random((n, 16), dtype=np.float32)
+    ph, sq, err = S.simulate(gs, u, 0)
+    wl = ph[:, 2, 3]
+    assert np.all((wl > 80.0) & (wl < 800.0))
+    assert 300.0 < np.median(wl) < 700.0          # 6500 K peaks near 446 nm
