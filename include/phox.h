@@ -75,6 +75,8 @@ typedef struct {
     int32_t  regroup;                 /* persistent kernel: bounces between lane refills */
     int32_t  chunk;                   /* persistent kernel: queue grab per warp in units of 32 photons */
     int32_t  use_graph;               /* batched launches: capture once as a CUDA graph and replay */
+    int64_t  wave_pool;               /* wavefront loop: in-flight path slots, 0 = 2^26 (176 B each); an
+                                         event with more photons refills freed slots from its queue */
 } phx_config;
 
 typedef struct {

@@ -41,7 +41,7 @@ class PhxConfig(C.Structure):
         ("epsilon0_mask", C.c_uint32), ("hit_mask", C.c_uint32),
         ("root_polish", C.c_int32), ("num_sensor", C.c_int32),
         ("kernel_mode", C.c_int32), ("block", C.c_int32), ("regroup", C.c_int32), ("chunk", C.c_int32),
-        ("use_graph", C.c_int32),
+        ("use_graph", C.c_int32), ("wave_pool", C.c_int64),
     ]
 
 

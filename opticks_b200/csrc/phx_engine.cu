@@ -769,6 +769,7 @@ void phx_config_default(phx_config* c)
     c->regroup = 1;
     c->chunk = 1;
     c->use_graph = 1;
+    c->wave_pool = 0;
 }
 
 int64_t phx_count_photons(const float* gensteps, int32_t num_genstep)
@@ -1050,6 +1051,12 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 #ifndef PHX_WAVE_POOL
 #define PHX_WAVE_POOL (1LL << 26)
 #endif
+
+// path slots of the wavefront loop: the configured count, or PHX_WAVE_POOL
+static long long wave_pool_of(const phx_engine* e)
+{
+    return e->cfg.wave_pool > 0 ? (long long)e->cfg.wave_pool : (long long)PHX_WAVE_POOL;
+}
 // calls of at most this many photons get their event-advanced RNG states in one coherent pass
 // ahead of the loop (24 B per photon of scratch); larger ones advance each state as it starts
 #define PHX_EV_RNG_MAX (1LL << 26)
@@ -1083,7 +1090,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     if ((rc = wave_grid(k_wave_shade<CV, ADJ>, dev, g_shade))) return rc;
     if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
-    const long long pool = std::max<long long>(1, std::min<long long>(N, PHX_WAVE_POOL));
+    const long long pool = std::max<long long>(1, std::min<long long>(N, wave_pool_of(e)));
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
     PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
     const bool refill = N > pool;
@@ -1122,11 +1129,18 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
         }
         PHX_CU(cudaGetLastError());
         PHX_CU(cudaMemcpyAsync(e->h_pinned + 40, cnt[cur], sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        if (refill) PHX_CU(cudaMemcpyAsync(e->h_pinned + 44, A.queue, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         PHX_CU(cudaStreamSynchronize(st));
         const unsigned live = e->h_pinned[40];
         done = live == 0u;
         e->last_rounds = r;
-        if (!done && !refill && live <= (unsigned)PHX_WAVE_TAIL) {
+        bool queue_done = !refill;                  // every photon of the queue has been started
+        if (refill) {
+            unsigned long long head;
+            memcpy(&head, e->h_pinned + 44, sizeof(head));
+            queue_done = head >= (unsigned long long)N;
+        }
+        if (!done && queue_done && live <= (unsigned)PHX_WAVE_TAIL) {
             // few paths left and none queued: finish them in one kernel
             W.act_in = act[cur]; W.n_in = cnt[cur];
             k_wave_tail<CV, ADJ><<<(unsigned)((live + 127) / 128), 128, 0, st>>>(W);
@@ -1229,7 +1243,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         // the pre-pass pays off where photons start a few lanes at a time (persistent refill,
         // wavefront refill); when every photon starts in the wavefront's first kernel, whole
         // warps advance their states there
-        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX && !(wave && N <= PHX_WAVE_POOL)) {
+        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX && !(wave && N <= wave_pool_of(e))) {
             PHX_CU(e->ev_rng.ensure((size_t)N * 6));
             k_rng_event<<<(unsigned)std::min<long long>((N + 255) / 256, 148LL * 16), 256, 0, st>>>(A, e->ev_rng.p, N);
             PHX_CU(cudaGetLastError());
@@ -1240,7 +1254,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
         e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + (A.ev_rng ? 1 : 0) +
-                           (wave ? 1 + (N > PHX_WAVE_POOL ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
+                           (wave ? 1 + (N > wave_pool_of(e) ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());

@@ -41,7 +41,8 @@ def _run(torch, eng, g, N, ev):
 @pytest.mark.parametrize("num_genstep,per,event,kw", [
     (20, 5000, 0, {}),
     (20, 5000, 3, {}),
-    (300, 10000, 1, {}),                                   # 3M photons: more than the 2M pool slots
+    (300, 10000, 1, {"wave_pool": 1 << 20}),               # 3M photons through 1M slots: refill, then the tail
+    (300, 10000, 1, {}),                                   # 3M photons, all in flight
     (40, 5000, 2, {"max_bounce": 3}),
     (40, 5000, 0, {"max_time": 40.0}),
 ])
@@ -62,13 +63,14 @@ def test_wave_equals_persistent(det, num_genstep, per, event, kw):
     a.close(); b.close()
 
 
-def test_wave_batched_equals_persistent(det):
+@pytest.mark.parametrize("kw", [{}, {"wave_pool": 1 << 18}])      # all in flight; refill through 256k slots
+def test_wave_batched_equals_persistent(det, kw):
     torch = det[0]
     gs = scenes.batched_events(64, median=20000.0, lib=det[2])
     ev = np.arange(len(gs), dtype=np.int32)
     counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
     N = int(counts.sum())
-    a, b = _engines(det, int(counts.max()))
+    a, b = _engines(det, int(counts.max()), **kw)
     g = torch.from_numpy(gs).cuda()
     e = torch.from_numpy(ev).cuda()
     outs = []
