@@ -134,7 +134,7 @@ struct phx_engine {
     DevBuf<uint32_t> ev_rng;               // per-call event-advanced XORWOW states (k_rng_event)
     cudaGraphExec_t batch_exec = nullptr;   // cached batched launch sequence (use_graph)
     PhxBatchCall batch_call;
-    const void* batch_bufs[12] = {};
+    const void* batch_bufs[13] = {};
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
     PhxMergeWs merge;
@@ -1435,6 +1435,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
     if (G > 0) {
         k_event_starts<<<(G + 255) / 256, 256, 0, st>>>(c.ev, e->gs_off.p, G, e->ev_start.p);
         k_jump_build<<<G, 160, 0, st>>>(c.ev, 0ull, e->jump_pow.p, e->jump_tab.p);
+        k_jump_nibbles<<<dim3((PHX_JUMP_BITS / 4 * 16 + 127) / 128, (unsigned)G), 128, 0, st>>>(e->jump_tab.p, e->jump4.p);
     }
     PHX_CU(cudaGetLastError());
     if (want_hits) PHX_CU(cudaMemsetAsync(e->hitword.p, 0, sizeof(uint32_t) * (size_t)std::max<long long>(1, nword), st));
@@ -1458,7 +1459,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
     a.rng = e->rng.p;
     a.rng_slots = e->rng_slots;
     a.jump = e->jump_tab.p;
-    a.jump4 = nullptr;
+    a.jump4 = e->jump4.p;
     a.photon = photon;
     a.seq = reinterpret_cast<phx_seq*>(c.seq);
     a.hitword = want_hits ? e->hitword.p : nullptr;
@@ -1536,10 +1537,11 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
     if (c.num_event > 0) PHX_CU(e->ev_left.ensure((size_t)c.num_event));
     if (N > 0 && N <= PHX_EV_RNG_MAX) PHX_CU(e->ev_rng.ensure((size_t)N * 6));
     PHX_CU(e->jump_tab.ensure((size_t)std::max(1, c.G) * PHX_JUMP_MATW));
+    PHX_CU(e->jump4.ensure((size_t)std::max(1, c.G) * PHX_JUMP_NIBW));
     if (e->cfg.use_graph && e->cfg.kernel_mode != 2) {
         // the captured graph bakes in every engine buffer pointer: reuse it only if none moved
-        const void* bufs[12] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
-                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p, e->ev_rng.p };
+        const void* bufs[13] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
+                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p, e->ev_rng.p, e->jump4.p };
         const bool reuse = e->batch_exec && e->batch_call == c && memcmp(bufs, e->batch_bufs, sizeof(bufs)) == 0;
         if (!reuse) {
             if (e->batch_exec) { cudaGraphExecDestroy(e->batch_exec); e->batch_exec = nullptr; }

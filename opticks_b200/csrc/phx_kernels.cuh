@@ -308,11 +308,14 @@ PHX_D void phx_rng_jump4(curandStateXORWOW& s, const uint32_t* __restrict__ T, u
     s.d += (unsigned int)((362437ull * n) & 0xffffffffull);
 }
 
-// the 4-bit group tables of one jump matrix M: thread t builds entry (t / 16, t % 16)
+// the 4-bit group tables of jump matrix blockIdx.y of M (one per genstep in batched calls):
+// thread t builds entry (t / 16, t % 16)
 __global__ void k_jump_nibbles(const uint32_t* __restrict__ M, uint32_t* T)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= PHX_JUMP_BITS / 4 * 16) return;
+    M += (size_t)blockIdx.y * PHX_JUMP_MATW;
+    T += (size_t)blockIdx.y * PHX_JUMP_NIBW;
     const int g = t >> 4, k = t & 15;
     uint32_t o[5] = { 0u, 0u, 0u, 0u, 0u };
     for (int b = 0; b < 4; b++) {

@@ -31,7 +31,7 @@ struct PersistArgs {
     const uint32_t* rng;
     long long rng_slots;
     const uint32_t* jump;           // event jump matrices: one (single event) or one per genstep (batched)
-    const uint32_t* jump4;          // single event: the 4-bit group tables of the matrix, or null
+    const uint32_t* jump4;          // the 4-bit group tables of those matrices (same indexing), or null
     const uint32_t* ev_rng;         // optional: XORWOW states already advanced to each photon's event
     long long ev_rng_n;             //   (six planes of ev_rng_n words, by photon index; k_rng_event)
     phx_photon* photon;
@@ -116,8 +116,8 @@ PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, lon
         curand_init(A.seed, (unsigned long long)slot, A.rng_offset, &s);
     }
     if (ev > 0ull) {
-        if (A.jump4 && !A.gs_event) phx_rng_jump4(s, A.jump4, A.skip * ev);
-        else if (A.jump) phx_rng_jump(s, A.jump + (A.gs_event ? (size_t)gi * 1280 : 0), A.skip * ev);
+        if (A.jump4) phx_rng_jump4(s, A.jump4 + (A.gs_event ? (size_t)gi * PHX_JUMP_NIBW : 0), A.skip * ev);
+        else if (A.jump) phx_rng_jump(s, A.jump + (A.gs_event ? (size_t)gi * PHX_JUMP_MATW : 0), A.skip * ev);
         else skipahead(A.skip * ev, &s);
     }
 }

@@ -412,7 +412,8 @@ PHX_D void phx_load_sphoton(PhxPhoton& p, const float4* r)
 }
 
 // qsim::generate_photon qudarap/qsim.h:2532-2561
-PHX_COLD void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
+// inlined into its callers: out of line, its photon and RNG state would go through local memory
+PHX_D void generate_photon(PhxPhoton& p, curandStateXORWOW& rng, const float4* g, unsigned long long photon_id, const PhxProps& P, unsigned& status)
 {
     const int gencode = __float_as_int(g[0].x);
     switch (gencode) {
