@@ -75,8 +75,11 @@ typedef struct {
     int32_t  regroup;                 /* persistent kernel: bounces between lane refills */
     int32_t  chunk;                   /* persistent kernel: queue grab per warp in units of 32 photons */
     int32_t  use_graph;               /* batched launches: capture once as a CUDA graph and replay */
-    int64_t  wave_pool;               /* wavefront loop: in-flight path slots, 0 = 2^26 (176 B each); an
-                                         event with more photons refills freed slots from its queue */
+    int64_t  wave_pool;               /* wavefront loop: in-flight path slots (180 B each); a call with
+                                         more photons refills freed slots from its queue.  0 = every
+                                         photon of the call in flight while that fits in half of the
+                                         free device memory, at least 2^26 slots; the engine keeps its
+                                         slots until phx_destroy */
 } phx_config;
 
 typedef struct {

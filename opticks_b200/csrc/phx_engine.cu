@@ -99,6 +99,7 @@ struct phx_engine {
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
     bool has_full = false;    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
     int last_tail = 0;        // the last wavefront call finished its paths in one tail kernel
+    long long last_pool = 0;  // path slots of the last wavefront call
     std::vector<int> prim_node_offset;
     // physics
     cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr, planck_arr = nullptr;
@@ -1044,18 +1045,31 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // Wavefront form (phx_wave.cuh): fill a pool of paths, then rounds of trace + shade launches
 // until no path is live.  The live count is read back every PHX_WAVE_ROUNDS rounds, so the call
 // synchronises the stream; it cannot be captured into a graph.
-// Paths in flight: an event of up to this many photons starts all of them at once (generation
-// in one coherent pass, no refill) at 176 B of HBM per path; larger calls refill slots as paths
-// finish.  Measured on the 10M-photon detector event: 2^21 slots 339M, 2^22 367M, 2^23 416M,
-// 2^24 (no refill) 439M photons/s.
+// Paths in flight: unless phx_config.wave_pool fixes the count, every photon of a call starts at
+// once (generation in one coherent pass, no refill) as long as its slots fit in half of the device
+// memory still free, and never fewer than PHX_WAVE_POOL slots start; a larger call refills slots
+// as paths finish.  Refill costs throughput: 4096 uneven events in one batched call (338.9M
+// photons) took 833 ms through 2^26 slots, 728 ms through 2^27, 677 ms through 2^28 and 652 ms
+// with all of them in flight.  The engine keeps its slots for later calls (grow-only).
 #ifndef PHX_WAVE_POOL
 #define PHX_WAVE_POOL (1LL << 26)
 #endif
+#define PHX_WAVE_POOL_MAX (1LL << 31)   // slot indexes are 32-bit
+#define PHX_WAVE_SLOT_BYTES (sizeof(PhxWaveSlot) + sizeof(PhxWavePrd) + sizeof(long long) + 3 * sizeof(uint32_t))
 
-// path slots of the wavefront loop: the configured count, or PHX_WAVE_POOL
-static long long wave_pool_of(const phx_engine* e)
+// path slots of a wavefront call over N photons (adj: with the 32 score terms per slot)
+static long long wave_pool_for(const phx_engine* e, long long N, bool adj)
 {
-    return e->cfg.wave_pool > 0 ? (long long)e->cfg.wave_pool : (long long)PHX_WAVE_POOL;
+    long long pool = e->cfg.wave_pool > 0 ? (long long)e->cfg.wave_pool : (long long)PHX_WAVE_POOL;
+    if (e->cfg.wave_pool <= 0 && N > pool) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const size_t per = PHX_WAVE_SLOT_BYTES + (adj ? 8 * sizeof(float4) : 0);
+            const long long fit = (long long)e->wslot.n + (long long)(free_b / 2 / per);
+            pool = std::max(pool, std::min(N, fit));
+        }
+    }
+    return std::max<long long>(1, std::min(std::min(N, pool), PHX_WAVE_POOL_MAX));
 }
 // calls of at most this many photons get their event-advanced RNG states in one coherent pass
 // ahead of the loop (24 B per photon of scratch); larger ones advance each state as it starts
@@ -1090,7 +1104,8 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     if ((rc = wave_grid(k_wave_shade<CV, ADJ>, dev, g_shade))) return rc;
     if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
-    const long long pool = std::max<long long>(1, std::min<long long>(N, wave_pool_of(e)));
+    const long long pool = wave_pool_for(e, N, ADJ);
+    e->last_pool = pool;
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
     PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
     const bool refill = N > pool;
@@ -1243,7 +1258,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         // the pre-pass pays off where photons start a few lanes at a time (persistent refill,
         // wavefront refill); when every photon starts in the wavefront's first kernel, whole
         // warps advance their states there
-        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX && !(wave && N <= wave_pool_of(e))) {
+        if (wave_ok && event_index > 0 && N <= PHX_EV_RNG_MAX && !(wave && N <= wave_pool_for(e, N, false))) {
             PHX_CU(e->ev_rng.ensure((size_t)N * 6));
             k_rng_event<<<(unsigned)std::min<long long>((N + 255) / 256, 148LL * 16), 256, 0, st>>>(A, e->ev_rng.p, N);
             PHX_CU(cudaGetLastError());
@@ -1254,7 +1269,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
         e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + (A.ev_rng ? 1 : 0) +
-                           (wave ? 1 + (N > wave_pool_of(e) ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
+                           (wave ? 1 + (N > e->last_pool ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());

@@ -176,8 +176,15 @@ PHX_D void persist_finish(PhxLane& L, const PersistArgs& A, const PhxScore* sc)
     }
     if (A.hitword && (L.p.flagmask & A.hit_mask) == A.hit_mask) atomicOr(A.hitword + (idx >> 5), 1u << (idx & 31));
     if (A.ev_left) {
+        // one atomic per event among the lanes finishing together; the lane whose subtraction
+        // empties the count stamps the event's completion time
         const int e = A.gs_event ? L.ev : 0;
-        if (e >= 0 && e < A.num_event && atomicSub(A.ev_left + e, 1u) == 1u) A.ev_done_ns[e] = phx_globaltimer();
+        if (e >= 0 && e < A.num_event) {
+            const unsigned peers = __match_any_sync(__activemask(), e);
+            const unsigned n = (unsigned)__popc(peers);
+            if ((int)(threadIdx.x & 31u) == __ffs(peers) - 1 && atomicSub(A.ev_left + e, n) == n)
+                A.ev_done_ns[e] = phx_globaltimer();
+        }
     }
 }
 
