@@ -84,3 +84,32 @@ def test_wave_batched_equals_persistent(det, kw):
     assert torch.equal(outs[0][0].view(torch.int32), outs[1][0].view(torch.int32))
     assert torch.equal(outs[0][1], outs[1][1])
     a.close(); b.close()
+
+
+def test_wave_batched_beyond_minimum_pool_equals_persistent(det):
+    """84M photons in one batched call with wave_pool left at 0: more than the 2^26-slot minimum
+    pool, so the slot count comes from the free device memory (every photon in flight here);
+    photons, seq and hit count bit for bit against the persistent loop"""
+    torch = det[0]
+    gs = scenes.batched_events(1024, median=50000.0, lib=det[2])
+    ev = np.arange(len(gs), dtype=np.int32)
+    counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
+    N = int(counts.sum())
+    assert N > (1 << 26)
+    a, b = _engines(det, int(counts.max()))
+    g = torch.from_numpy(gs).cuda()
+    e = torch.from_numpy(ev).cuda()
+    outs = []
+    for eng in (a, b):
+        ph = torch.empty((N, 4, 4), dtype=torch.float32, device="cuda")
+        sq = torch.empty((N, 2, 2), dtype=torch.int64, device="cuda")
+        nh, st = eng.simulate_batched_device(g, e, N, photon=ph, seq=sq, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert st == 0
+        outs.append((ph, sq, nh))
+        eng.close()
+    assert torch.equal(outs[0][0].view(torch.int32), outs[1][0].view(torch.int32))
+    assert torch.equal(outs[0][1], outs[1][1])
+    assert outs[0][2] == outs[1][2]
+    del outs
+    torch.cuda.empty_cache()
