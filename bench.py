@@ -41,6 +41,12 @@ METRIC = "photons/s"
 ENGINE_KW = {}          # engine config overrides from the command line (kernel_mode)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 BYTES_PER_PHOTON_FIXED = 24 + 64 + 32 + 4.0 / 32   # RNG state + sphoton + sseq + hit bit
+# DRAM bytes (read + write) per photon of the wavefront kernels (k_wave_init, k_wave_trace_df,
+# k_wave_shade, k_wave_tail) of one simulate call, from an ncu capture of the 2M-photon detector
+# event (3.60 GB per call, three calls within 0.2 %): the path pool's 128 B slot and 32 B PRD
+# cross HBM every round.  The 10M event runs 12 pool rounds against 8 there, so per photon this
+# undercounts it by the few rounds of its last few hundred thousand paths.
+DRAM_BYTES_PER_PHOTON_WAVE = 1801.6
 
 
 def load_peaks():
@@ -514,7 +520,11 @@ def main():
                 "gpu_launches": launches,
                 "hit_fraction": f_hit,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": None, "kernel_ms": k_ms,
+                             "traffic": N * DRAM_BYTES_PER_PHOTON_WAVE if mode == 2 else None,
+                             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_wave_* "
+                                                "launches of a 2M-photon call, scaled by photons to this call"
+                                                if mode == 2 else None),
+                             "kernel_ms": k_ms,
                              "kernel": ("k_wave_init + k_wave_trace_df/k_wave_shade rounds (whole simulate launch sequence)"
                                         if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
