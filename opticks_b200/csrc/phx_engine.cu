@@ -99,7 +99,7 @@ struct phx_engine {
     int num_node = 0, num_prim = 0, num_inst = 0, num_leaf = 0, bvh_depth = 0;
     bool has_full = false;    // a list node or a leaf beyond sphere/zsphere/cylinder/box3/torus: full CSG variant
     int last_tail = 0;        // the last wavefront call finished its paths in one tail kernel
-    long long last_pool = 0;  // path slots of the last wavefront call
+    long long last_wave_launches = 0;   // kernel launches of the last wavefront loop
     std::vector<int> prim_node_offset;
     // physics
     cudaArray_t bnd_arr = nullptr, icdf_arr = nullptr, planck_arr = nullptr;
@@ -144,6 +144,8 @@ struct phx_engine {
     DevBuf<PhxWavePrd> wprd;
     DevBuf<long long> wsidx;
     DevBuf<uint32_t> wact0, wact1, wfree;
+    DevBuf<uint32_t> wlive, wlive_off, wlive_blk;    // refill rounds: live bits, their word and block offsets
+    DevBuf<long long> wlive_tot;
     DevBuf<float4> wscore;                          // adjoint score terms per slot
     DevBuf<unsigned> wcnt;
     long long last_launches = 0, last_rounds = 0;   // of the last plain simulate call
@@ -804,6 +806,7 @@ int phx_destroy(phx_engine* e)
     e->jump_pow.release(); e->jump_tab.release(); e->jump4.release(); e->ev_rng.release();
     e->merge.release();
     e->wslot.release(); e->wprd.release(); e->wsidx.release(); e->wact0.release(); e->wact1.release(); e->wfree.release(); e->wscore.release(); e->wcnt.release();
+    e->wlive.release(); e->wlive_off.release(); e->wlive_blk.release(); e->wlive_tot.release();
     if (e->batch_exec) cudaGraphExecDestroy(e->batch_exec);
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -1048,9 +1051,10 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // Paths in flight: unless phx_config.wave_pool fixes the count, every photon of a call starts at
 // once (generation in one coherent pass, no refill) as long as its slots fit in half of the device
 // memory still free, and never fewer than PHX_WAVE_POOL slots start; a larger call refills slots
-// as paths finish.  Refill costs throughput: 4096 uneven events in one batched call (338.9M
-// photons) took 833 ms through 2^26 slots, 728 ms through 2^27, 677 ms through 2^28 and 652 ms
-// with all of them in flight.  The engine keeps its slots for later calls (grow-only).
+// as paths finish, with each refill round's live list rebuilt in slot order (k_wave_act).  4096
+// uneven events in one batched call (338.9M photons) take 723 ms through 2^23 slots, 703 ms
+// through 2^26, 655 ms through 2^28 and 652 ms with all of them in flight.  The engine keeps its
+// slots for later calls (grow-only).
 #ifndef PHX_WAVE_POOL
 #define PHX_WAVE_POOL (1LL << 26)
 #endif
@@ -1105,12 +1109,17 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
     const long long N = A.N;
     const long long pool = wave_pool_for(e, N, ADJ);
-    e->last_pool = pool;
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
     PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
     const bool refill = N > pool;
     PHX_CU(e->wfree.ensure((size_t)pool));
     if (ADJ) PHX_CU(e->wscore.ensure((size_t)pool * 8));
+    const long long nlw = (pool + 31) / 32, nlb = (nlw + 255) / 256;     // live-bit words, scan blocks
+    if (refill) {
+        PHX_CU(e->wlive.ensure((size_t)nlw)); PHX_CU(e->wlive_off.ensure((size_t)nlw));
+        PHX_CU(e->wlive_blk.ensure((size_t)nlb)); PHX_CU(e->wlive_tot.ensure(1));
+        PHX_CU(cudaMemsetAsync(e->wlive.p, 0, sizeof(uint32_t) * (size_t)nlw, st));
+    }
     PHX_CU(cudaMemsetAsync(e->wcnt.p, 0, 4 * sizeof(unsigned), st));
     WaveArgs W;
     W.A = A;
@@ -1122,14 +1131,18 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     W.n_free = e->wcnt.p + 2;
     W.trace_ctr = e->wcnt.p + 3;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
+    W.live_bits = nullptr;
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
     k_wave_init<CV, ADJ><<<gi, 128, 0, st>>>(W);
+    W.live_bits = refill ? e->wlive.p : nullptr;
     PHX_CU(cudaGetLastError());
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
     e->last_rounds = 0;
     e->last_tail = 0;
     int cur = 0;
     bool done = false;
+    bool filling = refill;                          // photons still wait in the queue (as last read)
+    long long nl = 1;                               // launches of this call (k_wave_init)
     for (long long r = 0; r < max_rounds && !done;) {
         for (int k = 0; k < PHX_WAVE_ROUNDS; k++, r++) {
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
@@ -1139,7 +1152,15 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
             k_wave_trace<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
 #endif
             k_wave_shade<CV, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
-            if (refill) k_wave_fill<CV, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
+            nl += 2;
+            if (filling) {
+                k_wave_fill<CV, ADJ><<<(unsigned)g_fill[dev], 128, 0, st>>>(W);
+                k_word_scan<<<(unsigned)nlb, 256, 0, st>>>(e->wlive.p, nlw, e->wlive_off.p, e->wlive_blk.p);
+                k_block_scan<<<1, 1024, 0, st>>>(e->wlive_blk.p, (int)nlb, e->wlive_tot.p);
+                k_wave_act<<<(unsigned)((nlw + 255) / 256), 256, 0, st>>>(e->wlive.p, nlw, e->wlive_off.p, e->wlive_blk.p,
+                                                                         e->wlive_tot.p, act[1 - cur], cnt[1 - cur]);
+                nl += 4;
+            }
             cur = 1 - cur;
         }
         PHX_CU(cudaGetLastError());
@@ -1155,15 +1176,22 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
             memcpy(&head, e->h_pinned + 44, sizeof(head));
             queue_done = head >= (unsigned long long)N;
         }
+        if (filling && queue_done) {
+            // nothing left to start: the live list (in slot order now) shrinks by appends again
+            filling = false;
+            W.live_bits = nullptr;
+        }
         if (!done && queue_done && live <= (unsigned)PHX_WAVE_TAIL) {
             // few paths left and none queued: finish them in one kernel
             W.act_in = act[cur]; W.n_in = cnt[cur];
             k_wave_tail<CV, ADJ><<<(unsigned)((live + 127) / 128), 128, 0, st>>>(W);
             PHX_CU(cudaGetLastError());
             e->last_tail = 1;
+            nl += 1;
             done = true;
         }
     }
+    e->last_wave_launches = nl;
     if (!done) return phx_fail(-5, "wavefront loop did not drain within %lld rounds", max_rounds);
     return 0;
 }
@@ -1269,7 +1297,7 @@ static int plain_enqueue(phx_engine* e, const PhxPlainBufs& b, const float* d_gs
         int rc = wave ? launch_wave(e, A, st) : launch_persistent(e, A, e->cfg.block, st);
         if (rc) return rc;
         e->last_launches = 1 + (event_index > 0 ? (b.jump4 ? 2 : 1) : 0) + (A.ev_rng ? 1 : 0) +
-                           (wave ? 1 + (N > e->last_pool ? 3 : 2) * e->last_rounds + e->last_tail : 1) + (want_hits ? 3 : 0);
+                           (wave ? e->last_wave_launches : 1) + (want_hits ? 3 : 0);
     } else if (N > 0) {
         launch_simulate(e, a, N, st);
         PHX_CU(cudaGetLastError());

@@ -49,6 +49,8 @@ struct WaveArgs {
     unsigned* n_free;
     unsigned* trace_ctr;      // rays of this round handed to warps (k_wave_trace_df); zeroed by the kernel before
     long long pool;           // slots (init only)
+    uint32_t* live_bits;      // refill rounds: live slots as bits, turned into the next list in slot
+                              // order by k_wave_act (null: live slots are appended to act_out)
 };
 
 PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L)
@@ -130,7 +132,36 @@ PHX_D void wave_push(uint32_t* list, unsigned* count, bool keep, uint32_t s)
     if (keep) list[base + __popc(m & ((1u << lane) - 1u))] = s;
 }
 
-PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s) { wave_push(W.act_out, W.n_out, keep, s); }
+PHX_D void wave_append(const WaveArgs& W, bool keep, uint32_t s)
+{
+    if (W.live_bits) {
+        if (keep) atomicOr(W.live_bits + (s >> 5), 1u << (s & 31u));
+    } else {
+        wave_push(W.act_out, W.n_out, keep, s);
+    }
+}
+
+// The next round's live list in slot order, from the live bits of a refill round (offsets by
+// k_word_scan / k_block_scan over the same words); the bits are cleared for the round after.
+// A refilled pool is nearly full, so slot order makes the next round's slot reads and writes
+// almost sequential, where appends in finishing order scatter them over the pool.
+__global__ void k_wave_act(uint32_t* bits, long long nword, const uint32_t* wordoff, const uint32_t* blocksum,
+                           const long long* total, uint32_t* act, unsigned* n)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n = (unsigned)*total;
+    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;     // one word per thread
+    if (w >= nword) return;
+    uint32_t b = bits[w];
+    if (!b) return;
+    bits[w] = 0u;
+    uint32_t* o = act + (long long)blocksum[w >> 8] + wordoff[w];
+    const uint32_t s0 = (uint32_t)(w << 5);
+    for (int k = 0; b != 0u && k < 32; k++) {
+        const int lane = __ffs(b) - 1;
+        *o++ = s0 + (uint32_t)lane;
+        b &= b - 1u;
+    }
+}
 
 // Lanes in `need` take new photons from the queue until each has a path that can be traced
 // (photons that cannot take a first bounce are finished at once) or the queue is empty.
