@@ -9,18 +9,26 @@ Also on the line:
   e2e          photons/s through the reference-facing host call (CSGOptiXService.simulate:
                H2D gensteps, D2H hits into pinned buffers), timed per step; e2e_full also returns
                every photon and its seq (about 1 GB per step over PCIe)
-  roofline     the simulate launch sequence: 120.1 algorithmic bytes/photon / its duration vs
-               measured HBM (the path is latency-bound ray tracing, far from the HBM roof)
-  cpu_baseline the CPU oracle (port of the reference's path) on a bounded sample, all threads
-  forms        batched (4,096 lognormal events in one call; the one-kernel persistent form
+  roofline     the simulate launch sequence: algorithmic bytes per photon (48 RNG state + 64 sphoton
+               + 32 seq + 64 x hit fraction + 96 / photons per genstep) / its duration vs measured HBM
+               (the path is latency-bound ray tracing, far from the HBM roof), with the issue figures
+               of the dominant kernel from its ncu capture
+  cpu_baseline the CPU oracle (port of the reference's path) on all host threads over a stride
+               sample of the same event (200 photons of each of its 1,000 gensteps), and the same
+               for the C1 and Cerenkov forms
+  forms        C1 (1M torch photons, sphere-in-box) and a Cerenkov event (1M photons from 200
+               tracks); batched (4,096 lognormal events in one call; the one-kernel persistent form
                autotuned and replayed as a CUDA graph, and the wavefront form) vs the per-event
                loop, with per-event latency p50/p99; the adjoint (C5) cost and FD table; the CSG scan
-               (16,777,216 rays vs the 15-node tree with torus, rays/s, FP64 distance error)
+               (16,777,216 rays vs the 15-node tree with torus, rays/s)
 
---impl reference: the reference's CPU implementation of the path on the host cores.  Its qsim
-headers need glm/plog (absent) to build for the CPU, so the oracle port stands in (kind: port).
-Multi-GPU: each rank simulates its own events (no data-path collective); value = photons of all
-ranks / max over ranks of the device time.
+--impl reference: the reference's CPU implementation of the path on the host cores, on the same
+stride sample.  Its qsim headers need glm/plog (absent) to build for the CPU, so the oracle port
+stands in (kind: port).
+Multi-GPU (`--gpus N` re-launches itself under torch.distributed.run when WORLD_SIZE is unset):
+each rank simulates its own events (no data-path collective); value = photons of all ranks / max
+over ranks of the device time.  A second line item, `sharded`, splits one C3 event across the
+ranks (genstep slices) and gathers its hits and sensor counts over NCCL.
 """
 from __future__ import annotations
 
@@ -30,6 +38,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -40,13 +49,22 @@ sys.path.insert(0, ROOT)
 METRIC = "photons/s"
 ENGINE_KW = {}          # engine config overrides from the command line (kernel_mode)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-BYTES_PER_PHOTON_FIXED = 24 + 64 + 32 + 4.0 / 32   # RNG state + sphoton + sseq + hit bit
-# DRAM bytes (read + write) per photon of the wavefront kernels (k_wave_init, k_wave_trace_df,
-# k_wave_shade, k_wave_tail) of one simulate call, from an ncu capture of the 2M-photon detector
-# event (3.60 GB per call, three calls within 0.2 %): the path pool's 128 B slot and 32 B PRD
-# cross HBM every round.  The 10M event runs 12 pool rounds against 8 there, so per photon this
-# undercounts it by the few rounds of its last few hundred thousand paths.
-DRAM_BYTES_PER_PHOTON_WAVE = 1801.6
+# algorithmic bytes of one photon: the reference's 48 B curandStateXORWOW read (the engine's own
+# layout reads 24 B of it), the 64 B sphoton and 32 B sseq writes; + 64 B per hit and the genstep
+# share are added per workload
+BYTES_PER_PHOTON_FIXED = 48 + 64 + 32
+SAMPLE_PER_GENSTEP = 200       # CPU sample: this many photons of every genstep of the event
+# DRAM bytes (read + write) of the wavefront kernels of one simulate call of the C3 event, from
+# an ncu capture of one call's launches (profiles/dram_wavefront_detector_2M.md)
+DRAM_TRAFFIC = {"bytes_per_call": 3.6032e9, "photons": 2_000_000,
+                "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the k_wave_* launches of one "
+                          "2M-photon call of the detector event (profiles/dram_wavefront_detector_2M.md), scaled by "
+                          "photons to this call"}
+# issue figures of the dominant kernel (k_wave_trace_df, 54 % of the step) from its ncu --set full
+# capture (profiles/k_wave_trace_df_detector_2M_ncu_full.md)
+ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.54, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
+         "warps_active": 0.185, "lane_issue_frac": 0.376 * 11.90 / 32,
+         "source": "profiles/k_wave_trace_df_detector_2M_ncu_full.md"}
 
 
 def load_peaks():
@@ -75,11 +93,10 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"phx_bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
@@ -112,44 +129,65 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(fd, phys, gs, target_s=12.0):
-    """oracle port on all host threads over a bounded sample of the same event"""
+def stride_sample(gs, per_genstep=SAMPLE_PER_GENSTEP):
+    """the CPU sample of an event: every genstep kept, each with at most `per_genstep` photons, so
+    the sample spans the event's vertices (and Cerenkov tracks) as the whole event does"""
+    g = np.array(gs, dtype=np.float32, copy=True).reshape(-1, 6, 4)
+    c = g.view(np.int32)[:, 0, 3]
+    c[:] = np.minimum(c, per_genstep)
+    return g
+
+
+def oracle_rate(fd, phys, gs, reps=1, K=512, seed=123):
+    """photons/s of the CPU oracle (all host threads) over the photons of `gs`, numpy uniforms"""
     from oracle import oracle as O
     S = O.Scene(fd.arrays(), phys)
-    K = 1024
-    rng = np.random.Generator(np.random.PCG64(123))
-    cores = O.lib().oracle_threads()
-    n = 2000
-    u = rng.random((n, K), dtype=np.float32)
-    t0 = time.perf_counter()
-    S.simulate(gs, u, 0)
-    rate = n / (time.perf_counter() - t0)
-    n2 = int(min(2_000_000, max(n, rate * target_s)))
-    u = rng.random((n2, K), dtype=np.float32)
-    t0 = time.perf_counter()
-    S.simulate(gs, u, 0)
-    dt = time.perf_counter() - t0
-    return {"value": n2 / dt, "unit": METRIC, "cores": cores, "kind": "port",
-            "sample": f"first {n2} photons of the 10M-photon detector event (CPU oracle, numpy uniforms)"}
+    n = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
+    u = np.random.Generator(np.random.PCG64(seed)).random((n, K), dtype=np.float32)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        S.simulate(gs, u, 0)
+        times.append(time.perf_counter() - t0)
+    return n / statistics.mean(times), n, O.lib().oracle_threads(), times
+
+
+def cpu_baseline(fd, phys, gs, form_workloads=()):
+    """oracle port on all host threads over the stride sample of the event (and of each form)"""
+    sample = stride_sample(gs)
+    v, n, cores, times = oracle_rate(fd, phys, sample, reps=4)
+    out = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+           "sample": f"{SAMPLE_PER_GENSTEP} photons of each of the {len(gs)} gensteps of the event ({n} photons), "
+                     f"CPU oracle with numpy uniforms, {len(times)} timed passes of {statistics.mean(times):.1f} s"}
+    forms = {}
+    for name, (ffd, fphys, fgs, per, reps) in form_workloads:
+        fv, fn, _, ft = oracle_rate(ffd, fphys, stride_sample(fgs, per), reps=reps)
+        forms[name] = {"value": fv, "unit": METRIC, "sample_photons": fn, "passes": reps, "seconds": sum(ft),
+                       "sample": f"at most {per} photons of each of the {len(fgs)} gensteps"}
+    if forms:
+        out["forms"] = forms
+    return out
 
 
 def run_reference(args):
-    """--impl reference : CPU implementation of the path on the host cores (rank 0 only)"""
+    """--impl reference : CPU implementation of the path on the host cores (rank 0 only), each
+    step the stride sample of the C3 event"""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
     from oracle import oracle as O
     S = O.Scene(fd.arrays(), phys)
-    K = 1024
-    rng = np.random.Generator(np.random.PCG64(7))
-    n = args.ref_sample
-    u = rng.random((n, K), dtype=np.float32)
+    K = 512
+    sample = stride_sample(gs)
+    n = int(sample.view(np.int32)[:, 0, 3].sum())
+    u = np.random.Generator(np.random.PCG64(123)).random((n, K), dtype=np.float32)
+    small = stride_sample(gs, 2)
     for _ in range(args.warmup):
-        S.simulate(gs, u[: min(n, 500)], 0)
+        S.simulate(small, u[: int(small.view(np.int32)[:, 0, 3].sum())], 0)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        S.simulate(gs, u, 0)
+        S.simulate(sample, u, 0)
         times.append(time.perf_counter() - t0)
     v = n / statistics.mean(times)
     cores = O.lib().oracle_threads()
@@ -159,8 +197,9 @@ def run_reference(args):
             "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": args.gensteps,
                        "photons_per_genstep": args.per_genstep, "sample_photons_per_step": n},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": f"first {n} photons of the event per step (oracle port; the reference's qsim "
-                                       f"needs glm/plog to build for the CPU)"},
+                             "sample": f"{SAMPLE_PER_GENSTEP} photons of each of the {len(gs)} gensteps of the event per "
+                                       f"step ({n} photons; oracle port: the reference's qsim needs glm/plog to build "
+                                       f"for the CPU; warm-up steps take 2 photons per genstep)"},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -242,9 +281,9 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
 
 
 def measure_scan(torch, E, dev, n_rays=1 << 24):
-    """C2: rays/s of the CSG scan over the 15-node tree with torus, and FP64 distance error"""
+    """C2: rays/s of the CSG scan over the 15-node tree with torus (its FP64 distance error is
+    measured by the GPU tests against the FP64 oracle)"""
     from opticks_b200 import scenes
-    from oracle import oracle as O
     fd, p = scenes.csg_scan_tree(with_torus=True)
     A = fd.arrays()
     _, lib, _, _ = scenes.sphere_in_box(1)
@@ -265,18 +304,65 @@ def measure_scan(torch, E, dev, n_rays=1 << 24):
         e1.record(st)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 3
-        o = out.cpu().numpy()
-        sub = slice(0, 1 << 21)
-        t64, _ = O.csg_scan_t64(A["node"], A["itra"], int(A["prim"].view(np.int32)[p, 0, 1]), rays[:, sub], 0.0)
-        hg, h64 = o[sub, 3] > 0, t64 > 0
-        both = hg & h64
-        rel = np.abs(o[sub, 3][both] - t64[both]) / np.maximum(t64[both], 1.0)
-        res["polish" if pol else "fp32"] = {"rays_per_s": n_rays / (ms / 1e3), "ms": ms,
-                                            "bytes_per_ray": 40, "achieved_gbs": 40 * n_rays / (ms / 1e3) / 1e9,
-                                            "fp64_check_rays": int(1 << 21), "hit_miss_mismatch": int((hg != h64).sum()),
-                                            "rel_t_err_p999": float(np.quantile(rel, 0.999)), "rel_t_err_max": float(rel.max())}
+        hits = int((out[:, 3] > 0).sum().item())
+        res["polish" if pol else "fp32"] = {"rays_per_s": n_rays / (ms / 1e3), "ms": ms, "hits": hits,
+                                            "bytes_per_ray": 40, "achieved_gbs": 40 * n_rays / (ms / 1e3) / 1e9}
     eng.close()
     return dict(workload=f"{n_rays} rays, origins uniform in a 2 m cube, isotropic; 15-node CSG tree with torus", **res)
+
+
+def measure_plain(torch, E, fd, phys, gs, dev, event=7, reps=5, num_sensor=0):
+    """photons/s of one event (device-resident gensteps, photons + seq + hits out), CUDA events on
+    the launch stream; status must stay clear (no rejection loop reached its cap)"""
+    N = int(gs.view(np.int32)[:, 0, 3].sum())
+    eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=N, num_sensor=num_sensor, **ENGINE_KW), device=dev.index)
+    g = torch.from_numpy(gs).to(dev)
+    photon = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
+    seq = torch.empty((N, 2, 2), dtype=torch.int64, device=dev)
+    hit = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    assert st.cuda_stream != 0
+    run = lambda ev: eng.simulate_device(g, N, ev, photon=photon, seq=seq, hit=hit, hit_capacity=N, stream=st.cuda_stream)
+    for w in range(3):
+        run(event + 1000 + w)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    status, hits = 0, 0
+    for r in range(reps):
+        nh, stt = run(event + r)
+        status |= stt
+        hits += nh
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    eng.close()
+    return {"photons": N, "photons_per_s": N / (ms / 1e3), "ms": ms, "hit_fraction": hits / (N * reps), "status": status,
+            "steps": reps}
+
+
+def c1_workload():
+    """C1: 1M torch photons (isotropic, 440 nm, random linear polarisation) in the sphere-in-box"""
+    from opticks_b200 import scenes
+    fd, lib, _, gs = scenes.sphere_in_box(1_000_000)
+    return fd, lib.arrays(), gs
+
+
+def cerenkov_workload(lib, num_track=200, per_track=5000, seed=21):
+    """1M Cerenkov photons from 200 tracks in the liquid scintillator: 1-40 mm steps, beta from
+    0.75 to 0.9999 (the bnd-texture rejection sampling of wavelength and cone angle)"""
+    from opticks_b200 import scenes
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ml = lib.material_line("LS")
+    pos = scenes.uniform_ball(num_track, 16000.0, rng)
+    gs = []
+    for k in range(num_track):
+        d = rng.normal(size=3)
+        d *= rng.uniform(1.0, 40.0) / np.linalg.norm(d)
+        beta = rng.uniform(0.75, 0.9999)
+        gs.append(scenes.cerenkov_genstep(per_track, tuple(pos[k]), ml, delta=tuple(d), beta_inverse=1.0 / beta,
+                                          time=float(rng.uniform(0.0, 5.0))))
+    return np.stack(gs)
 
 
 def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=10000, fd_events=4, precise_events=96,
@@ -374,6 +460,32 @@ def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=1
                                      "rows": precise}}}
 
 
+def relaunch(n):
+    """--gpus N without a launcher: run this script again as N ranks under torch.distributed.run"""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    sys.exit(subprocess.call(cmd))
+
+
+def check_ranks():
+    """every rank joins a gloo group and sums its rank; rank 0 prints what it saw"""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    t = torch.tensor([dist.get_rank()], dtype=torch.int64)
+    dist.all_reduce(t)
+    if dist.get_rank() == 0:
+        print(json.dumps({"check_ranks": dist.get_world_size(), "rank_sum": int(t.item())}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,16 +494,25 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--gensteps", type=int, default=1000)
     ap.add_argument("--per-genstep", type=int, default=10000)
-    ap.add_argument("--ref-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--kernel-mode", type=int, default=None, help="engine kernel_mode override (1 persistent, 2 wavefront)")
+    ap.add_argument("--tune-cache", default=None, help="json file holding the autotuner's choice between runs")
+    ap.add_argument("--check-ranks", action="store_true",
+                    help="start the ranks and exchange one gloo all-reduce, then exit (launch check, no GPU)")
     args = ap.parse_args()
     if args.kernel_mode is not None:
         ENGINE_KW["kernel_mode"] = args.kernel_mode
     args.warmup = max(args.warmup, 3)
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1 and args.impl == "engine":
+        return relaunch(args.gpus)
+    world_env = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "engine" and world_env != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE {world_env}")
+    if args.check_ranks:
+        return check_ranks()
     if args.impl == "reference":
         return run_reference(args)
 
@@ -470,7 +591,7 @@ def main():
     k_ms = k0.elapsed_time(k1) / ksteps
     f_hit = hits_total / (N * args.steps)
     ppg = N / len(gs)
-    bytes_per_photon = BYTES_PER_PHOTON_FIXED + 96.0 / ppg
+    bytes_per_photon = BYTES_PER_PHOTON_FIXED + 64.0 * f_hit + 96.0 / ppg
     peak, peak_kind = load_peaks()
     achieved = N * bytes_per_photon / (k_ms / 1e3) / 1e9
 
@@ -494,6 +615,29 @@ def main():
                 "d2h_bytes_per_step": int(statistics.mean(d2h)), "ms_per_step": 1e3 * statistics.mean(times)}
     e2e = dict(host_run(False, base_event + 300), api="phx_simulate: host gensteps in, host hits out (CSGOptiXService.simulate)")
     e2e_full = dict(host_run(True, base_event + 400), api="phx_simulate: host gensteps in, host photons + seq + hits out")
+    sharded = None
+    if world > 1:
+        # strong scaling: one C3 event split across the ranks in genstep slices (photon offsets keep
+        # the single-GPU RNG streams), hits all-gathered in photon order and sensor counts summed
+        from opticks_b200 import shard
+        fn = shard.engine_slice_fn(eng, dev, num_sensor=scenes.NUM_PMT, stream=sp)
+        shard.simulate_sharded(fn, gs, 1)
+        torch.cuda.synchronize()
+        dist.barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        s0.record(stream)
+        for r in range(reps):
+            out = shard.simulate_sharded(fn, gs, 2 + r)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([s0.elapsed_time(s1) / reps], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sharded = {"photons_per_s": N / (float(t.item()) / 1e3), "ms_per_event": float(t.item()), "photons_per_event": N,
+                   "hits_gathered": int(out["hit"].shape[0]), "scaling": "strong",
+                   "note": "one event split across the ranks (genstep slices), NCCL all-gather of hits and all-reduce "
+                           "of per-sensor counts inside the timed region; max over ranks"}
+        del out
     eng.close()
     del photon, seq, hit
     torch.cuda.empty_cache()
@@ -501,12 +645,20 @@ def main():
     clocks = clk.summary()
     if rank == 0:
         forms = None
+        c1_fd, c1_phys, c1_gs = c1_workload()
+        ck_gs = cerenkov_workload(lib)
         if not args.no_forms and world == 1:
-            forms = {"batched": measure_batched(torch, E, fd, lib, phys, dev, args.events,
-                                                tune_cache=os.path.join(ROOT, "gpurun_out", "autotune.json")),
+            forms = {"c1": dict(measure_plain(torch, E, c1_fd, c1_phys, c1_gs, dev),
+                                workload="C1: 1,000,000 torch photons (T_SPHERE with random linear polarisation, 440 nm) "
+                                         "from the centre of a 1 m water sphere in a 3 m detecting box"),
+                     "cerenkov": dict(measure_plain(torch, E, fd, phys, ck_gs, dev, num_sensor=scenes.NUM_PMT),
+                                      workload=f"detector, {len(ck_gs)} Cerenkov tracks x 5,000 photons, beta 0.75-0.9999, "
+                                               "1-40 mm steps in the liquid scintillator"),
+                     "batched": measure_batched(torch, E, fd, lib, phys, dev, args.events, tune_cache=args.tune_cache),
                      "scan": measure_scan(torch, E, dev),
                      "adjoint": measure_adjoint(torch, E, fd, lib, phys, dev)}
-        cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(fd, phys, gs)
+        cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(
+            fd, phys, gs, form_workloads=(("c1", (c1_fd, c1_phys, c1_gs, 200_000, 50)), ("cerenkov", (fd, phys, ck_gs, 500, 2))))
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -520,16 +672,16 @@ def main():
                 "gpu_launches": launches,
                 "hit_fraction": f_hit,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "traffic": N * DRAM_BYTES_PER_PHOTON_WAVE if mode == 2 else None,
-                             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_wave_* "
-                                                "launches of a 2M-photon call, scaled by photons to this call"
-                                                if mode == 2 else None),
+                             "traffic": DRAM_TRAFFIC["bytes_per_call"] * N / DRAM_TRAFFIC["photons"] if mode == 2 else None,
+                             "traffic_source": DRAM_TRAFFIC["source"] if mode == 2 else None,
+                             "issue": ISSUE if mode == 2 else None,
                              "kernel_ms": k_ms,
                              "kernel": ("k_wave_init + k_wave_trace_df/k_wave_shade rounds (whole simulate launch sequence)"
                                         if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
                              "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},
-                "e2e": e2e, "e2e_full": e2e_full, "clocks": clocks, "cpu_baseline": cpu, "forms": forms}
+                "e2e": e2e, "e2e_full": e2e_full, "clocks": clocks, "cpu_baseline": cpu, "forms": forms,
+                "sharded": sharded}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -19,6 +19,7 @@
  *   phx_count_photons     SGenstep::GetNumPhoton / QEvt::setGenstepUpload  qudarap/QEvt.cc:199-330
  *   phx_csg_scan[_device] CSGScan / _CSGScan_intersect  CSG/CSGScan.cc:29-130, CSG/CSGScan.cu:11-25
  *   phx_rng_sequence      QSim::rng_sequence          qudarap/QSim.cc:1070-1168, qudarap/QSim.cu:43-68
+ *   phx_trace[_device]    the trace step of simtrace  CSGOptiX/CSGOptiX7.cu:112-218, :563-603
  *   phx_simulate_batched  (no counterpart: the reference loops QSim::simulate per event,
  *                          qudarap/QSim.cc:436-595)
  *   phx_adjoint_device    (no counterpart: score-function gradients of expected hits)
@@ -103,6 +104,13 @@ const char* phx_version(void);
 int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_config* cfg, int device, phx_engine** out);
 int phx_destroy(phx_engine* e);
 
+/* Release the device memory the engine grew for its calls (no reference counterpart): the wavefront
+ * path pool (180 B per in-flight path; by default every photon of the largest call), the event-advanced
+ * RNG states, the host path's staging buffers and the hit-merge workspace.  For a host application
+ * that shares the GPU after a large call; the next call allocates what it needs again.  Waits for
+ * all work on the device first.  *bytes_released (optional) receives the bytes freed. */
+int phx_trim(phx_engine* e, int64_t* bytes_released);
+
 /* sum of quad6 q0.w photon counts */
 int64_t phx_count_photons(const float* gensteps, int32_t num_genstep);
 
@@ -122,12 +130,16 @@ int phx_simulate_device(phx_engine* e, const float* d_gensteps, int32_t num_gens
  * cudaMalloc/cudaFree may imply): it calls no cudaMalloc, cudaFree or allocating library routine.
  * Its scratch is one fixed device array in the library (about 2.6 MB, held on every GPU that loads
  * the library until the process exits), sized for at most 8,388,608 photons and 65,536 gensteps per
- * call; larger calls are rejected with an error.  Inputs and outputs are the caller's device
+ * call; larger calls are rejected with an error.  Its bounce loop is always the one-kernel form
+ * (the persistent work queue; one thread per photon with kernel_mode 0), never the wavefront rounds
+ * that phx_simulate_device runs by default, because their path pool is sized per call: results are
+ * bit-identical, throughput is that of kernel_mode 1.  Inputs and outputs are the caller's device
  * buffers as for phx_simulate_device; when hits or sensor counts are requested the photon output
  * must be given (hits are selected from it).  The photons must lie within the RNG slots prepared at
  * phx_create (config max_photon); otherwise the call is rejected rather than growing them.
  * The first call on a device looks up the device address of the scratch array (once per device);
- * make that first call before any stream capture.  All calls share the one array: calls that
+ * make that first call before any stream capture.  The looked-up address is kept for the life of the
+ * process: resetting the device (cudaDeviceReset) after the first call is not supported.  All calls share the one array: calls that
  * overlap on the GPU (on any engine of the same device) race; serialise them. */
 int phx_simulate_device_noalloc(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                                 int32_t event_index, int64_t photon_offset, phx_outputs* d_out, void* stream);
@@ -150,6 +162,17 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
 int phx_csg_scan(phx_engine* e, int32_t prim, float t_min, const float* rays, int64_t n, float* isect);
 int phx_csg_scan_device(phx_engine* e, int32_t prim, float t_min, const float* d_rays, int64_t n, float* d_isect,
                         int32_t polish, void* stream);
+
+/* Closest hit of arbitrary rays over the whole geometry: the trace step of simtrace
+ * (CSGOptiX/CSGOptiX7.cu:563-603, which calls trace() :112-218 and records the PRD).  rays SoA (6,n) =
+ * ox,oy,oz,dx,dy,dz ; prd (n,2,4) in the reference's quad2 layout (sysrap/squad.h:180-245):
+ * q0 = world normal xyz (unnormalised, as the CH program leaves it), t ; q1 = lposcost, 0,
+ * iindex<<16|identity, globalPrimIdx<<16|boundary, all of q1.zw 0xffffffff for a miss.  Hits with
+ * t outside [t_min, t_max) are ignored.  *status (optional) receives the PHX_STATUS bits of the
+ * rays (the call then synchronises the stream). */
+int phx_trace(phx_engine* e, const float* rays, int64_t n, float t_min, float t_max, float* prd, uint32_t* status);
+int phx_trace_device(phx_engine* e, const float* d_rays, int64_t n, float t_min, float t_max, float* d_prd, uint32_t* status,
+                     void* stream);
 
 /* per-photon uniform streams (QSim::rng_sequence): out (num_photon, num_per_photon) float32,
  * photon slots photon_offset..photon_offset+num_photon-1 advanced by the event skipahead */

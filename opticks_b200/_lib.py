@@ -60,6 +60,7 @@ SIGNATURES = {
     "phx_version": (C.c_char_p, []),
     "phx_create": (C.c_int, [C.POINTER(PhxGeometry), C.POINTER(PhxPhysics), C.POINTER(PhxConfig), C.c_int, C.POINTER(C.c_void_p)]),
     "phx_destroy": (C.c_int, [C.c_void_p]),
+    "phx_trim": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "phx_count_photons": (C.c_int64, [C.c_void_p, C.c_int32]),
     "phx_simulate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(PhxOutputs)]),
     "phx_simulate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int64, C.POINTER(PhxOutputs),
@@ -70,6 +71,9 @@ SIGNATURES = {
                                               C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PhxOutputs), C.c_void_p]),
     "phx_csg_scan": (C.c_int, [C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p]),
     "phx_csg_scan_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32, C.c_void_p]),
+    "phx_trace": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "phx_trace_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_float, C.c_void_p, C.POINTER(C.c_uint32),
+                                   C.c_void_p]),
     "phx_rng_sequence": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_void_p]),
     "phx_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_int32,
                                      C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -411,6 +411,25 @@ __global__ void k_csg_scan(PhxCsgCtx csg, int root, float t_min, const float* ra
     if (st) atomicOr(status, st);
 }
 
+// The trace step of simtrace (CSGOptiX/CSGOptiX7.cu:563-603 calls trace(), :112-218): the closest
+// hit of arbitrary rays over the whole geometry, one thread per ray (SoA rays), written as the
+// reference's quad2 PRD (sysrap/squad.h:180-245): q0 normal.xyz (world, unnormalised), t;
+// q1 lposcost, 0, iindex<<16|identity, globalPrimIdx<<16|boundary (0xffffffff words: a miss)
+template <int CV>
+__global__ void k_trace_rays(PhxScene S, const float* rays, long long n, float t_min, float t_max, float4* prd_out, unsigned* status)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float3 o = make_float3(__ldg(rays + i), __ldg(rays + n + i), __ldg(rays + 2 * n + i));
+    const float3 d = make_float3(__ldg(rays + 3 * n + i), __ldg(rays + 4 * n + i), __ldg(rays + 5 * n + i));
+    unsigned st = 0;
+    PhxPRD prd;
+    phx_trace<CV>(S, o, d, t_min, t_max, prd, st);
+    prd_out[2 * i] = make_float4(prd.normal.x, prd.normal.y, prd.normal.z, prd.distance);
+    prd_out[2 * i + 1] = make_float4(prd.lposcost, 0.f, __uint_as_float(prd.ii_id), __uint_as_float(prd.gp_bd));
+    if (st) atomicOr(status, st);
+}
+
 // QSim::rng_sequence : uniforms of each photon slot after the event skipahead
 __global__ void k_rng_sequence(const uint32_t* rng, long long slots, unsigned long long skip, long long first, long long n, int K, float* out)
 {
@@ -811,6 +830,23 @@ int phx_destroy(phx_engine* e)
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
+    return 0;
+}
+
+int phx_trim(phx_engine* e, int64_t* bytes_released)
+{
+    if (!e) return phx_fail(-1, "phx_trim: null engine");
+    PHX_CU(cudaSetDevice(e->device));
+    PHX_CU(cudaStreamSynchronize(e->stream));
+    PHX_CU(cudaDeviceSynchronize());   // calls on caller streams may still use the buffers
+    int64_t b = 0;
+    auto rel = [&b](auto& buf) { b += (int64_t)(buf.n * sizeof(*buf.p)); buf.release(); };
+    rel(e->wslot); rel(e->wprd); rel(e->wsidx); rel(e->wact0); rel(e->wact1); rel(e->wfree); rel(e->wscore); rel(e->wcnt);
+    rel(e->wlive); rel(e->wlive_off); rel(e->wlive_blk); rel(e->wlive_tot);
+    rel(e->ev_rng); rel(e->photon); rel(e->seq); rel(e->hit); rel(e->hitword); rel(e->wordoff);
+    e->merge.release();
+    if (e->batch_exec) { cudaGraphExecDestroy(e->batch_exec); e->batch_exec = nullptr; }
+    if (bytes_released) *bytes_released = b;
     return 0;
 }
 
@@ -1227,6 +1263,20 @@ static void launch_scan_t(const PhxCsgCtx& csg, int root, float t_min, const flo
     k_csg_scan<CV><<<(unsigned)((n + B - 1) / B), B, 0, st>>>(csg, root, t_min, d_rays, n, out, status);
 }
 
+template <int CV>
+static void launch_trace_t(const PhxScene& S, const float* d_rays, long long n, float t_min, float t_max, float4* out, unsigned* status,
+                           cudaStream_t st)
+{
+    const int B = 128;
+    k_trace_rays<CV><<<(unsigned)((n + B - 1) / B), B, 0, st>>>(S, d_rays, n, t_min, t_max, out, status);
+}
+
+static int launch_trace(phx_engine* e, const float* d_rays, long long n, float t_min, float t_max, float4* out, cudaStream_t st)
+{
+    const PhxScene S = scene_of(e, e->cfg.root_polish);
+    PHX_CV_RETURN(cv_of(e, e->cfg.root_polish != 0), (launch_trace_t<CVK>(S, d_rays, n, t_min, t_max, out, e->status.p, st), 0));
+}
+
 extern "C" {
 
 // device buffers of one plain simulate call (engine buffers, or the fixed no-alloc scratch)
@@ -1435,6 +1485,45 @@ int phx_csg_scan(phx_engine* e, int32_t prim, float t_min, const float* rays, in
     if (!rc && n > 0) {
         cudaError_t ce = cudaMemcpyAsync(isect, d_o, n * 16, cudaMemcpyDeviceToHost, st);
         if (ce != cudaSuccess) rc = phx_fail(-2, "phx_csg_scan: copy back failed: %s", cudaGetErrorString(ce));
+    }
+    cudaFreeAsync(d_r, st);
+    cudaFreeAsync(d_o, st);
+    PHX_CU(cudaStreamSynchronize(st));
+    return rc;
+}
+
+int phx_trace_device(phx_engine* e, const float* d_rays, int64_t n, float t_min, float t_max, float* d_prd, uint32_t* status,
+                     void* stream)
+{
+    if (!e || (n > 0 && (!d_rays || !d_prd))) return phx_fail(-1, "phx_trace_device: null argument");
+    if (!(t_max > t_min)) return phx_fail(-1, "phx_trace_device: t_max %g must exceed t_min %g", (double)t_max, (double)t_min);
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+    PHX_CU(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned), st));
+    if (n > 0) launch_trace(e, d_rays, n, t_min, t_max, reinterpret_cast<float4*>(d_prd), st);
+    PHX_CU(cudaGetLastError());
+    if (status) {
+        PHX_CU(cudaMemcpyAsync(e->h_pinned, e->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        PHX_CU(cudaStreamSynchronize(st));
+        *status = e->h_pinned[0];
+    }
+    return 0;
+}
+
+int phx_trace(phx_engine* e, const float* rays, int64_t n, float t_min, float t_max, float* prd, uint32_t* status)
+{
+    if (!e || (n > 0 && (!rays || !prd))) return phx_fail(-1, "phx_trace: null argument");
+    PHX_CU(cudaSetDevice(e->device));
+    cudaStream_t st = e->stream;
+    float* d_r = nullptr;
+    float* d_o = nullptr;
+    PHX_CU(cudaMallocAsync(&d_r, std::max<int64_t>(1, n) * 24, st));
+    PHX_CU(cudaMallocAsync(&d_o, std::max<int64_t>(1, n) * 32, st));
+    if (n > 0) PHX_CU(cudaMemcpyAsync(d_r, rays, n * 24, cudaMemcpyHostToDevice, st));
+    int rc = phx_trace_device(e, d_r, n, t_min, t_max, d_o, status, st);
+    if (!rc && n > 0) {
+        cudaError_t ce = cudaMemcpyAsync(prd, d_o, n * 32, cudaMemcpyDeviceToHost, st);
+        if (ce != cudaSuccess) rc = phx_fail(-2, "phx_trace: copy back failed: %s", cudaGetErrorString(ce));
     }
     cudaFreeAsync(d_r, st);
     cudaFreeAsync(d_o, st);
@@ -1723,10 +1812,13 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
 // Some callers cannot allocate device memory per call: a framework whose caching allocator owns
 // every device byte, or a per-event loop that cannot afford the device-wide synchronisation that
 // cudaMalloc/cudaFree may imply.  phx_simulate_device_noalloc serves them: its scratch (genstep
-// offsets, hit bit words and their prefix sums, counters, status) lives in one fixed file-scope
-// device array instead of engine buffers that grow on demand.  The array below is sized for
-// PHX_NOALLOC_MAX_PHOTON photons and PHX_NOALLOC_MAX_GENSTEP gensteps per call (about 2.6 MB)
-// and is held on every GPU that loads this library until the process exits.
+// offsets, hit bit words and their prefix sums, counters, status, the event jump matrix and its
+// 4-bit group tables) lives in one fixed file-scope device array instead of engine buffers that
+// grow on demand.  The array below is sized for PHX_NOALLOC_MAX_PHOTON photons and
+// PHX_NOALLOC_MAX_GENSTEP gensteps per call (about 2.6 MB) and is held on every GPU that loads
+// this library until the process exits.  The bounce loop is always the one-kernel form (the
+// persistent work queue, or one thread per photon when kernel_mode is 0): the wavefront loop's
+// path pool is sized per call and would need allocation.
 #define PHX_NOALLOC_MAX_PHOTON (1ll << 23)
 #define PHX_NOALLOC_MAX_GENSTEP 65536
 #define PHX_NOALLOC_WORDS (PHX_NOALLOC_MAX_PHOTON / 32)
@@ -1740,6 +1832,7 @@ struct PhxNoAllocScratch {
     long long counters[8];
     unsigned status[8];
     __align__(16) uint32_t jump[PHX_JUMP_MATW];
+    __align__(16) uint32_t jump4[PHX_JUMP_NIBW];
 };
 
 static __device__ __align__(256) PhxNoAllocScratch g_phx_noalloc_scratch;
@@ -1792,8 +1885,10 @@ extern "C" int phx_simulate_device_noalloc(phx_engine* e, const float* d_genstep
     if (rc) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
     const long long N = num_photon;
-    // the same launch sequence as phx_simulate_device, on the fixed scratch
-    PhxPlainBufs b = { scr->gs_off, scr->hitword, scr->wordoff, scr->blocksum, scr->counters, scr->status, scr->jump };
+    // phx_simulate_device's launch sequence in its one-kernel loop form (never the wavefront
+    // rounds), on the fixed scratch
+    PhxPlainBufs b = { scr->gs_off, scr->hitword, scr->wordoff, scr->blocksum, scr->counters, scr->status, scr->jump,
+                       scr->jump4 };
     rc = plain_enqueue(e, b, d_gensteps, num_genstep, N, event_index, photon_offset, reinterpret_cast<phx_photon*>(d_out->photon),
                        reinterpret_cast<phx_seq*>(d_out->seq), reinterpret_cast<phx_photon*>(d_out->hit), d_out->hit_capacity,
                        d_out->sensor_hits, want_hits, st);

@@ -115,6 +115,12 @@ class Engine:
             _lib.lib().phx_destroy(self._h)
             self._h = None
 
+    def trim(self) -> int:
+        """release the device memory grown for calls (wavefront pool and the like); returns bytes freed"""
+        b = C.c_int64(0)
+        _lib.check(_lib.lib().phx_trim(self._h, C.byref(b)), "phx_trim")
+        return int(b.value)
+
     def __del__(self):
         try:
             self.close()
@@ -202,6 +208,17 @@ class Engine:
         _lib.check(_lib.lib().phx_csg_scan_device(self._h, int(prim), float(t_min), C.c_void_p(rays_dev.data_ptr()), int(n),
                                                   C.c_void_p(isect_dev.data_ptr()), int(polish),
                                                   C.c_void_p(stream) if stream else None), "phx_csg_scan_device")
+
+    def trace(self, rays: np.ndarray, t_min: float = 0.0, t_max: float = 1e6) -> tuple[np.ndarray, int]:
+        """closest hit of each ray (SoA (6,n)) over the whole geometry: (n,2,4) quad2 PRD rows
+        (normal, t; lposcost, 0, iindex<<16|identity, globalPrimIdx<<16|boundary) and the status bits"""
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        assert rays.ndim == 2 and rays.shape[0] == 6
+        n = rays.shape[1]
+        out = np.empty((n, 2, 4), np.float32)
+        st = C.c_uint32(0)
+        _lib.check(_lib.lib().phx_trace(self._h, _ptr(rays), n, float(t_min), float(t_max), _ptr(out), C.byref(st)), "phx_trace")
+        return out, int(st.value)
 
     def rng_sequence(self, eventID: int, photon_offset: int, num_photon: int, num_per_photon: int) -> np.ndarray:
         out = np.empty((num_photon, num_per_photon), np.float32)

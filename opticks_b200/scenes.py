@@ -137,6 +137,29 @@ def sphere_in_box(num_photon: int = 1_000_000):
     return fd, lib, None, gs
 
 
+def sphere_in_box_surface(num_photon: int = 200_000, detect: float = 0.2, absorb: float = 0.2,
+                          reflect_specular: float = 0.3, reflect_diffuse: float = 0.3):
+    """C1's sphere-in-box with a box surface that also reflects: each wall hit detects, absorbs,
+    reflects diffusely (Lambertian) or specularly with the given fractions, so photons cross the
+    box and the water sphere many times (qudarap/qsim.h:1680-1750 picks the branch with one
+    uniform; the specular share is what is left over, qsim.h never reads reflect_specular)"""
+    lib = M.BoundaryLib()
+    lib.mat(VACUUM)
+    lib.mat(M.Material("Rock", rindex=1.5, absorption_length=1.0, scattering_length=1e9))
+    lib.mat(WATER_C1)
+    lib.sur(M.Surface("Wall", detect=detect, absorb=absorb, reflect_specular=reflect_specular,
+                      reflect_diffuse=reflect_diffuse))
+    b_box = lib.add("Rock", "", "Wall", "Vacuum")
+    b_sph = lib.add("Vacuum", "", "", "Water")
+    fd = F.Foundry()
+    p0 = fd.add_prim(F.box3(3000.0, 3000.0, 3000.0), b_box)
+    p1 = fd.add_prim(F.sphere(1000.0), b_sph)
+    s0 = fd.add_solid("box_sphere", [p0, p1])
+    fd.add_inst(np.eye(4), s0)
+    gs = torch_genstep(num_photon, wavelength=440.0, radius=0.0, type_=T_SPHERE, distance=0.25)[None]
+    return fd, lib, None, gs
+
+
 # ---------------------------------------------------------------- C2
 def csg_scan_tree(with_torus: bool = True):
     """returns (foundry, prim index) of the 15-node tree"""
@@ -311,7 +334,12 @@ def ls_rindex(wl):
     return np.clip(1.50 + (wl - 300.0) * (1.48 - 1.50) / 300.0, 1.44, 1.56)
 
 
-def detector_lib():
+def detector_lib(pmt_ems: int = M.EMS_SURFACE, world_surface: M.Surface | None = None):
+    """the detector's boundary library.  ``pmt_ems`` is the PMT cathode's surface kind: with
+    ``EMS_SENSOR_A`` (smatsur_Surface_zplus_sensor_A) a hit on the PMT's upper hemisphere (local
+    z >= 0) always detects and one below it takes the ordinary surface branch (qudarap/qsim.h:
+    2304-2316).  ``world_surface`` replaces the absorbing rock surface, e.g. with a reflecting one
+    so that photons come back onto the backs of the PMTs."""
     lib = M.BoundaryLib()
     ls = M.Material("LS", rindex=ls_rindex, absorption_length=60000.0, scattering_length=27000.0,
                     reemission_prob=lambda wl: np.where(np.asarray(wl) < 400.0, 0.5, 0.0))
@@ -321,17 +349,18 @@ def detector_lib():
     pyrex = M.Material("Pyrex", rindex=1.458, absorption_length=1e3, scattering_length=1e9)
     for m in (ls, acr, water, rock, pyrex):
         lib.mat(m)
-    lib.sur(M.Surface("RockAbsorber", detect=0.0, absorb=1.0))
-    lib.sur(M.Surface("PMTCathode", detect=0.3, absorb=0.7))
-    b_world = lib.add("Rock", "", "RockAbsorber", "Water")
+    world = world_surface or M.Surface("RockAbsorber", detect=0.0, absorb=1.0)
+    lib.sur(world)
+    lib.sur(M.Surface("PMTCathode", detect=0.3, absorb=0.7, ems=pmt_ems))
+    b_world = lib.add("Rock", "", world.name, "Water")
     b_acr = lib.add("Water", "", "", "Acrylic")
     b_ls = lib.add("Acrylic", "", "", "LS")
     b_pmt = lib.add("Water", "PMTCathode", "PMTCathode", "Pyrex")
     return lib, (b_world, b_acr, b_ls, b_pmt)
 
 
-def detector(num_pmt: int = NUM_PMT):
-    lib, (b_world, b_acr, b_ls, b_pmt) = detector_lib()
+def detector(num_pmt: int = NUM_PMT, pmt_ems: int = M.EMS_SURFACE, world_surface: M.Surface | None = None):
+    lib, (b_world, b_acr, b_ls, b_pmt) = detector_lib(pmt_ems, world_surface)
     fd = F.Foundry()
     p_world = fd.add_prim(F.sphere(R_WATER), b_world)
     p_acr = fd.add_prim(F.sphere(R_LS + T_ACRYLIC), b_acr)

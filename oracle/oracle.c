@@ -153,6 +153,26 @@ int oracle_csg_scan_t64(const float* node, const float* itra, const float* plan,
     return err_all;
 }
 
+/* the same with FP64 rays (SoA (6,n) doubles): rays carried into a prim's frame in double keep
+   the world ray exactly, so the distance error measured against it is the FP32 path's alone */
+int oracle_csg_scan_t64d(const float* node, const float* itra, const float* plan, int root, double tmin, const double* rays,
+                         long long n, double* t)
+{
+    oracle_csg g = { node, itra, 0, plan };
+    int err_all = 0;
+#pragma omp parallel for schedule(static) reduction(| : err_all)
+    for (long long i = 0; i < n; i++) {
+        int err = 0;
+        vec_d o = mk_d(rays[i], rays[n + i], rays[2 * n + i]);
+        vec_d d = mk_d(rays[3 * n + i], rays[4 * n + i], rays[5 * n + i]);
+        double is[4];
+        int v = prim_d(is, &g, root, tmin, o, d, &err);
+        t[i] = v ? is[3] : 0.0;
+        err_all |= err;
+    }
+    return err_all;
+}
+
 /* ------------------------------------------------------------------ textures */
 typedef struct { float x, y, z, w; } f4;
 

@@ -64,6 +64,9 @@ def lib() -> C.CDLL:
         L.oracle_csg_scan_t64.restype = C.c_int
         L.oracle_csg_scan_t64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_longlong,
                                           C.c_void_p]
+        L.oracle_csg_scan_t64d.restype = C.c_int
+        L.oracle_csg_scan_t64d.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_longlong,
+                                           C.c_void_p]
         L.oracle_csg_action.restype = C.c_int
         L.oracle_csg_action.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
         L.oracle_tex2d_f1.restype = C.c_float
@@ -239,6 +242,42 @@ def csg_scan_t64(node, itra, root: int, rays: np.ndarray, tmin: float = 0.0, pla
     t = np.zeros((n,), np.float64)
     err = lib().oracle_csg_scan_t64(_p(node), _p(itra), _p(pl), root, tmin, _p(rays), n, _p(t))
     return t, err
+
+
+def csg_scan_t64d(node, itra, root: int, rays64: np.ndarray, tmin: float = 0.0, plan=None):
+    """FP64 distances of FP64 rays (SoA (6,n) float64) against one prim; 0 for a miss"""
+    node = np.ascontiguousarray(node, np.float32)
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    pl = _plan(plan)
+    rays64 = np.ascontiguousarray(rays64, np.float64)
+    n = rays64.shape[1]
+    t = np.zeros((n,), np.float64)
+    err = lib().oracle_csg_scan_t64d(_p(node), _p(itra), _p(pl), root, tmin, _p(rays64), n, _p(t))
+    return t, err
+
+
+def trace_t64(geom: dict, rays: np.ndarray, inst_idx: np.ndarray, prim_idx: np.ndarray, tmin: float = 0.0) -> np.ndarray:
+    """FP64 distance along each world ray (SoA (6,n) float32) to the given (instance, prim): the ray is
+    carried into the prim's frame in double (row-vector qat4 convention, identity words in the .w
+    column zeroed) and intersected with the FP64 CSG evaluator; 0 where it misses that prim"""
+    inst = geom["inst"].astype(np.float64)
+    prim = geom["prim"]
+    pi = prim.view(np.int32)
+    n = rays.shape[1]
+    t = np.zeros(n, np.float64)
+    o = np.c_[rays[:3].T.astype(np.float64), np.ones(n)]
+    d = np.c_[rays[3:].T.astype(np.float64), np.zeros(n)]
+    m = inst.copy()
+    m[:, :3, 3] = 0.0
+    m[:, 3, 3] = 1.0
+    inv = np.linalg.inv(m)[inst_idx]
+    lo = np.einsum("ni,nij->nj", o, inv)[:, :3]
+    ld = np.einsum("ni,nij->nj", d, inv)[:, :3]
+    for p in np.unique(prim_idx):
+        sel = np.nonzero(prim_idx == p)[0]
+        r64 = np.ascontiguousarray(np.concatenate([lo[sel].T, ld[sel].T]))
+        t[sel], _ = csg_scan_t64d(geom["node"], geom.get("itra"), int(pi[p, 0, 1]), r64, tmin, plan=geom.get("plan"))
+    return t
 
 
 def tex2d_f1(data: np.ndarray, x: float, y: float) -> float:
