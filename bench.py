@@ -54,15 +54,14 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # share are added per workload
 BYTES_PER_PHOTON_FIXED = 48 + 64 + 32
 SAMPLE_PER_GENSTEP = 200       # CPU sample: this many photons of every genstep of the event
-# DRAM bytes (read + write) of the wavefront kernels of one simulate call of the C3 event, from
-# an ncu capture of one call's launches (profiles/dram_wavefront_detector_2M.md)
-DRAM_TRAFFIC = {"bytes_per_call": 3.6032e9, "photons": 2_000_000,
-                "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the k_wave_* launches of one "
-                          "2M-photon call of the detector event (profiles/dram_wavefront_detector_2M.md), scaled by "
-                          "photons to this call"}
-# issue figures of the dominant kernel (k_wave_trace_df, 54 % of the step) from its ncu --set full
+# DRAM bytes (read + write) of all kernels of one simulate call of this 10M-photon event, from a
+# one-pass ncu capture of the bench's own launches (profiles/launches_dram_wavefront_detector_10M.md)
+DRAM_TRAFFIC = {"bytes_per_call": 20.157e9, "photons": 10_000_000,
+                "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 32 launches of one "
+                          "10M-photon simulate call of this workload (profiles/launches_dram_wavefront_detector_10M.md)"}
+# issue figures of the dominant kernel (k_wave_trace_df, 58 % of the step) from its ncu --set full
 # capture (profiles/k_wave_trace_df_detector_2M_ncu_full.md)
-ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.54, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
+ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.58, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
          "warps_active": 0.185, "lane_issue_frac": 0.376 * 11.90 / 32,
          "source": "profiles/k_wave_trace_df_detector_2M_ncu_full.md"}
 
