@@ -255,7 +255,7 @@ def test_c3_sample_matches_reference(c3_sample, pool):
     assert res["status"] == 0, E.status_names(res["status"])
     print(f"   pool {pool}: {stats['wave_rounds']} wavefront rounds, {stats['kernel_launches']} launches")
     if pool:
-        assert stats["wave_rounds"] > 2 * 31 // 3       # refilled: more rounds than one pass of the bounce limit
+        assert stats["wave_rounds"] >= N // pool         # refilled: at least one round per pool of photons
     ph, sq = c3_sample["ref"]
     same = _compare(f"C3 200k sample pool {pool}", res, ph, sq)
     # per-sensor hits: the engine's counts against the reference's photons
