@@ -495,6 +495,7 @@ def main():
     ap.add_argument("--per-genstep", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--forms", default="c1,cerenkov,batched,scan,adjoint", help="comma list of the forms to measure")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--kernel-mode", type=int, default=None, help="engine kernel_mode override (1 persistent, 2 wavefront)")
@@ -647,15 +648,17 @@ def main():
         c1_fd, c1_phys, c1_gs = c1_workload()
         ck_gs = cerenkov_workload(lib)
         if not args.no_forms and world == 1:
-            forms = {"c1": dict(measure_plain(torch, E, c1_fd, c1_phys, c1_gs, dev),
-                                workload="C1: 1,000,000 torch photons (T_SPHERE with random linear polarisation, 440 nm) "
-                                         "from the centre of a 1 m water sphere in a 3 m detecting box"),
-                     "cerenkov": dict(measure_plain(torch, E, fd, phys, ck_gs, dev, num_sensor=scenes.NUM_PMT),
-                                      workload=f"detector, {len(ck_gs)} Cerenkov tracks x 5,000 photons, beta 0.75-0.9999, "
-                                               "1-40 mm steps in the liquid scintillator"),
-                     "batched": measure_batched(torch, E, fd, lib, phys, dev, args.events, tune_cache=args.tune_cache),
-                     "scan": measure_scan(torch, E, dev),
-                     "adjoint": measure_adjoint(torch, E, fd, lib, phys, dev)}
+            runners = {
+                "c1": lambda: dict(measure_plain(torch, E, c1_fd, c1_phys, c1_gs, dev),
+                                   workload="C1: 1,000,000 torch photons (T_SPHERE with random linear polarisation, 440 nm) "
+                                            "from the centre of a 1 m water sphere in a 3 m detecting box"),
+                "cerenkov": lambda: dict(measure_plain(torch, E, fd, phys, ck_gs, dev, num_sensor=scenes.NUM_PMT),
+                                         workload=f"detector, {len(ck_gs)} Cerenkov tracks x 5,000 photons, beta 0.75-0.9999, "
+                                                  "1-40 mm steps in the liquid scintillator"),
+                "batched": lambda: measure_batched(torch, E, fd, lib, phys, dev, args.events, tune_cache=args.tune_cache),
+                "scan": lambda: measure_scan(torch, E, dev),
+                "adjoint": lambda: measure_adjoint(torch, E, fd, lib, phys, dev)}
+            forms = {k: runners[k]() for k in args.forms.split(",") if k}
         cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(
             fd, phys, gs, form_workloads=(("c1", (c1_fd, c1_phys, c1_gs, 200_000, 50)), ("cerenkov", (fd, phys, ck_gs, 500, 2))))
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

@@ -21,7 +21,8 @@ import os
 import numpy as np
 
 FOUNDRY_ARRAYS = ("solid", "prim", "node", "tran", "itra", "inst", "plan")
-FOUNDRY_SHAPES = {"solid": (3, 4), "prim": (4, 4), "node": (4, 4), "tran": (4, 4), "itra": (4, 4), "inst": (4, 4), "plan": (4,)}
+# CSGFoundry::save_ writes plan as (n,1,4) (CSG/CSGFoundry.cc:2769-2800); the engine takes (n,4)
+FOUNDRY_SHAPES = {"solid": (3, 4), "prim": (4, 4), "node": (4, 4), "tran": (4, 4), "itra": (4, 4), "inst": (4, 4), "plan": (1, 4)}
 FOUNDRY_DTYPES = {"solid": np.int32}
 STANDARD_DIR = os.path.join("SSim", "stree", "standard")
 
@@ -62,6 +63,8 @@ def write_meta(npy_path: str, meta: dict) -> None:
 
 def _check(name: str, a: np.ndarray) -> np.ndarray:
     tail = FOUNDRY_SHAPES[name]
+    if name == "plan" and a.ndim == 2 and a.shape[1:] == (4,):
+        a = a.reshape(-1, 1, 4)
     if a.ndim != 1 + len(tail) or tuple(a.shape[1:]) != tail:
         raise ValueError(f"{name}.npy has shape {a.shape}, expected (n,{','.join(map(str, tail))})")
     want = FOUNDRY_DTYPES.get(name)
@@ -83,6 +86,8 @@ def load_foundry(fold: str) -> dict:
         p = os.path.join(fold, f"{k}.npy")
         if os.path.exists(p):
             out[k] = _check(k, np.load(p))
+            if k == "plan":
+                out[k] = out[k].reshape(-1, 4)
         elif k != "plan":
             raise FileNotFoundError(f"{p} missing")
     out.setdefault("plan", np.zeros((0, 4), dtype=np.float32))
@@ -114,14 +119,21 @@ def load_standard(fold: str, hd_factor: int = 20) -> dict:
     """bnd/optical/icdf of SSim/stree/standard as the physics dict of engine.Engine"""
     bnd_path = os.path.join(fold, "bnd.npy")
     bnd = np.load(bnd_path)
-    if bnd.ndim != 5 or bnd.shape[1:3] != (4, 2) or bnd.shape[4] != 4 or bnd.dtype != np.float32:
-        raise ValueError(f"bnd.npy has shape {bnd.shape} {bnd.dtype}, expected float32 (num_bnd,4,2,num_wl,4)")
+    if bnd.ndim != 5 or bnd.shape[1:3] != (4, 2) or bnd.shape[4] != 4 or bnd.dtype not in (np.float32, np.float64):
+        raise ValueError(f"bnd.npy has shape {bnd.shape} {bnd.dtype}, expected float64/32 (num_bnd,4,2,num_wl,4)")
+    # sstandard writes double; QBnd narrows a wide array before the texture upload
+    # (qudarap/QBnd.cc:75-82, NP::MakeNarrowIfWide)
+    bnd = bnd.astype(np.float32)
     meta = read_meta(bnd_path)
     if "domain_low" not in meta or "domain_step" not in meta:
         raise ValueError("bnd_meta.txt must give domain_low and domain_step (the texture needs its domain)")
     optical = np.load(os.path.join(fold, "optical.npy"))
-    if optical.shape != (bnd.shape[0] * 4, 4) or optical.dtype.itemsize != 4:
-        raise ValueError(f"optical.npy has shape {optical.shape}, expected ({bnd.shape[0] * 4},4) 32-bit")
+    # sstandard::make_optical writes int32 (num_bnd,4,4) (sysrap/sstandard.h:311-330); one row per
+    # texture line, as (num_bnd*4,4) here
+    if optical.shape in ((bnd.shape[0], 4, 4), (bnd.shape[0] * 4, 4)) and optical.dtype.itemsize == 4:
+        optical = optical.reshape(bnd.shape[0] * 4, 4)
+    else:
+        raise ValueError(f"optical.npy has shape {optical.shape}, expected ({bnd.shape[0]},4,4) 32-bit")
     phys = {"bnd": np.ascontiguousarray(bnd), "optical": np.ascontiguousarray(optical).view(np.uint32),
             "wl_low": float(meta["domain_low"]), "wl_step": float(meta["domain_step"]), "hd_factor": int(hd_factor),
             "bnd_names": _read_names(os.path.join(fold, "bnd_names.txt"))}
@@ -138,15 +150,19 @@ def load_standard(fold: str, hd_factor: int = 20) -> dict:
 
 def save_standard(fold: str, phys: dict, bnd_names=None) -> None:
     os.makedirs(fold, exist_ok=True)
-    bnd = np.ascontiguousarray(phys["bnd"], np.float32)
+    # the reference's dtypes and shapes: bnd double with its domain metadata, optical int32
+    # (num_bnd,4,4), icdf double (sysrap/sstandard.h:311-330, 495-506)
+    bnd = np.ascontiguousarray(phys["bnd"], np.float64)
     p = os.path.join(fold, "bnd.npy")
     np.save(p, bnd)
     lo, step = float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0))
-    write_meta(p, {"domain_low": lo, "domain_high": lo + step * (bnd.shape[3] - 1), "domain_step": step})
-    np.save(os.path.join(fold, "optical.npy"), np.ascontiguousarray(phys["optical"], np.uint32))
+    hi = lo + step * (bnd.shape[3] - 1)
+    write_meta(p, {"domain_low": f"{lo:g}", "domain_high": f"{hi:g}", "domain_step": f"{step:g}", "domain_range": f"{hi - lo:g}"})
+    opt = np.ascontiguousarray(phys["optical"], np.uint32).view(np.int32)
+    np.save(os.path.join(fold, "optical.npy"), opt.reshape(bnd.shape[0], 4, 4))
     icdf = phys.get("icdf")
     if icdf is not None:
-        icdf = np.ascontiguousarray(icdf, np.float32)
+        icdf = np.ascontiguousarray(icdf, np.float64)
         np.save(os.path.join(fold, "icdf.npy"), icdf.reshape(icdf.shape[0], icdf.shape[1], 1))
     _write_names(os.path.join(fold, "bnd_names.txt"), bnd_names or phys.get("bnd_names") or [])
 

@@ -28,7 +28,7 @@ REF_SPM = os.path.join(HERE, "_ref", "libref_spm.so")
 def build(ref: bool = False) -> None:
     """make liboracle.so (and the reference builds when the reference checkout is present)"""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(os.environ.get("REF", "/root/reference")):
+    if ref and subprocess.run(["make", "-s", "-C", HERE, "ref-present"]).returncode == 0:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
