@@ -226,8 +226,12 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
     for mode in (1, 2):
         eng = E.Engine(fd.arrays(), phys, E.default_config(max_photon=int(counts.max()), num_sensor=scenes.NUM_PMT,
                                                            kernel_mode=mode), device=dev.index)
-        best = autotune.tune_batched(eng, gs, ev, torch, cache=tune_cache) if mode == 1 else None
-        kw = {k: best[k] for k in ("block", "regroup", "chunk")} if best else {}
+        if mode == 1:
+            best = autotune.tune_batched(eng, gs, ev, torch, cache=tune_cache)
+            kw = {k: best[k] for k in ("block", "regroup", "chunk")}
+        else:
+            best = autotune.tune_wavefront(eng, gs, ev, torch, cache=tune_cache, seq=seq)   # left set on the engine
+            kw = {}
 
         def batch():
             return eng.simulate_batched_device(g, e, N, photon=photon, seq=seq, hit=hit, hit_capacity=N, num_event=num_event,
@@ -236,6 +240,7 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
         torch.cuda.synchronize()
         e0.record(st)
         nh_b, st_b = batch()
+        graph_b = eng.last_call_stats()["graph"]
         e1.record(st)
         torch.cuda.synchronize()
         ms_b = e0.elapsed_time(e1)
@@ -259,6 +264,21 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
         ms_l = e0.elapsed_time(e1)
         per = np.array(per) * 1e3
         lat_l = np.cumsum(per)
+        bounded = None
+        if mode == 2:
+            # events finishing before the end of the call: a pool of 2^24 paths refilled from the
+            # queue (host-read schedule), per-event completion times from the device clock
+            eng.set_launch_config(wave_pool=1 << 24, wave_rounds=0)
+            batch()
+            torch.cuda.synchronize()
+            e0.record(st)
+            batch()
+            e1.record(st)
+            torch.cuda.synchronize()
+            d = done.cpu().numpy()
+            lat_p = (d[:num_event] - d[num_event]) / 1e6
+            bounded = {"wave_pool": 1 << 24, "batched_ms": e0.elapsed_time(e1),
+                       "event_done_ms_p50_p99": [float(np.percentile(lat_p, 50)), float(np.percentile(lat_p, 99))]}
         eng.close()
         forms["persistent" if mode == 1 else "wavefront"] = {
             "batched_photons_per_s": N / (ms_b / 1e3), "batched_ms": ms_b,
@@ -266,9 +286,9 @@ def measure_batched(torch, E, fd, lib, phys, dev, num_event=4096, tune_cache=Non
             "batched_event_done_ms_p50_p99": [float(np.percentile(lat_b, 50)), float(np.percentile(lat_b, 99))],
             "loop_event_ms_p50_p99": [float(np.percentile(per, 50)), float(np.percentile(per, 99))],
             "loop_event_done_ms_p50_p99": [float(np.percentile(lat_l, 50)), float(np.percentile(lat_l, 99))],
-            "cuda_graph": mode == 1, "hits": nh_b, "status": st_b,
-            **({"autotuned": {k: best[k] for k in ("block", "regroup", "chunk", "photons_per_s", "sample_photons")}}
-               if best else {})}
+            "cuda_graph": graph_b, "hits": nh_b, "status": st_b,
+            "autotuned": {k: best[k] for k in best if k != "table"},
+            **({"bounded_pool": bounded} if bounded else {})}
     bb = min(forms, key=lambda k: forms[k]["batched_ms"])
     bl = min(forms, key=lambda k: forms[k]["loop_ms"])
     return {"workload": f"{num_event} events, one scintillation genstep each, lognormal(median 50k, sigma_ln 1) "
@@ -364,8 +384,8 @@ def cerenkov_workload(lib, num_track=200, per_track=5000, seed=21):
     return np.stack(gs)
 
 
-def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=10000, fd_events=4, precise_events=96,
-                    rel_step=1e-3, precise_step=1e-2):
+def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=10000, fd_events=4, precise_events=256,
+                    rel_step=1e-3, precise_step=1e-3):
     """C5: adjoint pass cost vs the plain forward, and agreement with central finite differences under
     common random numbers (per-parameter means and standard errors over independent events)"""
     from opticks_b200 import adjoint as ADJ
@@ -436,24 +456,24 @@ def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=1
         return rows
 
     def summary(rows):
-        cmp = [r for r in rows if r["fd"] is not None and r["kind"] != "rindex" and r.get("z") is not None]
+        cmp = [r for r in rows if r["fd"] is not None and r.get("z") is not None]
         return {"compared": len(cmp),
                 "within_2pct": sum(1 for r in cmp if r["rel_diff"] is not None and abs(r["rel_diff"]) <= 0.02),
                 "within_3se": sum(1 for r in cmp if abs(r["z"]) <= 3.0)}
 
     all_rows = fd_table(range(32), fd_events, 11, rel_step)
-    # the bins holding most of the scintillation spectrum, with a 10x step: the CRN difference of
-    # integer hit counts has noise ~ 1/sqrt(step), its bias (curvature) stays far below the noise
-    dominant = [2, 3, 4, 10, 11]
+    # the bins holding most of the scintillation spectrum (absorption, Rayleigh, refractive index)
+    dominant = [2, 3, 4, 10, 11, 26, 27, 28]
     precise = fd_table(dominant, precise_events, 1000, precise_step)
     eng.close()
     return {"workload": f"{N} photons from {num_genstep} scintillation gensteps, theta = 4 properties x 8 bins of LS over 300-620 nm",
             "adjoint_ms": ms_adj, "forward_ms_with_outputs": ms_fwd, "forward_ms_no_outputs": ms_fwd_bare,
             "adjoint_over_forward": ms_adj / ms_fwd, "adjoint_over_forward_no_outputs": ms_adj / ms_fwd_bare,
             "fd": {"common_random_numbers": True,
-                   "note": "rindex rows hold the score (Fresnel) part only: the pathwise refraction term is not "
-                           "included, so they are reported but not compared; z is omitted where the CRN "
-                           "difference moved no photon in any event",
+                   "note": "rindex rows include the pathwise refraction term (tangent of the refracted direction "
+                           "carried through later segments, Fresnel probabilities and Rayleigh densities; terms "
+                           "clipped at 1e4, tangents at 100 per unit n); z is omitted where the CRN difference "
+                           "moved no photon in any event",
                    "all_params": {"events": fd_events, "rel_step": rel_step, "summary": summary(all_rows), "rows": all_rows},
                    "dominant_bins": {"events": precise_events, "rel_step": precise_step, "summary": summary(precise),
                                      "rows": precise}}}

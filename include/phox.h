@@ -80,7 +80,18 @@ typedef struct {
                                          more photons refills freed slots from its queue.  0 = every
                                          photon of the call in flight while that fits in half of the
                                          free device memory, at least 2^26 slots; the engine keeps its
-                                         slots until phx_destroy */
+                                         slots until phx_destroy (or phx_trim) */
+    int32_t  wave_refill;             /* wavefront closest-hit kernel: idle lanes a warp waits for before
+                                         it takes new rays (1..32; 12) */
+    int32_t  wave_rounds;             /* wavefront loop of batched calls (phx_simulate_batched_device;
+                                         single-event calls always read the count): 0 = the host reads the live
+                                         count every few rounds and starts the tail kernel below
+                                         wave_tail paths; n > 0 = a fixed schedule of n rounds and then
+                                         the tail kernel for whatever is left, with no host read, so the
+                                         call is captured as a CUDA graph (use_graph) when every photon
+                                         of it is in flight at once (0) */
+    int64_t  wave_tail;               /* live paths at or below which the tail kernel finishes them
+                                         (host-read schedule; 262144) */
 } phx_config;
 
 typedef struct {
@@ -110,6 +121,13 @@ int phx_destroy(phx_engine* e);
  * that shares the GPU after a large call; the next call allocates what it needs again.  Waits for
  * all work on the device first.  *bytes_released (optional) receives the bytes freed. */
 int phx_trim(phx_engine* e, int64_t* bytes_released);
+
+/* Change the launch shape of later calls (no reference counterpart): kernel_mode, block, regroup,
+ * chunk, use_graph, wave_pool, wave_refill, wave_rounds and wave_tail are taken from *cfg (a smaller
+ * wave_pool takes effect when the engine's pool is next released or grown), every other field is
+ * ignored.  None of them changes results (every loop form gives the same photons, seq and hits);
+ * they are the knobs the autotuner sets. */
+int phx_set_launch_config(phx_engine* e, const phx_config* cfg);
 
 /* sum of quad6 q0.w photon counts */
 int64_t phx_count_photons(const float* gensteps, int32_t num_genstep);
@@ -186,12 +204,18 @@ int phx_rng_sequence(phx_engine* e, int32_t event_index, int64_t photon_offset, 
  * that material is re-tabulated with theta for this call (the engine's own tables stay unchanged; the
  * group velocity in the bins is c/n).  One forward pass over the device gensteps accumulates
  * d_hits[s] = hits on sensor s and d_grad[s*32+k] = sum over those hits of d log p(path)/d theta_k
- * (absorption/scattering/sail densities, reemission and Fresnel branch probabilities; the change of
- * the refracted direction with n is not included).  d_hits, d_grad: device doubles, (num_sensor)
- * and (num_sensor*32); the engine must have config num_sensor > 0. */
+ * (absorption/scattering/sail densities, reemission and Fresnel branch probabilities).  With flags
+ * PHX_ADJ_PATHWISE the refractive-index rows also carry the pathwise part: the refracted direction's
+ * change with n, carried forward as a tangent of position, direction and polarisation into every
+ * later segment length, incidence angle, Fresnel probability and Rayleigh density (the surface
+ * curvature from a probe intersection of the hit prim); not carried: a tangent through a
+ * reemission or a diffuse reflection (both redraw the direction), and hits that move across a
+ * sensor's edge (the visibility boundary term).  d_hits, d_grad: device doubles, (num_sensor) and
+ * (num_sensor*32); the engine must have config num_sensor > 0. */
+#define PHX_ADJ_PATHWISE 0x1
 int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                        int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
-                       double* d_hits, double* d_grad, void* stream);
+                       double* d_hits, double* d_grad, int32_t flags, void* stream);
 
 /* Hit merging: SPM::merge_partial_select (sysrap/SPM.cu:110-200, called per launch from
  * QEvt::PerLaunchMerge qudarap/QEvt.cc:1172 and on concatenated results from QEvt::FinalMerge).
@@ -228,8 +252,9 @@ int phx_planck_icdf(float* out, int n);
 
 /* Diagnostics of the last phx_simulate / phx_simulate_device call on this engine (no reference
  * counterpart): kernels it launched and, in kernel_mode 2, wavefront rounds (one closest-hit and
- * one physics launch each). */
-int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds);
+ * one physics launch each) and, for phx_simulate_batched_device, whether it replayed a captured
+ * CUDA graph (*graph 1). */
+int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds, int32_t* graph);
 
 #ifdef __cplusplus
 }

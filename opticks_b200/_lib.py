@@ -42,6 +42,7 @@ class PhxConfig(C.Structure):
         ("root_polish", C.c_int32), ("num_sensor", C.c_int32),
         ("kernel_mode", C.c_int32), ("block", C.c_int32), ("regroup", C.c_int32), ("chunk", C.c_int32),
         ("use_graph", C.c_int32), ("wave_pool", C.c_int64),
+        ("wave_refill", C.c_int32), ("wave_rounds", C.c_int32), ("wave_tail", C.c_int64),
     ]
 
 
@@ -61,6 +62,7 @@ SIGNATURES = {
     "phx_create": (C.c_int, [C.POINTER(PhxGeometry), C.POINTER(PhxPhysics), C.POINTER(PhxConfig), C.c_int, C.POINTER(C.c_void_p)]),
     "phx_destroy": (C.c_int, [C.c_void_p]),
     "phx_trim": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "phx_set_launch_config": (C.c_int, [C.c_void_p, C.POINTER(PhxConfig)]),
     "phx_count_photons": (C.c_int64, [C.c_void_p, C.c_int32]),
     "phx_simulate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(PhxOutputs)]),
     "phx_simulate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_int64, C.POINTER(PhxOutputs),
@@ -76,12 +78,12 @@ SIGNATURES = {
                                    C.c_void_p]),
     "phx_rng_sequence": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_void_p]),
     "phx_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_int32,
-                                     C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+                                     C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "phx_merge_hits_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint32, C.c_float, C.c_void_p,
                                         C.c_int64, C.POINTER(C.c_int64), C.c_void_p]),
     "phx_merge_hits": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_uint32, C.c_float, C.c_void_p, C.c_int64,
                                  C.POINTER(C.c_int64)]),
-    "phx_last_call_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "phx_last_call_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "phx_set_input_photon": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "phx_planck_icdf": (C.c_int, [C.c_void_p, C.c_int]),
     "phx_set_input_photon_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),

@@ -63,14 +63,19 @@ def retabulate(phys: dict, theta, mat_line: int, wl_lo: float = 300.0, wl_hi: fl
     return out
 
 
+PATHWISE = 0x1   # phx_adjoint_device flag: the refracted direction's change with n, carried as a tangent
+
+
 def adjoint_device(engine, gs_dev, num_photon: int, event: int, theta, mat_line: int, wl_lo: float, wl_hi: float,
-                   hits_dev, grad_dev, stream: int = 0) -> None:
+                   hits_dev, grad_dev, stream: int = 0, pathwise: bool = True) -> None:
+    """one adjoint pass: hits per sensor and their score sums (see phx_adjoint_device); pathwise
+    False gives the score terms alone (the rindex rows then hold the Fresnel score only)"""
     th = np.ascontiguousarray(np.asarray(theta, dtype=np.float32).reshape(32))
     G = gs_dev.numel() // 24
     _lib.check(_lib.lib().phx_adjoint_device(engine._h, C.c_void_p(gs_dev.data_ptr()), int(G), int(num_photon), int(event),
                                              th.ctypes.data_as(C.c_void_p), int(mat_line), float(wl_lo), float(wl_hi),
                                              C.c_void_p(hits_dev.data_ptr()), C.c_void_p(grad_dev.data_ptr()),
-                                             C.c_void_p(stream) if stream else None),
+                                             PATHWISE if pathwise else 0, C.c_void_p(stream) if stream else None),
                "phx_adjoint_device")
 
 

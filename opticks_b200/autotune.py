@@ -1,5 +1,8 @@
-"""Autotuner for the persistent photon kernel: block size, refill interval ("regroup") and queue
-chunk, chosen by timing the batched launch on a sample of the caller's own workload.
+"""Autotuners for the batched photon launch, chosen by timing it on a sample of the caller's own
+workload.  ``tune_batched``: the persistent kernel's block size, refill interval ("regroup") and
+queue chunk.  ``tune_wavefront``: the wavefront loop's refill threshold of the closest-hit kernel
+(idle lanes before a warp takes new rays) and its schedule: host-read rounds with a tail threshold,
+or a fixed number of rounds followed by the tail kernel, captured and replayed as a CUDA graph.
 
 The search is a small grid (the kernel is compiled for blocks of 32/64/128/256); each candidate
 is timed with CUDA events over a few repetitions after a warm-up, and the fastest is returned.
@@ -67,6 +70,77 @@ def tune_batched(engine, gs: np.ndarray, ev: np.ndarray, torch, reps: int = 2, s
                 if best is None or rate > best["photons_per_s"]:
                     best = {"block": b, "regroup": r, "chunk": c, "photons_per_s": rate}
     best = dict(best, sample_photons=N, table=rows)
+    if cache:
+        try:
+            table = {}
+            if os.path.exists(cache):
+                with open(cache) as f:
+                    table = json.load(f)
+            table[key] = best
+            os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+            with open(cache, "w") as f:
+                json.dump(table, f, indent=1)
+        except Exception:
+            pass
+    return best
+
+
+WAVE_REFILLS = (12,)
+WAVE_TAILS = (1 << 18,)                          # host-read schedule
+WAVE_ROUNDS = (12, 14, 16, 18, 20, 24)           # fixed schedule, graph-captured
+
+
+def tune_wavefront(engine, gs: np.ndarray, ev: np.ndarray, torch, reps: int = 1, sample_photons: int | None = None,
+                   cache: str | None = None, refills=WAVE_REFILLS, tails=WAVE_TAILS, rounds=WAVE_ROUNDS, seq=None) -> dict:
+    """Time the batched wavefront call for each refill threshold and schedule on the first events of
+    (gs, ev) holding about `sample_photons` photons, leave the fastest set on the engine and return
+    {"wave_refill", "wave_rounds", "wave_tail", "use_graph", "photons_per_s", "sample_photons", "table"}."""
+    counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
+    # the live count after n rounds is a fraction of the call, so the schedule is timed on the whole
+    # call unless a sample is asked for
+    keep = len(gs) if sample_photons is None else max(1, int(np.searchsorted(np.cumsum(counts), sample_photons)) + 1)
+    gs_s, ev_s = gs[:keep], ev[:keep]
+    key = f"wave|{torch.cuda.get_device_name()}|{_signature(gs_s, ev_s)}"
+    fields = ("wave_refill", "wave_rounds", "wave_tail", "use_graph")
+    if cache and os.path.exists(cache):
+        try:
+            with open(cache) as f:
+                table = json.load(f)
+            if key in table:
+                engine.set_launch_config(kernel_mode=2, **{k: table[key][k] for k in fields})
+                return table[key]
+        except Exception:
+            pass
+    dev = torch.device("cuda", engine.device)
+    N = int(counts[:keep].sum())
+    g = torch.from_numpy(np.ascontiguousarray(gs_s)).to(dev)
+    e = torch.from_numpy(np.ascontiguousarray(ev_s, dtype=np.int32)).to(dev)
+    if seq is None or seq.shape[0] < N:          # the caller's seq buffer may be reused
+        seq = torch.empty((N, 2, 2), dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    cands = [dict(wave_refill=r, wave_rounds=0, wave_tail=t, use_graph=0) for r in refills for t in tails]
+    cands += [dict(wave_refill=r, wave_rounds=n, wave_tail=1 << 18, use_graph=1) for r in refills for n in rounds]
+    rows, best = [], None
+    for c in cands:
+        engine.set_launch_config(kernel_mode=2, **c)
+
+        def run():
+            engine.simulate_batched_device(g, e, N, seq=seq, stream=stream.cuda_stream)
+        run()                     # warm-up (and graph capture)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(reps):
+            run()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        rows.append(dict(c, ms=ms, photons_per_s=N / (ms / 1e3)))
+        if best is None or rows[-1]["photons_per_s"] > best["photons_per_s"]:
+            best = rows[-1]
+    best = dict(best, sample_photons=N, table=rows)
+    engine.set_launch_config(kernel_mode=2, **{k: best[k] for k in fields})
     if cache:
         try:
             table = {}

@@ -123,6 +123,7 @@ struct phx_engine {
     DevBuf<float4> gs;
     DevBuf<long long> gs_off;
     DevBuf<int> gs_event;
+    DevBuf<int> prim_node_d;              // root node of each prim
     DevBuf<phx_photon> photon;
     DevBuf<phx_seq> seq;
     DevBuf<phx_photon> hit;
@@ -135,7 +136,9 @@ struct phx_engine {
     DevBuf<uint32_t> ev_rng;               // per-call event-advanced XORWOW states (k_rng_event)
     cudaGraphExec_t batch_exec = nullptr;   // cached batched launch sequence (use_graph)
     PhxBatchCall batch_call;
-    const void* batch_bufs[13] = {};
+#define PHX_BATCH_BUFS 20
+    const void* batch_bufs[PHX_BATCH_BUFS] = {};
+    unsigned long long batch_launch = 0;     // launch_key of the captured graph
     DevBuf<unsigned> status;
     unsigned* h_pinned = nullptr;  // 16 words of pinned readback
     PhxMergeWs merge;
@@ -149,6 +152,7 @@ struct phx_engine {
     DevBuf<float4> wscore;                          // adjoint score terms per slot
     DevBuf<unsigned> wcnt;
     long long last_launches = 0, last_rounds = 0;   // of the last plain simulate call
+    int last_graph = 0;                             // the last batched call replayed a CUDA graph
 };
 
 static PhxScene scene_of(const phx_engine* e, int polish)
@@ -792,6 +796,28 @@ void phx_config_default(phx_config* c)
     c->chunk = 1;
     c->use_graph = 1;
     c->wave_pool = 0;
+    c->wave_refill = 12;
+    c->wave_rounds = 0;
+    c->wave_tail = 1 << 18;
+}
+
+// the launch-shape fields a captured batched graph depends on, packed into one word
+static unsigned long long launch_key(const phx_engine* e)
+{
+    const phx_config& c = e->cfg;
+    return (unsigned long long)(c.kernel_mode & 3) | ((unsigned long long)(c.wave_refill & 63) << 2) |
+           ((unsigned long long)(c.wave_rounds & 0x1fff) << 8) | ((unsigned long long)(c.wave_tail & 0xffffffffll) << 21) |
+           ((unsigned long long)(c.use_graph & 1) << 53);
+}
+
+// the launch-shape fields of a config, checked (they change no result, only how work is launched)
+static int check_launch_config(const phx_config* c)
+{
+    if (c->kernel_mode < 0 || c->kernel_mode > 2) return phx_fail(-1, "kernel_mode %d not in 0..2", c->kernel_mode);
+    if (c->wave_refill < 1 || c->wave_refill > 32) return phx_fail(-1, "wave_refill %d not in 1..32", c->wave_refill);
+    if (c->wave_rounds < 0 || c->wave_rounds > 4096) return phx_fail(-1, "wave_rounds %d not in 0..4096", c->wave_rounds);
+    if (c->wave_tail < 0) return phx_fail(-1, "wave_tail %lld is negative", (long long)c->wave_tail);
+    return 0;
 }
 
 int64_t phx_count_photons(const float* gensteps, int32_t num_genstep)
@@ -817,7 +843,7 @@ int phx_destroy(phx_engine* e)
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
     if (e->planck_tex) cudaDestroyTextureObject(e->planck_tex);
     if (e->planck_arr) cudaFreeArray(e->planck_arr);
-    e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release();
+    e->node.release(); e->itra.release(); e->plan.release(); e->inst_inv.release(); e->prim_node_d.release();
     e->bvh.release(); e->leaves.release(); e->globals.release(); e->leaf_sph.release(); e->global_sph.release(); e->optical.release(); e->rng.release();
     e->gs.release(); e->gs_off.release(); e->gs_event.release(); e->photon.release(); e->seq.release();
     e->hit.release(); e->hitword.release(); e->wordoff.release(); e->blocksum.release(); e->sensor.release();
@@ -830,6 +856,23 @@ int phx_destroy(phx_engine* e)
     if (e->h_pinned) cudaFreeHost(e->h_pinned);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
+    return 0;
+}
+
+int phx_set_launch_config(phx_engine* e, const phx_config* cfg)
+{
+    if (!e || !cfg) return phx_fail(-1, "phx_set_launch_config: null argument");
+    int rc = check_launch_config(cfg);
+    if (rc) return rc;
+    e->cfg.kernel_mode = cfg->kernel_mode;
+    e->cfg.block = cfg->block;
+    e->cfg.regroup = cfg->regroup;
+    e->cfg.chunk = cfg->chunk;
+    e->cfg.use_graph = cfg->use_graph;
+    e->cfg.wave_refill = cfg->wave_refill;
+    e->cfg.wave_rounds = cfg->wave_rounds;
+    e->cfg.wave_tail = cfg->wave_tail;
+    e->cfg.wave_pool = cfg->wave_pool;
     return 0;
 }
 
@@ -860,7 +903,8 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
     phx_engine* e = new phx_engine();
     e->device = device;
     if (cfg_in) e->cfg = *cfg_in; else phx_config_default(&e->cfg);
-    int rc = 0;
+    int rc = check_launch_config(&e->cfg);
+    if (rc) { delete e; return rc; }
 #define PHX_TRY(x) do { rc = (x); if (rc) { phx_destroy(e); return rc; } } while (0)
 #define PHX_TRYCU(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) { rc = phx_fail(-2, "%s failed: %s", #call, cudaGetErrorString(_e)); phx_destroy(e); return rc; } } while (0)
     PHX_TRYCU(cudaSetDevice(device));
@@ -891,6 +935,10 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
         memcpy(&nn, geo->prim + 16 * p + 0, 4);
         if (no < 0 || no + std::max(nn, 1) > geo->num_node) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d node range out of bounds", p); }
         if (const char* m = check_prim_nodes(geo, no)) { phx_destroy(e); return phx_fail(-1, "phx_create: prim %d: %s", p, m); }
+    }
+    if (geo->num_prim > 0) {   // root node per prim on the device (the adjoint's probe intersections)
+        PHX_TRYCU(e->prim_node_d.ensure((size_t)geo->num_prim));
+        PHX_TRYCU(cudaMemcpy(e->prim_node_d.p, e->prim_node_offset.data(), sizeof(int) * (size_t)geo->num_prim, cudaMemcpyHostToDevice));
     }
     for (int i = 0; i < geo->num_node && !e->has_full; i++) {
         uint32_t tc;
@@ -1097,14 +1145,14 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 #define PHX_WAVE_POOL_MAX (1LL << 31)   // slot indexes are 32-bit
 #define PHX_WAVE_SLOT_BYTES (sizeof(PhxWaveSlot) + sizeof(PhxWavePrd) + sizeof(long long) + 3 * sizeof(uint32_t))
 
-// path slots of a wavefront call over N photons (adj: with the 32 score terms per slot)
+// path slots of a wavefront call over N photons (adj: with the score terms and tangent per slot)
 static long long wave_pool_for(const phx_engine* e, long long N, bool adj)
 {
     long long pool = e->cfg.wave_pool > 0 ? (long long)e->cfg.wave_pool : (long long)PHX_WAVE_POOL;
     if (e->cfg.wave_pool <= 0 && N > pool) {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-            const size_t per = PHX_WAVE_SLOT_BYTES + (adj ? 8 * sizeof(float4) : 0);
+            const size_t per = PHX_WAVE_SLOT_BYTES + (adj ? PHX_WAVE_SCORE_F4 * sizeof(float4) : 0);
             const long long fit = (long long)e->wslot.n + (long long)(free_b / 2 / per);
             pool = std::max(pool, std::min(N, fit));
         }
@@ -1129,9 +1177,9 @@ static int wave_grid(K kernel, int dev, int* cache)
 }
 
 template <int CV, bool ADJ = false>
-static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
+static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st, bool batched)
 {
-    static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {};
+    static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {}, g_tail[128] = {};
     const int dev = e->device;
     if (dev < 0 || dev >= 128) return phx_fail(-1, "device ordinal %d out of range", dev);
     int rc;
@@ -1143,13 +1191,14 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 #endif
     if ((rc = wave_grid(k_wave_shade<CV, ADJ>, dev, g_shade))) return rc;
     if ((rc = wave_grid(k_wave_fill<CV, ADJ>, dev, g_fill))) return rc;
+    if ((rc = wave_grid(k_wave_tail<CV, ADJ>, dev, g_tail))) return rc;
     const long long N = A.N;
     const long long pool = wave_pool_for(e, N, ADJ);
     PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
     PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
     const bool refill = N > pool;
     PHX_CU(e->wfree.ensure((size_t)pool));
-    if (ADJ) PHX_CU(e->wscore.ensure((size_t)pool * 8));
+    if (ADJ) PHX_CU(e->wscore.ensure((size_t)pool * PHX_WAVE_SCORE_F4));
     const long long nlw = (pool + 31) / 32, nlb = (nlw + 255) / 256;     // live-bit words, scan blocks
     if (refill) {
         PHX_CU(e->wlive.ensure((size_t)nlw)); PHX_CU(e->wlive_off.ensure((size_t)nlw));
@@ -1168,14 +1217,37 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     W.trace_ctr = e->wcnt.p + 3;
     W.act_in = nullptr; W.n_in = nullptr; W.act_out = act[0]; W.n_out = cnt[0];
     W.live_bits = nullptr;
+    W.refill_idle = e->cfg.wave_refill;
     const unsigned gi = (unsigned)std::min<long long>(g_init[dev], (pool + 127) / 128);
     k_wave_init<CV, ADJ><<<gi, 128, 0, st>>>(W);
     W.live_bits = refill ? e->wlive.p : nullptr;
     PHX_CU(cudaGetLastError());
+    int cur = 0;
+    if (batched && e->cfg.wave_rounds > 0 && !refill) {
+        // fixed schedule, no host read: wave_rounds rounds, then the tail kernel finishes whatever is
+        // still live (it reads the count on the device; a grid-stride loop over any count), so the
+        // whole call can be captured as a CUDA graph
+        for (int r = 0; r < e->cfg.wave_rounds; r++) {
+            W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
+#if PHX_WAVE_TRACE_DF
+            k_wave_trace_df<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+#else
+            k_wave_trace<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
+#endif
+            k_wave_shade<CV, ADJ><<<(unsigned)g_shade[dev], 128, 0, st>>>(W);
+            cur = 1 - cur;
+        }
+        W.act_in = act[cur]; W.n_in = cnt[cur];
+        k_wave_tail<CV, ADJ><<<(unsigned)g_tail[dev], 128, 0, st>>>(W);
+        PHX_CU(cudaGetLastError());
+        e->last_rounds = e->cfg.wave_rounds;
+        e->last_tail = 1;
+        e->last_wave_launches = 2 + 2LL * e->cfg.wave_rounds;
+        return 0;
+    }
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;
     e->last_rounds = 0;
     e->last_tail = 0;
-    int cur = 0;
     bool done = false;
     bool filling = refill;                          // photons still wait in the queue (as last read)
     long long nl = 1;                               // launches of this call (k_wave_init)
@@ -1217,7 +1289,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
             filling = false;
             W.live_bits = nullptr;
         }
-        if (!done && queue_done && live <= (unsigned)PHX_WAVE_TAIL) {
+        if (!done && queue_done && (long long)live <= e->cfg.wave_tail) {
             // few paths left and none queued: finish them in one kernel
             W.act_in = act[cur]; W.n_in = cnt[cur];
             k_wave_tail<CV, ADJ><<<(unsigned)((live + 127) / 128), 128, 0, st>>>(W);
@@ -1233,14 +1305,14 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 }
 
 template <bool ADJ = false>
-static int launch_wave_cv(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st)
+static int launch_wave_cv(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st, bool batched = false)
 {
-    PHX_CV_RETURN(cv, (launch_wave_t<CVK, ADJ>(e, A, st)));
+    PHX_CV_RETURN(cv, (launch_wave_t<CVK, ADJ>(e, A, st, batched)));
 }
 
-static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st)
+static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st, bool batched = false)
 {
-    return launch_wave_cv(e, A, cv_of(e, e->cfg.root_polish != 0), st);
+    return launch_wave_cv(e, A, cv_of(e, e->cfg.root_polish != 0), st, batched);
 }
 
 template <int CV>
@@ -1615,7 +1687,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
         A.ev_rng_n = N;
     }
     if (N > 0) {
-        int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st) : launch_persistent(e, A, c.block, st);
+        int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st, true) : launch_persistent(e, A, c.block, st);
         if (rc) return rc;
     }
     if (want_hits && N > 0) {
@@ -1670,11 +1742,22 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
     if (N > 0 && N <= PHX_EV_RNG_MAX) PHX_CU(e->ev_rng.ensure((size_t)N * 6));
     PHX_CU(e->jump_tab.ensure((size_t)std::max(1, c.G) * PHX_JUMP_MATW));
     PHX_CU(e->jump4.ensure((size_t)std::max(1, c.G) * PHX_JUMP_NIBW));
-    if (e->cfg.use_graph && e->cfg.kernel_mode != 2) {
+    // the wavefront loop is capturable when its schedule is fixed (wave_rounds) and the pool holds
+    // every photon of the call (no refill rounds, which the host drives)
+    const bool wave_fixed = e->cfg.kernel_mode == 2 && e->cfg.wave_rounds > 0 && N > 0 && wave_pool_for(e, N, false) >= N;
+    if (e->cfg.use_graph && (e->cfg.kernel_mode != 2 || wave_fixed)) {
         // the captured graph bakes in every engine buffer pointer: reuse it only if none moved
-        const void* bufs[13] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
-                                 e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p, e->ev_rng.p, e->jump4.p };
-        const bool reuse = e->batch_exec && e->batch_call == c && memcmp(bufs, e->batch_bufs, sizeof(bufs)) == 0;
+        if (wave_fixed) {   // size the path pool before the capture
+            const long long pool = wave_pool_for(e, N, false);
+            PHX_CU(e->wslot.ensure((size_t)pool)); PHX_CU(e->wprd.ensure((size_t)pool)); PHX_CU(e->wsidx.ensure((size_t)pool));
+            PHX_CU(e->wact0.ensure((size_t)pool)); PHX_CU(e->wact1.ensure((size_t)pool)); PHX_CU(e->wcnt.ensure(4));
+            PHX_CU(e->wfree.ensure((size_t)pool));
+        }
+        const void* bufs[PHX_BATCH_BUFS] = { e->hitword.p, e->wordoff.p, e->blocksum.p, e->gs_off.p, e->ev_start.p, e->ev_left.p,
+                                             e->counters.p, e->status.p, e->photon.p, e->rng.p, e->jump_tab.p, e->ev_rng.p, e->jump4.p,
+                                             e->wslot.p, e->wprd.p, e->wsidx.p, e->wact0.p, e->wact1.p, e->wcnt.p, e->wfree.p };
+        const bool reuse = e->batch_exec && e->batch_call == c && e->batch_launch == launch_key(e) &&
+                           memcmp(bufs, e->batch_bufs, sizeof(bufs)) == 0;
         if (!reuse) {
             if (e->batch_exec) { cudaGraphExecDestroy(e->batch_exec); e->batch_exec = nullptr; }
             cudaGraph_t graph = nullptr;
@@ -1687,10 +1770,13 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
             cudaGraphDestroy(graph);
             if (ce != cudaSuccess) { e->batch_exec = nullptr; return phx_fail(-2, "batched graph instantiate failed: %s", cudaGetErrorString(ce)); }
             e->batch_call = c;
+            e->batch_launch = launch_key(e);
             memcpy(e->batch_bufs, bufs, sizeof(bufs));
         }
         PHX_CU(cudaGraphLaunch(e->batch_exec, c.st));
+        e->last_graph = 1;
     } else {
+        e->last_graph = 0;
         int rc = batched_enqueue(e, c, photon, want_hits);
         if (rc) return rc;
     }
@@ -1705,7 +1791,7 @@ int phx_simulate_batched_device(phx_engine* e, const float* d_gensteps, const in
 
 int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genstep, int64_t num_photon,
                        int32_t event_index, const float* theta, int32_t mat_line, float wl_lo, float wl_hi,
-                       double* d_hits, double* d_grad, void* stream)
+                       double* d_hits, double* d_grad, int32_t flags, void* stream)
 {
     if (!e || !theta || !d_hits || !d_grad || (num_genstep > 0 && !d_gensteps)) return phx_fail(-1, "phx_adjoint_device: null argument");
     if (num_genstep < 0 || num_photon < 0 || event_index < 0) return phx_fail(-1, "phx_adjoint_device: negative size");
@@ -1794,6 +1880,8 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     A.adj_nms = e->nms;
     A.adj_wl_lo = wl_lo;
     A.adj_binw = binw;
+    A.adj_pathwise = (flags & PHX_ADJ_PATHWISE) ? 1 : 0;
+    A.adj_prim_node = e->prim_node_d.p;
     if (N > 0) {
         const int cv = cv_of(e, false);
         rc = e->cfg.kernel_mode == 2 ? launch_wave_cv<true>(e, A, cv, st) : launch_persistent_b<64, true>(e, A, cv, st);
@@ -2080,10 +2168,11 @@ int phx_set_input_photon_device(phx_engine* e, const float* d_photon, int64_t nu
     return 0;
 }
 
-int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds)
+int phx_last_call_stats(phx_engine* e, int64_t* kernel_launches, int64_t* wave_rounds, int32_t* graph)
 {
     if (!e) return phx_fail(-1, "phx_last_call_stats: null engine");
     if (kernel_launches) *kernel_launches = e->last_launches;
     if (wave_rounds) *wave_rounds = e->last_rounds;
+    if (graph) *graph = e->last_graph;
     return 0;
 }

@@ -51,7 +51,22 @@ struct PersistArgs {
     int num_sensor;
     unsigned adj_mat;
     float adj_nm0, adj_nms, adj_wl_lo, adj_binw;
+    int adj_pathwise;               // carry the refraction tangent (d/d n terms beyond the Fresnel score)
+    const int* adj_prim_node;       // root node of each prim, for the tangent's probe intersections
 };
+
+// the adjoint accumulator's constant fields for one kernel
+PHX_D void score_setup(PhxScore& score, const PersistArgs& A)
+{
+    score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
+    score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
+    score.pathwise = A.adj_pathwise;
+    score.csg = A.S.csg;
+    score.inst_inv = A.S.inst_inv;
+    score.prim_node = A.adj_prim_node;
+    score.tmin = A.C.tmin; score.tmin0 = A.C.tmin0; score.eps0_mask = A.C.eps0_mask;
+    score_tangent_reset(score);
+}
 
 PHX_D unsigned long long phx_globaltimer()
 {
@@ -128,6 +143,7 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
     if (ADJ) {
 #pragma unroll
         for (int k = 0; k < 32; k++) sc->g[k] = 0.f;
+        score_tangent_reset(*sc);
     }
     const int gi = phx_find_genstep(A.gs_off, A.G, idx);
     const float4* g = A.gs + 6 * gi;     // read in place: a local copy would live in local memory
@@ -221,10 +237,7 @@ template <int CV, int BLOCK, bool ADJ = false>
 __global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persistent(PersistArgs A)
 {
     PhxScore score;
-    if (ADJ) {
-        score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
-        score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
-    }
+    if (ADJ) score_setup(score, A);
     PhxScore* sc = ADJ ? &score : nullptr;
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;

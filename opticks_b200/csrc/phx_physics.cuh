@@ -20,6 +20,7 @@
 #include <curand_kernel.h>
 #include "phx_vec.cuh"
 #include "phx_pod.h"
+#include "phx_csg.cuh"
 
 enum { PHX_CONTINUE = 0, PHX_BREAK = 1, PHX_BOUNDARY = 2 };
 
@@ -71,12 +72,40 @@ struct PhxState {
 // 2 reemission probability, 3 refractive index).  A property at wavelength wl is the texture's
 // linear interpolation of its 1 nm samples, so d prop / d theta_b is the filter weight of the
 // samples that lie in bin b.
+//
+// The refractive index also moves the path itself: a refracted direction depends on n, so every
+// later segment length, incidence angle and Fresnel probability does.  With the path's random
+// variables held fixed (event distances, branch choices, sampled directions), that pathwise part
+// of d log p / d n is carried forward as a tangent: the derivatives of the position, direction and
+// polarisation with respect to nu, the parametrised index at the photon's current wavelength.
+// A hit point's tangent and the change of the surface normal come from a probe: the same prim
+// intersected along the ray moved a small step along the tangent.
 struct PhxScore {
     float g[32];
     unsigned mat;              // 1-based material index of the parametrised material
     float nm0, nms;            // texture wavelength domain
     float wl_lo, binw;         // bins [wl_lo + b binw, wl_lo + (b+1) binw), b < 8
+    float3 tpos, tdir, tpol;   // d pos, d mom, d pol / d nu
+    int pathwise;              // carry the tangent (0: score terms only)
+    PhxCsgCtx csg;             // geometry of the probe intersections
+    const float4* inst_inv;
+    const int* prim_node;      // root node of each prim (globalPrimIdx)
+    float tmin, tmin0;         // the trace's tmin by the last flag (probe intersections use the same)
+    unsigned eps0_mask;
 };
+
+PHX_D void score_tangent_reset(PhxScore& S)
+{
+    S.tpos = make_float3(0.f, 0.f, 0.f);
+    S.tdir = S.tpos;
+    S.tpol = S.tpos;
+}
+
+PHX_D bool score_tangent_zero(const PhxScore& S)
+{
+    return S.tpos.x == 0.f && S.tpos.y == 0.f && S.tpos.z == 0.f && S.tdir.x == 0.f && S.tdir.y == 0.f && S.tdir.z == 0.f &&
+           S.tpol.x == 0.f && S.tpol.y == 0.f && S.tpol.z == 0.f;
+}
 
 PHX_D void score_add(PhxScore& S, int kind, float wl, float v)
 {
@@ -90,6 +119,19 @@ PHX_D void score_add(PhxScore& S, int kind, float wl, float v)
     if (b1 >= 0 && b1 < 8) S.g[kind * 8 + b1] += a * v;
 }
 
+// a refractive-index term of the path: clipped at PHX_ADJ_SCORE_CAP (terms near the critical angle, at
+// grazing incidence and along the dipole axis of a scattering have a finite mean and no finite
+// variance).  The two caps were chosen against central differences on the detector's 1M-photon
+// event: 1e3 / 10 leave the dominant bins 6-18 % low, 1e4 / 100 within the differences' 2-6 %
+// errors, 1e5 lets single photons dominate the sum again.
+#ifndef PHX_ADJ_SCORE_CAP
+#define PHX_ADJ_SCORE_CAP 10000.f
+#endif
+PHX_D void score_add_capped(PhxScore& S, float wl, float v)
+{
+    score_add(S, 3, wl, fminf(fmaxf(v, -PHX_ADJ_SCORE_CAP), PHX_ADJ_SCORE_CAP));
+}
+
 // forward-mode dual numbers for d TransCoeff / d n
 struct PhxDual { float v, d; };
 PHX_D PhxDual dd(float v, float d) { PhxDual r; r.v = v; r.d = d; return r; }
@@ -98,6 +140,24 @@ PHX_D PhxDual operator-(PhxDual a, PhxDual b) { return dd(a.v - b.v, a.d - b.d);
 PHX_D PhxDual operator*(PhxDual a, PhxDual b) { return dd(a.v * b.v, a.d * b.v + a.v * b.d); }
 PHX_D PhxDual operator/(PhxDual a, PhxDual b) { return dd(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
 PHX_D PhxDual dsqrt(PhxDual a) { const float r = sqrtf(a.v); return dd(r, r > 0.f ? 0.5f * a.d / r : 0.f); }
+
+PHX_D PhxDual operator-(PhxDual a) { return dd(-a.v, -a.d); }
+PHX_D PhxDual dfabs(PhxDual a) { return a.v < 0.f ? -a : a; }
+
+// dual 3-vectors: value and tangent
+struct PhxDual3 { float3 v, d; };
+PHX_D PhxDual3 d3(float3 v, float3 d) { PhxDual3 r; r.v = v; r.d = d; return r; }
+PHX_D PhxDual3 operator+(PhxDual3 a, PhxDual3 b) { return d3(a.v + b.v, a.d + b.d); }
+PHX_D PhxDual3 operator-(PhxDual3 a, PhxDual3 b) { return d3(a.v - b.v, a.d - b.d); }
+PHX_D PhxDual3 operator*(PhxDual s, PhxDual3 a) { return d3(s.v * a.v, s.d * a.v + s.v * a.d); }
+PHX_D PhxDual ddot(PhxDual3 a, PhxDual3 b) { return dd(dot(a.v, b.v), dot(a.d, b.v) + dot(a.v, b.d)); }
+PHX_D PhxDual3 dcross(PhxDual3 a, PhxDual3 b) { return d3(cross(a.v, b.v), cross(a.d, b.v) + cross(a.v, b.d)); }
+PHX_D PhxDual3 dnormalize(PhxDual3 a)
+{
+    const PhxDual l = dsqrt(ddot(a, a));
+    const PhxDual inv = dd(1.f, 0.f) / l;
+    return inv * a;
+}
 
 // TransCoeff of propagate_at_boundary as a function of (n1, n2) at fixed c1 and E1 amplitudes
 PHX_D PhxDual trans_coeff_dual(PhxDual n1, PhxDual n2, float c1, float E1x, float E1y)
@@ -478,10 +538,20 @@ PHX_COLD void rayleigh_scatter(PhxPhoton& p, curandStateXORWOW& rng, unsigned& s
     p.pol = polarization;
 }
 
+// the pathwise tangent over one segment: the hit point's tangent and the change of the segment
+// length (from the probe); on = the photon carries a nonzero tangent
+struct PhxAdjSeg {
+    bool on;
+    float dD;
+    float3 dpos_hit;
+    float3 dnormal;
+};
+
 template <bool ADJ = false>
-PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, float distance_to_boundary, const PhxProps& P, unsigned& status, PhxScore* sc = nullptr)
+PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, float distance_to_boundary, const PhxProps& P, unsigned& status, PhxScore* sc = nullptr, const PhxAdjSeg* seg = nullptr)
 {
     const bool scored = ADJ && s.m1idx == sc->mat;
+    const bool carry = ADJ && seg && seg->on;
     const float absorption_length = s.material1.y;
     const float scattering_length = s.material1.z;
     const float reemission_prob = s.material1.w;
@@ -502,6 +572,7 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
                 score_add(*sc, 1, p.wavelength, d / (scattering_length * scattering_length));
                 score_add(*sc, 2, p.wavelength, u_reemit < reemission_prob ? 1.f / reemission_prob : -1.f / (1.f - reemission_prob));
             }
+            if (ADJ && carry) score_tangent_reset(*sc);   // a new wavelength and direction: nu changes
             if (u_reemit < reemission_prob) {
                 float u_re_wavelength = phx_uniform(rng);
                 float u_re_mom_ph = phx_uniform(rng);
@@ -527,7 +598,23 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
             }
             p.time += scattering_distance / group_velocity;
             p.pos += scattering_distance * (p.mom);
+            const float3 e0 = p.pol;
             rayleigh_scatter(p, rng, status);
+            if (ADJ && carry) {
+                // the scattered direction d' is a path variable with density ~ 1 - (e.d')^2 about the
+                // old polarisation e; the new polarisation is +-normalize(e - (e.d') d')
+                const float3 d1 = p.mom, e1 = p.pol, de = sc->tpol;
+                const float ed = dot(e0, d1);
+                const float q = 1.f - ed * ed;
+                if (q > 1e-12f) score_add_capped(*sc, p.wavelength, -2.f * ed * dot(de, d1) / q);
+                const float3 u = e0 - ed * d1;
+                const float ul = length(u);
+                const float3 du = de - dot(de, d1) * d1;
+                const float sgn = dot(e1, u) < 0.f ? -1.f : 1.f;
+                sc->tpos = sc->tpos + scattering_distance * sc->tdir;
+                sc->tdir = make_float3(0.f, 0.f, 0.f);
+                sc->tpol = ul > 1e-12f ? (sgn / ul) * (du - dot(e1, du) * e1) : make_float3(0.f, 0.f, 0.f);
+            }
             flag = PHX_BULK_SCATTER;
             return PHX_CONTINUE;
         }
@@ -538,13 +625,76 @@ PHX_D int propagate_to_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
         score_add(*sc, 0, p.wavelength, D / (absorption_length * absorption_length));
         score_add(*sc, 1, p.wavelength, D / (scattering_length * scattering_length));
     }
+    if (ADJ && carry) {
+        // the same survival with the segment length moved by the tangent, in whatever material
+        score_add_capped(*sc, p.wavelength, -seg->dD * (1.f / absorption_length + 1.f / scattering_length));
+        sc->tpos = seg->dpos_hit;
+    }
     p.pos += distance_to_boundary * (p.mom);
     p.time += distance_to_boundary / group_velocity;
     return PHX_BOUNDARY;
 }
 
+#ifndef PHX_ADJ_TANGENT_CAP
+#define PHX_ADJ_TANGENT_CAP 100.f
+#endif
+// d TransCoeff / d nu and the tangents of the new direction and polarisation: the arithmetic of
+// propagate_at_boundary in dual numbers, with n1, n2, the direction, polarisation and surface
+// normal carrying their derivatives; the branches (TIR, normal incidence, reflect) are the
+// photon's own
+PHX_D void adj_boundary_tangent(PhxScore& sc, const PhxPhoton& p, const PhxState& s, const float3& normal, const float3& dnormal,
+                                bool tir, bool normal_incidence, bool reflect)
+{
+    const PhxDual one = dd(1.f, 0.f), two = dd(2.f, 0.f);
+    const PhxDual n1 = dd(s.material1.x, s.m1idx == sc.mat ? 1.f : 0.f);
+    const PhxDual n2 = dd(s.material2.x, s.m2idx == sc.mat ? 1.f : 0.f);
+    const PhxDual eta = n1 / n2;
+    const PhxDual3 mom = d3(p.mom, sc.tdir), pol = d3(p.pol, sc.tpol), nrm = d3(normal, dnormal);
+    const PhxDual _c1 = -ddot(mom, nrm);
+    const PhxDual3 on = _c1.v < 0.f ? d3(-1.f * nrm.v, -1.f * nrm.d) : nrm;
+    const PhxDual3 trans = dcross(mom, on);
+    const PhxDual trans_length = dsqrt(ddot(trans, trans));
+    const PhxDual3 A_trans = normal_incidence ? pol : (one / trans_length) * trans;
+    const PhxDual E1_perp = ddot(pol, A_trans);
+    const PhxDual c1 = dfabs(_c1);
+    const PhxDual c2 = tir ? dd(0.f, 0.f) : dsqrt(one - eta * eta * (one - c1 * c1));
+    const PhxDual EdotN = ddot(pol, on);
+    const PhxDual n1c1 = n1 * c1, n2c2 = n2 * c2, n2c1 = n2 * c1, n1c2 = n1 * c2;
+    PhxDual E1x = dd(0.f, 0.f), E1y = dd(1.f, 0.f);
+    if (!normal_incidence) {
+        const PhxDual3 r = pol - E1_perp * A_trans;
+        E1x = E1_perp;
+        E1y = dsqrt(ddot(r, r));
+    }
+    const PhxDual tx = two * n1c1 * E1x / (n1c1 + n2c2);
+    const PhxDual ty = two * n1c1 * E1y / (n2c1 + n1c2);
+    const PhxDual T = (tir || n1c1.v == 0.f) ? dd(0.f, 0.f) : n2c2 * (tx * tx + ty * ty) / n1c1;
+    if (!tir && T.v > 0.f && T.v < 1.f) {
+        score_add_capped(sc, p.wavelength, (reflect ? -1.f / (1.f - T.v) : 1.f / T.v) * T.d);
+    }
+    const PhxDual3 mom2 = reflect ? mom + (two * c1) * on : eta * mom + (eta * c1 - c2) * on;
+    PhxDual3 pol2;
+    if (normal_incidence) {
+        pol2 = reflect ? (s.material2.x > s.material1.x ? d3(-1.f * pol.v, -1.f * pol.d) : pol) : pol;
+    } else if (reflect && tir) {
+        pol2 = (two * EdotN) * on - pol;
+    } else {
+        const PhxDual3 A_paral = dnormalize(dcross(mom2, A_trans));
+        const PhxDual rx = reflect ? tx - E1x : tx, ry = reflect ? (n2 * ty / n1) - E1y : ty;
+        const PhxDual rl = dsqrt(rx * rx + ry * ry);
+        pol2 = (rx / rl) * A_trans + (ry / rl) * A_paral;
+    }
+    // Near the critical angle the refracted direction's derivative grows without bound (d theta2/d n
+    // ~ 1/cos theta2) while the transmission probability vanishes: the estimator's mean stays finite
+    // but its variance does not.  The direction tangent is capped at PHX_ADJ_TANGENT_CAP (per unit
+    // of n), a bias confined to rays refracted within about half a degree of grazing.
+    const float tl = length(mom2.d), pl = length(pol2.d);
+    sc.tdir = (tl > PHX_ADJ_TANGENT_CAP ? PHX_ADJ_TANGENT_CAP / tl : 1.f) * mom2.d;
+    sc.tpol = (pl > PHX_ADJ_TANGENT_CAP ? PHX_ADJ_TANGENT_CAP / pl : 1.f) * pol2.d;
+}
+
 template <bool ADJ = false>
-PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal, PhxScore* sc = nullptr)
+PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW& rng, const PhxState& s, const float3& normal, PhxScore* sc = nullptr, const PhxAdjSeg* seg = nullptr)
 {
     const float n1 = s.material1.x;
     const float n2 = s.material2.x;
@@ -573,11 +723,13 @@ PHX_D int propagate_at_boundary(unsigned& flag, PhxPhoton& p, curandStateXORWOW&
     const float TransCoeff = (tir || n1c1 == 0.f ? 0.f : n2c2 * dot2(E2_t, E2_t) / n1c1);
     const float u_reflect = phx_uniform(rng);
     bool reflect = u_reflect > TransCoeff;
-    if (ADJ && !tir && n1c1 != 0.f && TransCoeff > 0.f && TransCoeff < 1.f && (s.m1idx == sc->mat || s.m2idx == sc->mat)) {
-        // Fresnel branch probability: log T (transmit) or log(1-T) (reflect), T = T(n1, n2)
-        const float k = reflect ? -1.f / (1.f - TransCoeff) : 1.f / TransCoeff;
-        if (s.m1idx == sc->mat) score_add(*sc, 3, p.wavelength, k * trans_coeff_dual(dd(n1, 1.f), dd(n2, 0.f), c1, E1.x, E1.y).d);
-        if (s.m2idx == sc->mat) score_add(*sc, 3, p.wavelength, k * trans_coeff_dual(dd(n1, 0.f), dd(n2, 1.f), c1, E1.x, E1.y).d);
+    if (ADJ && ((seg && seg->on) || s.m1idx == sc->mat || s.m2idx == sc->mat)) {
+        // Fresnel branch probability log T (transmit) or log(1-T) (reflect) with T(n1, n2, incidence,
+        // polarisation), and the new direction and polarisation tangents
+        if (!(seg && seg->on)) score_tangent_reset(*sc);
+        adj_boundary_tangent(*sc, p, s, normal, seg && seg->on ? seg->dnormal : make_float3(0.f, 0.f, 0.f), tir,
+                             normal_incidence, reflect);
+        if (!sc->pathwise) score_tangent_reset(*sc);
     }
     p.mom = reflect ? p.mom + 2.0f * c1 * oriented_normal : eta * (p.mom) + (eta * c1 - c2) * oriented_normal;
     const float3 A_paral = normalize(cross(p.mom, A_trans));
@@ -657,6 +809,70 @@ PHX_D int propagate_at_surface(unsigned& flag, PhxPhoton& p, curandStateXORWOW& 
     return action;
 }
 
+// The probe of the pathwise tangent: the prim the closest hit found, intersected along the ray moved
+// by eps along the tangent (origin + eps tpos, direction + eps tdir); the differences give the
+// hit point's tangent, the segment length's and the normal's.  A probe that misses the prim or
+// lands on another face of it (normal turned by more than ~25 degrees) falls back to the
+// tangent plane at the hit (no curvature).
+#define PHX_ADJ_PROBE_SHIFT 10.f      // mm the probe moves the hit point
+PHX_D void adj_probe(PhxAdjSeg& seg, const PhxScore& sc, const PhxPhoton& p, const PhxPRD& prd, unsigned& status)
+{
+    seg.on = sc.pathwise && !score_tangent_zero(sc);
+    seg.dD = 0.f;
+    seg.dpos_hit = make_float3(0.f, 0.f, 0.f);
+    seg.dnormal = seg.dpos_hit;
+    if (!seg.on) return;
+    const float3 n1 = prd.normal;
+    const float D = prd.distance;
+    // tangent plane fallback: the hit point slides in the plane of the normal
+    const float dn = dot(n1, p.mom);
+    const float3 w = sc.tpos + D * sc.tdir;
+    if (fabsf(dn) > 1e-6f) {
+        seg.dD = -dot(n1, w) / dn;
+        seg.dpos_hit = w + seg.dD * p.mom;
+    }
+    const float mag = length(sc.tpos) + D * length(sc.tdir);
+    if (!(mag > 0.f) || !sc.prim_node) return;
+    const float eps = PHX_ADJ_PROBE_SHIFT / mag;
+    const float3 o2 = p.pos + eps * sc.tpos;
+    const float3 d2 = normalize(p.mom + eps * sc.tdir);
+    const unsigned gp = prd.gp_bd >> 16, ii = prd.ii_id >> 16;
+    const float4* q = sc.inst_inv + 4 * ii;
+    float4 m[4] = { __ldg(q + 0), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3) };
+    const float3 lo = xform_row(m, o2, 1.f), ld = xform_row(m, d2, 0.f);
+    const float tmin = (p.obf & sc.eps0_mask) ? sc.tmin0 : sc.tmin;
+    float4 is;
+    unsigned st = 0;
+    if (!intersect_prim<PHX_CV_FULL>(is, sc.csg, __ldg(sc.prim_node + gp), tmin, lo, ld, st)) return;
+    const float3 n2 = normalize(xform_col(m, make_float3(is.x, is.y, is.z), 0.f));
+    if (dot(n1, n2) < 0.9f) return;
+    const float3 h1 = p.pos + D * p.mom;
+    const float3 h2 = o2 + is.w * d2;
+    seg.dD = (is.w - D) / eps;
+    seg.dpos_hit = (1.f / eps) * (h2 - h1);
+    seg.dnormal = (1.f / eps) * (n2 - n1);
+    status |= st & PHX_STATUS_CSG_STACK;
+}
+
+// tangents through a surface: specular reflection as the mirror map (normal change included), a
+// diffuse reflection draws a new direction (its density cos(angle to the normal) does not
+// involve the old direction; the tangent restarts, the polarisation's change is not carried)
+PHX_D void adj_surface_tangent(PhxScore& sc, unsigned flag, const float3& mom0, const float3& pol0, const float3& normal,
+                               const float3& dnormal)
+{
+    if (flag == PHX_SURFACE_SREFLECT) {
+        const PhxDual two = dd(2.f, 0.f);
+        const PhxDual3 mom = d3(mom0, sc.tdir), pol = d3(pol0, sc.tpol), nrm = d3(normal, dnormal);
+        const PhxDual3 mom2 = mom - (two * ddot(mom, nrm)) * nrm;
+        const PhxDual3 pol2 = (two * ddot(pol, nrm)) * nrm - pol;
+        sc.tdir = mom2.d;
+        sc.tpol = pol2.d;
+    } else if (flag == PHX_SURFACE_DREFLECT) {
+        sc.tdir = make_float3(0.f, 0.f, 0.f);
+        sc.tpol = sc.tdir;
+    }
+}
+
 // qsim::propagate : returns CONTINUE/BREAK, sets the flag.  ADJ adds the score terms.
 template <bool ADJ = false>
 PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, const PhxProps& P, unsigned& status, PhxScore* sc = nullptr)
@@ -671,15 +887,17 @@ PHX_D int propagate(PhxPhoton& p, curandStateXORWOW& rng, const PhxPRD& prd, con
     PhxState s;
     fill_state<ADJ>(s, P, boundary, p.wavelength, cosTheta);
     unsigned flag = 0;
-    int command = propagate_to_boundary<ADJ>(flag, p, rng, s, prd.distance, P, status, sc);
+    PhxAdjSeg seg;
+    if (ADJ) adj_probe(seg, *sc, p, prd, status);
+    int command = propagate_to_boundary<ADJ>(flag, p, rng, s, prd.distance, P, status, sc, ADJ ? &seg : nullptr);
     if (command == PHX_BOUNDARY) {
         const int ems = (int)s.optical.y;
         if (ems == PHX_EMS_NOSURFACE) {
-            command = propagate_at_boundary<ADJ>(flag, p, rng, s, normal, sc);
-        } else if (ems == PHX_EMS_SURFACE) {
+            command = propagate_at_boundary<ADJ>(flag, p, rng, s, normal, sc, ADJ ? &seg : nullptr);
+        } else if (ems == PHX_EMS_SURFACE || lposcost < 0.f) {
+            float3 mom0 = p.mom, pol0 = p.pol;
             command = propagate_at_surface(flag, p, rng, s, normal);
-        } else if (lposcost < 0.f) {
-            command = propagate_at_surface(flag, p, rng, s, normal);
+            if (ADJ && seg.on) adj_surface_tangent(*sc, flag, mom0, pol0, normal, seg.dnormal);
         } else if (ems == PHX_EMS_SURFACE_ZPLUS_SENSOR_A) {
             (void)phx_uniform(rng);   // alignment burn of propagate_at_surface_Detect
             flag = PHX_SURFACE_DETECT;

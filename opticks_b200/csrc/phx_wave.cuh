@@ -51,6 +51,7 @@ struct WaveArgs {
     long long pool;           // slots (init only)
     uint32_t* live_bits;      // refill rounds: live slots as bits, turned into the next list in slot
                               // order by k_wave_act (null: live slots are appended to act_out)
+    int refill_idle;          // k_wave_trace_df: idle lanes a warp waits for before taking new rays
 };
 
 PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L)
@@ -89,27 +90,35 @@ PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
     L.idx = W.sidx[s];
 }
 
+// the 32 score terms and the refraction tangent (pos, mom, pol) of a path: PHX_WAVE_SCORE_F4 float4
+#define PHX_WAVE_SCORE_F4 11
 PHX_D void wave_store_score(const WaveArgs& W, uint32_t s, const PhxScore* sc)
 {
-    float4* o = W.score + 8 * (size_t)s;
+    float4* o = W.score + PHX_WAVE_SCORE_F4 * (size_t)s;
 #pragma unroll
     for (int k = 0; k < 8; k++) o[k] = make_float4(sc->g[4 * k], sc->g[4 * k + 1], sc->g[4 * k + 2], sc->g[4 * k + 3]);
+    o[8] = make_float4(sc->tpos.x, sc->tpos.y, sc->tpos.z, sc->tdir.x);
+    o[9] = make_float4(sc->tdir.y, sc->tdir.z, sc->tpol.x, sc->tpol.y);
+    o[10] = make_float4(sc->tpol.z, 0.f, 0.f, 0.f);
 }
 
 PHX_D void wave_load_score(const WaveArgs& W, uint32_t s, PhxScore* sc)
 {
-    const float4* o = W.score + 8 * (size_t)s;
+    const float4* o = W.score + PHX_WAVE_SCORE_F4 * (size_t)s;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         const float4 v = o[k];
         sc->g[4 * k] = v.x; sc->g[4 * k + 1] = v.y; sc->g[4 * k + 2] = v.z; sc->g[4 * k + 3] = v.w;
     }
+    const float4 a = o[8], b = o[9], c = o[10];
+    sc->tpos = make_float3(a.x, a.y, a.z);
+    sc->tdir = make_float3(a.w, b.x, b.y);
+    sc->tpol = make_float3(b.z, b.w, c.x);
 }
 
 PHX_D void wave_score_setup(PhxScore& score, const PersistArgs& A)
 {
-    score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
-    score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
+    score_setup(score, A);
 }
 
 // a path may take another bounce (the loop condition of CSGOptiX/CSGOptiX7.cu:477)
@@ -252,10 +261,6 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
 #ifndef PHX_WAVE_TRACE_DF
 #define PHX_WAVE_TRACE_DF 1
 #endif
-// idle lanes a warp waits for before it takes new rays (32: refill only when the whole warp is done)
-#ifndef PHX_WAVE_TRACE_REFILL
-#define PHX_WAVE_TRACE_REFILL 12
-#endif
 template <int CV>
 __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(WaveArgs W)
 {
@@ -280,7 +285,8 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
     for (;;) {
         // hand new rays to the idle lanes (at most a window and a fresh window per step)
         unsigned idle = __ballot_sync(FULL, !has);
-        if (__popc(idle) < PHX_WAVE_TRACE_REFILL) idle = 0u;
+        // idle lanes a warp waits for before it takes new rays (32: only when the whole warp is done)
+        if (__popc(idle) < W.refill_idle) idle = 0u;
         for (int pass = 0; pass < 2 && idle != 0u && !drained; pass++) {
             if (wnext >= wend) {
                 unsigned b = 0u;
@@ -353,9 +359,6 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
 // takes one path and runs its remaining bounces to the end with the one-kernel loop's step
 // (persist_step: the shared closest-hit and physics code), so a long chain no longer costs two
 // launches per bounce.  Photons, seq and hits are the same as the rounds would give.
-#ifndef PHX_WAVE_TAIL
-#define PHX_WAVE_TAIL (1 << 18)
-#endif
 template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
 {

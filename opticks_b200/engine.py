@@ -115,6 +115,17 @@ class Engine:
             _lib.lib().phx_destroy(self._h)
             self._h = None
 
+    LAUNCH_FIELDS = ("kernel_mode", "block", "regroup", "chunk", "use_graph", "wave_pool", "wave_refill", "wave_rounds",
+                     "wave_tail")
+
+    def set_launch_config(self, **kw) -> None:
+        """change the launch shape of later calls (fields of LAUNCH_FIELDS); results do not change"""
+        for k, v in kw.items():
+            if k not in self.LAUNCH_FIELDS:
+                raise KeyError(f"{k} is not a launch field")
+            setattr(self.config, k, v)
+        _lib.check(_lib.lib().phx_set_launch_config(self._h, C.byref(self.config)), "phx_set_launch_config")
+
     def trim(self) -> int:
         """release the device memory grown for calls (wavefront pool and the like); returns bytes freed"""
         b = C.c_int64(0)
@@ -246,9 +257,9 @@ class Engine:
 
     def last_call_stats(self) -> dict:
         """kernel launches and wavefront rounds of the last simulate call"""
-        k, r = C.c_int64(0), C.c_int64(0)
-        _lib.check(_lib.lib().phx_last_call_stats(self._h, C.byref(k), C.byref(r)), "phx_last_call_stats")
-        return {"kernel_launches": int(k.value), "wave_rounds": int(r.value)}
+        k, r, g = C.c_int64(0), C.c_int64(0), C.c_int32(0)
+        _lib.check(_lib.lib().phx_last_call_stats(self._h, C.byref(k), C.byref(r), C.byref(g)), "phx_last_call_stats")
+        return {"kernel_launches": int(k.value), "wave_rounds": int(r.value), "graph": bool(g.value)}
 
     # ------------------------------------------------------------------ hit merging
     def merge_hits(self, records: np.ndarray, select_flagmask: int = 0xFFFFFFFF, time_window: float = 1.0) -> np.ndarray:

@@ -27,13 +27,13 @@ def det(cuda):
     eng.close()
 
 
-def _adj(d, gs, theta, event=0):
+def _adj(d, gs, theta, event=0, pathwise=True):
     torch = d["torch"]
     g = torch.from_numpy(gs).cuda()
     N = int(gs.view(np.int32)[:, 0, 3].sum())
     hits = torch.zeros((scenes.NUM_PMT,), dtype=torch.float64, device="cuda")
     grad = torch.zeros((scenes.NUM_PMT, 32), dtype=torch.float64, device="cuda")
-    ADJ.adjoint_device(d["eng"], g, N, event, theta, d["mat_line"], *WL, hits, grad)
+    ADJ.adjoint_device(d["eng"], g, N, event, theta, d["mat_line"], *WL, hits, grad, pathwise=pathwise)
     torch.cuda.synchronize()
     return hits.cpu().numpy(), grad.cpu().numpy()
 
@@ -52,7 +52,7 @@ def test_adjoint_forward_equals_plain_engine(det):
 def test_adjoint_scores_match_fp64_cpu_estimator(det):
     gs = scenes.detector_gensteps(2, 1500, seed=22, lib=det["lib"])
     n = 3000
-    hits, grad = _adj(det, gs, det["theta"])
+    hits, grad = _adj(det, gs, det["theta"], pathwise=False)    # the FP64 estimator holds the score terms
     phys2 = ADJ.retabulate(det["phys"], det["theta"], det["mat_line"], *WL)
     eng2 = det["E"].Engine(det["fd"].arrays(), phys2, det["E"].default_config(max_photon=n))
     u = eng2.rng_sequence(0, 0, n, 1024)
@@ -109,8 +109,10 @@ def test_autograd_function_and_finite_differences(det):
         assert abs(z) < 4.0
 
 
-def test_adjoint_wavefront_equals_persistent(det):
-    """the adjoint pass in both loop forms: identical hits, score sums equal to float accumulation order"""
+@pytest.mark.parametrize("pool", [0, 1 << 12])
+def test_adjoint_wavefront_equals_persistent(det, pool):
+    """the adjoint pass in both loop forms: identical hits, score sums equal to float accumulation order;
+    also through a 4,096-slot pool, whose refill rounds reload the score slots in slot order"""
     torch = det["torch"]
     gs = scenes.detector_gensteps(6, 3000, seed=31, lib=det["lib"])
     N = int(gs.view(np.int32)[:, 0, 3].sum())
@@ -118,7 +120,8 @@ def test_adjoint_wavefront_equals_persistent(det):
     out = []
     for mode in (1, 2):
         eng = det["E"].Engine(det["fd"].arrays(), det["phys"],
-                              det["E"].default_config(max_photon=N, num_sensor=scenes.NUM_PMT, kernel_mode=mode))
+                              det["E"].default_config(max_photon=N, num_sensor=scenes.NUM_PMT, kernel_mode=mode,
+                                                      wave_pool=pool))
         h = torch.zeros((scenes.NUM_PMT,), dtype=torch.float64, device="cuda")
         j = torch.zeros((scenes.NUM_PMT, 32), dtype=torch.float64, device="cuda")
         ADJ.adjoint_device(eng, g, N, 2, det["theta"], det["mat_line"], *WL, h, j, torch.cuda.current_stream().cuda_stream)
@@ -131,3 +134,30 @@ def test_adjoint_wavefront_equals_persistent(det):
     # cancelling Fresnel scores, so their totals agree to a relative 2e-3 of the term scale
     scale = np.abs(out[0][1]).sum(0) + 1e-12
     assert np.all(np.abs(out[0][1].sum(0) - out[1][1].sum(0)) <= 2e-3 * scale)
+
+
+def test_refractive_index_gradient_with_pathwise_term(det):
+    """d(total hits)/d n in the bin holding the emission peak (420-460 nm): the pathwise tangent of the
+    refracted direction carries most of it (the Fresnel score alone is a few per cent of it); the
+    adjoint agrees with central differences (step 1e-3 relative, common random numbers)"""
+    M = 48
+    gs = scenes.detector_gensteps(50, 10000, seed=29, lib=det["lib"])
+    base = det["theta"].astype(np.float64)
+    k = 27
+    h = 1e-3 * base[k]
+    adj, adj0, fd = [], [], []
+    for ev in range(1, M + 1):
+        adj.append(_adj(det, gs, det["theta"], event=ev)[1][:, k].sum())
+        adj0.append(_adj(det, gs, det["theta"], event=ev, pathwise=False)[1][:, k].sum())
+        tp, tm = base.copy(), base.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd.append((_adj(det, gs, tp.astype(np.float32), event=ev)[0].sum() -
+                   _adj(det, gs, tm.astype(np.float32), event=ev)[0].sum()) / (2 * h))
+    a, a0, f = np.array(adj), np.array(adj0), np.array(fd)
+    se = np.sqrt(a.var(ddof=1) / M + f.var(ddof=1) / M)
+    z = (a.mean() - f.mean()) / se
+    print(f"rindex bin 3: adjoint {a.mean():.1f} +- {a.std(ddof=1)/np.sqrt(M):.1f} (score only {a0.mean():.1f}) "
+          f"fd {f.mean():.1f} +- {f.std(ddof=1)/np.sqrt(M):.1f}  z {z:.2f}")
+    assert f.mean() < 0 and abs(a0.mean()) < 0.3 * abs(f.mean())    # the score alone misses it
+    assert abs(z) < 4.0

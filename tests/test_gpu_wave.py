@@ -86,6 +86,44 @@ def test_wave_batched_equals_persistent(det, kw):
     a.close(); b.close()
 
 
+@pytest.mark.parametrize("launch", [dict(wave_rounds=3, use_graph=1, wave_refill=8),
+                                    dict(wave_rounds=10, use_graph=1, wave_refill=32),
+                                    dict(wave_rounds=0, wave_tail=1 << 12, wave_refill=1)])
+def test_wave_schedules_equal_persistent(det, launch):
+    """the autotuner's knobs change no result: a fixed schedule of rounds then the tail kernel,
+    captured as a CUDA graph and replayed (second call), other refill thresholds, another tail
+    threshold; batched and plain calls"""
+    torch = det[0]
+    gs = scenes.batched_events(48, median=20000.0, lib=det[2])
+    ev = np.arange(len(gs), dtype=np.int32)
+    counts = gs.view(np.int32)[:, 0, 3].astype(np.int64)
+    N = int(counts.sum())
+    a, b = _engines(det, int(counts.max()))
+    b.set_launch_config(**launch)
+    g = torch.from_numpy(gs).cuda()
+    e = torch.from_numpy(ev).cuda()
+    outs = []
+    for eng, calls in ((a, 1), (b, 2)):
+        ph = torch.empty((N, 4, 4), dtype=torch.float32, device="cuda")
+        sq = torch.empty((N, 2, 2), dtype=torch.int64, device="cuda")
+        for _ in range(calls):
+            ph.fill_(0.0)
+            nh, st = eng.simulate_batched_device(g, e, N, photon=ph, seq=sq, stream=torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            assert st == 0
+        outs.append((ph, sq))
+    assert torch.equal(outs[0][0].view(torch.int32), outs[1][0].view(torch.int32))
+    assert torch.equal(outs[0][1], outs[1][1])
+    # plain call of one event with the same launch shape (a fixed schedule applies to batched calls only)
+    g1 = torch.from_numpy(np.ascontiguousarray(gs[:3])).cuda()
+    n1 = int(counts[:3].sum())
+    ra, rb = _run(torch, a, g1, n1, 7), _run(torch, b, g1, n1, 7)
+    assert rb[4] == 0
+    assert torch.equal(ra[0].view(torch.int32), rb[0].view(torch.int32))
+    assert torch.equal(ra[1], rb[1]) and torch.equal(ra[3], rb[3])
+    a.close(); b.close()
+
+
 def test_wave_batched_beyond_minimum_pool_equals_persistent(det):
     """84M photons in one batched call with wave_pool left at 0: more than the 2^26-slot minimum
     pool, so the slot count comes from the free device memory (every photon in flight here);
