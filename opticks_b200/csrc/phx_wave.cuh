@@ -54,19 +54,30 @@ struct WaveArgs {
     int refill_idle;          // k_wave_trace_df: idle lanes a warp waits for before taking new rays
 };
 
-PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L)
+// The slot's first 32 B sector (position, time, direction, q1.w) is all the closest-hit kernel
+// needs: bit 31 of the stored q1.w carries the choice of tmin (the last flag against the epsilon0
+// mask), and the photon's own bit 31 of q1.w rides in bit 30 of the bounce word.  `first`: the
+// slot takes a new photon (its index is written once).
+PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L, bool first)
 {
     PhxWaveSlot* o = W.slot + s;
     const PhxPhoton& p = L.p;
+    const unsigned eps0 = (p.obf & W.A.C.eps0_mask) ? 0x80000000u : 0u;
     o->q0 = make_float4(p.pos.x, p.pos.y, p.pos.z, p.time);
-    o->q1 = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float(p.hitcount_iindex));
+    o->q1 = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float((p.hitcount_iindex & 0x7fffffffu) | eps0));
     o->q2 = make_float4(p.pol.x, p.pol.y, p.pol.z, p.wavelength);
     o->q3 = make_float4(__uint_as_float(p.obf), __uint_as_float(p.identity), __uint_as_float(p.index), __uint_as_float(p.flagmask));
     o->ra = make_uint4(L.rng.d, L.rng.v[0], L.rng.v[1], L.rng.v[2]);
-    o->rb = make_uint4(L.rng.v[3], L.rng.v[4], (unsigned)L.bounce, (unsigned)L.ev);
+    o->rb = make_uint4(L.rng.v[3], L.rng.v[4], (unsigned)L.bounce | ((p.hitcount_iindex >> 1) & 0x40000000u), (unsigned)L.ev);
     o->his = make_ulonglong2(L.seqhis[0], L.seqhis[1]);
     o->bnd = make_ulonglong2(L.seqbnd[0], L.seqbnd[1]);
-    W.sidx[s] = L.idx;
+    if (first) W.sidx[s] = L.idx;
+}
+
+// the tmin of a slot's next closest hit, from its first sector
+PHX_D float wave_tmin(const WaveArgs& W, const float4& q1)
+{
+    return (__float_as_uint(q1.w) & 0x80000000u) ? W.A.C.tmin0 : W.A.C.tmin;
 }
 
 PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
@@ -75,7 +86,7 @@ PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
     const float4 q0 = o->q0, q1 = o->q1, q2 = o->q2, q3 = o->q3;
     PhxPhoton& p = L.p;
     p.pos = make_float3(q0.x, q0.y, q0.z); p.time = q0.w;
-    p.mom = make_float3(q1.x, q1.y, q1.z); p.hitcount_iindex = __float_as_uint(q1.w);
+    p.mom = make_float3(q1.x, q1.y, q1.z);
     p.pol = make_float3(q2.x, q2.y, q2.z); p.wavelength = q2.w;
     p.obf = __float_as_uint(q3.x); p.identity = __float_as_uint(q3.y);
     p.index = __float_as_uint(q3.z); p.flagmask = __float_as_uint(q3.w);
@@ -84,7 +95,8 @@ PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
     L.rng.v[3] = rb.x; L.rng.v[4] = rb.y;
     L.rng.boxmuller_flag = 0; L.rng.boxmuller_flag_double = 0;
     L.rng.boxmuller_extra = 0.f; L.rng.boxmuller_extra_double = 0.0;
-    L.bounce = (int)rb.z; L.ev = (int)rb.w;
+    L.bounce = (int)(rb.z & 0x3fffffffu); L.ev = (int)rb.w;
+    p.hitcount_iindex = (__float_as_uint(q1.w) & 0x7fffffffu) | ((rb.z & 0x40000000u) << 1);
     const ulonglong2 h = o->his, b = o->bnd;
     L.seqhis[0] = h.x; L.seqhis[1] = h.y; L.seqbnd[0] = b.x; L.seqbnd[1] = b.y;
     L.idx = W.sidx[s];
@@ -215,7 +227,7 @@ __global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
         const long long s = base + (threadIdx.x & 31);
         const bool live = wave_refill<CV, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
         if (live) {
-            wave_store(W, (uint32_t)s, L);
+            wave_store(W, (uint32_t)s, L, true);
             if (ADJ) wave_store_score(W, (uint32_t)s, &score);
         }
         wave_append(W, live, (uint32_t)s);
@@ -241,8 +253,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace(WaveArg
         const uint32_t s = W.act_in[i];
         const PhxWaveSlot* o = W.slot + s;
         const float4 q0 = o->q0, q1 = o->q1;
-        const unsigned obf = __float_as_uint(o->q3.x);
-        const float tmin = (obf & W.A.C.eps0_mask) ? W.A.C.tmin0 : W.A.C.tmin;
+        const float tmin = wave_tmin(W, q1);
         const PhxPRD prd = phx_trace_step<CV>(W.A.S, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z), tmin,
                                                   W.A.C.tmax, status);
         W.prd[s].nd = make_float4(prd.normal.x, prd.normal.y, prd.normal.z, prd.distance);
@@ -302,8 +313,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
                 s = W.act_in[wnext + rank];
                 const PhxWaveSlot* ps = W.slot + s;
                 const float4 q0 = ps->q0, q1 = ps->q1;
-                const unsigned obf = __float_as_uint(ps->q3.x);
-                tmin = (obf & W.A.C.eps0_mask) ? W.A.C.tmin0 : W.A.C.tmin;
+                tmin = wave_tmin(W, q1);
                 o = make_float3(q0.x, q0.y, q0.z);
                 d = make_float3(q1.x, q1.y, q1.z);
                 phx_ray_slabs(o, d, inv, oi);
@@ -431,7 +441,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
             live = !done;
         }
         if (live) {
-            wave_store(W, s, L);
+            wave_store(W, s, L, false);
             if (ADJ) wave_store_score(W, s, &score);
         }
         wave_append(W, live, s);
@@ -457,7 +467,7 @@ __global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
         const uint32_t s = valid ? W.free_list[i] : 0u;
         const bool live = wave_refill<CV, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
         if (live) {
-            wave_store(W, s, L);
+            wave_store(W, s, L, true);
             if (ADJ) wave_store_score(W, s, &score);
         }
         wave_append(W, live, s);

@@ -330,3 +330,33 @@ def test_c3_fp64_distance_error(cuda, polish):
     assert r["hits"] == n
     assert r["fp64_disagrees"] <= n // 100000
     assert r["p999"] < 1e-5
+
+
+# ---------------------------------------------------------------- Cerenkov at scale
+@NEED_REF
+def test_cerenkov_event_matches_reference(cuda):
+    """120,000 Cerenkov photons from 40 tracks of beta 0.75-0.9999 in the liquid scintillator (the
+    bnd-texture rejection sampling of wavelength and cone angle, qudarap/qcerenkov.h:56-320):
+    seqhis and photons against the reference's device code, and no rejection loop at its cap"""
+    from opticks_b200 import engine as E
+    fd, lib, icdf = scenes.detector()
+    phys = lib.arrays()
+    phys["icdf"] = icdf
+    ml = lib.material_line("LS")
+    rng = np.random.Generator(np.random.PCG64(41))
+    pos = scenes.uniform_ball(40, 16000.0, rng)
+    gs = []
+    for k in range(40):
+        d = rng.normal(size=3)
+        d *= rng.uniform(1.0, 40.0) / np.linalg.norm(d)
+        gs.append(scenes.cerenkov_genstep(3000, tuple(pos[k]), ml, delta=tuple(d), beta_inverse=1.0 / rng.uniform(0.75, 0.9999),
+                                          time=float(rng.uniform(0.0, 5.0))))
+    gs = np.stack(gs)
+    N = 120_000
+    eng = _engine(fd, phys, max_photon=N, num_sensor=scenes.NUM_PMT)
+    res = eng.simulate(gs, 6, sensor_hits=True)
+    eng.close()
+    assert res["status"] == 0, E.status_names(res["status"])          # LOOP_CAP clear
+    assert np.all((res["seq"][:, 0, 0] & 0xF) == 1)                      # CK first
+    ph, sq = O.ref_simulate_gpu(fd.arrays(), phys, gs, event_index=6)
+    _compare("Cerenkov 120k", res, ph, sq)
