@@ -53,7 +53,7 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # layout reads 24 B of it), the 64 B sphoton and 32 B sseq writes; + 64 B per hit and the genstep
 # share are added per workload
 BYTES_PER_PHOTON_FIXED = 48 + 64 + 32
-SAMPLE_PER_GENSTEP = 200       # CPU sample: this many photons of every genstep of the event
+SAMPLE_PER_GENSTEP = 30        # CPU sample: this many photons of every genstep of the event
 # DRAM bytes (read + write) of all kernels of one simulate call of this 10M-photon event, from a
 # one-pass ncu capture of the bench's own launches (profiles/launches_dram_wavefront_detector_10M.md)
 DRAM_TRAFFIC = {"bytes_per_call": 20.157e9, "photons": 10_000_000,
@@ -138,7 +138,7 @@ def stride_sample(gs, per_genstep=SAMPLE_PER_GENSTEP):
 
 
 def oracle_rate(fd, phys, gs, reps=1, K=512, seed=123):
-    """photons/s of the CPU oracle (all host threads) over the photons of `gs`, numpy uniforms"""
+    """photons/s of the C restatement (all host threads) over the photons of `gs`, numpy uniforms"""
     from oracle import oracle as O
     S = O.Scene(fd.arrays(), phys)
     n = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
@@ -151,17 +151,49 @@ def oracle_rate(fd, phys, gs, reps=1, K=512, seed=123):
     return n / statistics.mean(times), n, O.lib().oracle_threads(), times
 
 
+def reference_rate(fd, phys, gs, reps=1):
+    """photons/s of the reference's own qsim/CSG path compiled for the CPU (all host threads), or
+    None when that build is absent"""
+    from oracle import oracle as O
+    if not O.have_ref_cpu_sim():
+        return None
+    times, n, nt = [], 0, 0
+    for r in range(reps):
+        ph, _, secs, nt = O.ref_simulate_cpu(fd.arrays(), phys, gs, seed=1 + r, outputs=False)
+        times.append(secs)
+    n = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
+    return n / statistics.mean(times), n, nt, times
+
+
+def cpu_rate(fd, phys, gs, reps=1):
+    """(photons/s, photons, threads, times, kind): the reference's CPU build where it was built,
+    else the C restatement"""
+    r = reference_rate(fd, phys, gs, reps)
+    if r is not None:
+        return (*r, "reference")
+    return (*oracle_rate(fd, phys, gs, reps), "port")
+
+
+KIND_NOTE = {"reference": "the reference's qsim/CSG headers compiled for the CPU (MOCK_CURAND: its mt19937_64 "
+                          "uniforms and nearest-sample mock textures), closest hit over world-box-culled instances",
+             "port": "the C restatement of the path (numpy uniforms); the reference's CPU build is absent"}
+
+
 def cpu_baseline(fd, phys, gs, form_workloads=()):
-    """oracle port on all host threads over the stride sample of the event (and of each form)"""
+    """the CPU implementation on all host threads over the stride sample of the event (and of each
+    form); the C restatement's figure on the same sample beside it"""
     sample = stride_sample(gs)
-    v, n, cores, times = oracle_rate(fd, phys, sample, reps=4)
-    out = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+    v, n, cores, times, kind = cpu_rate(fd, phys, sample, reps=3)
+    out = {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
            "sample": f"{SAMPLE_PER_GENSTEP} photons of each of the {len(gs)} gensteps of the event ({n} photons), "
-                     f"CPU oracle with numpy uniforms, {len(times)} timed passes of {statistics.mean(times):.1f} s"}
+                     f"{KIND_NOTE[kind]}; {len(times)} timed passes of {statistics.mean(times):.1f} s"}
+    if kind == "reference":
+        pv, _, _, pt = oracle_rate(fd, phys, sample, reps=2)
+        out["port"] = {"value": pv, "unit": METRIC, "note": "the C restatement (oracle) on the same sample"}
     forms = {}
     for name, (ffd, fphys, fgs, per, reps) in form_workloads:
-        fv, fn, _, ft = oracle_rate(ffd, fphys, stride_sample(fgs, per), reps=reps)
-        forms[name] = {"value": fv, "unit": METRIC, "sample_photons": fn, "passes": reps, "seconds": sum(ft),
+        fv, fn, _, ft, fk = cpu_rate(ffd, fphys, stride_sample(fgs, per), reps=reps)
+        forms[name] = {"value": fv, "unit": METRIC, "kind": fk, "sample_photons": fn, "passes": reps, "seconds": sum(ft),
                        "sample": f"at most {per} photons of each of the {len(fgs)} gensteps"}
     if forms:
         out["forms"] = forms
@@ -170,35 +202,29 @@ def cpu_baseline(fd, phys, gs, form_workloads=()):
 
 def run_reference(args):
     """--impl reference : CPU implementation of the path on the host cores (rank 0 only), each
-    step the stride sample of the C3 event"""
+    step the stride sample of the C3 event: the reference's own qsim/CSG path compiled for the
+    CPU where it was built, else the C restatement"""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
-    from oracle import oracle as O
-    S = O.Scene(fd.arrays(), phys)
-    K = 512
     sample = stride_sample(gs)
     n = int(sample.view(np.int32)[:, 0, 3].sum())
-    u = np.random.Generator(np.random.PCG64(123)).random((n, K), dtype=np.float32)
-    small = stride_sample(gs, 2)
     for _ in range(args.warmup):
-        S.simulate(small, u[: int(small.view(np.int32)[:, 0, 3].sum())], 0)
+        cpu_rate(fd, phys, stride_sample(gs, 2), reps=1)
     times = []
+    kind, cores = "port", 0
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        S.simulate(sample, u, 0)
-        times.append(time.perf_counter() - t0)
+        v1, _, cores, t1, kind = cpu_rate(fd, phys, sample, reps=1)
+        times.append(t1[0])
     v = n / statistics.mean(times)
-    cores = O.lib().oracle_threads()
     line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "detector-17612pmt-scint-10M", "gensteps": args.gensteps,
                        "photons_per_genstep": args.per_genstep, "sample_photons_per_step": n},
-            "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
                              "sample": f"{SAMPLE_PER_GENSTEP} photons of each of the {len(gs)} gensteps of the event per "
-                                       f"step ({n} photons; oracle port: the reference's qsim needs glm/plog to build "
-                                       f"for the CPU; warm-up steps take 2 photons per genstep)"},
+                                       f"step ({n} photons), {KIND_NOTE[kind]}; warm-up steps take 2 photons per genstep"},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -365,6 +391,16 @@ def c1_workload():
     from opticks_b200 import scenes
     fd, lib, _, gs = scenes.sphere_in_box(1_000_000)
     return fd, lib.arrays(), gs
+
+
+def c1_reference_gs(gs):
+    """C1's genstep with the reference's T_SPHERE torch type (its fixed polarisation phase) for the
+    CPU baselines: the random-polarisation type is this engine's extension, unknown to the
+    reference's storch"""
+    from opticks_b200 import scenes
+    g = np.array(gs, copy=True)
+    g.view(np.int32)[:, 5, 3] = scenes.T_SPHERE
+    return g
 
 
 def cerenkov_workload(lib, num_track=200, per_track=5000, seed=21):
@@ -680,7 +716,8 @@ def main():
                 "adjoint": lambda: measure_adjoint(torch, E, fd, lib, phys, dev)}
             forms = {k: runners[k]() for k in args.forms.split(",") if k}
         cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(
-            fd, phys, gs, form_workloads=(("c1", (c1_fd, c1_phys, c1_gs, 200_000, 50)), ("cerenkov", (fd, phys, ck_gs, 500, 2))))
+            fd, phys, gs, form_workloads=(("c1", (c1_fd, c1_phys, c1_reference_gs(c1_gs), 200_000, 10)),
+                                          ("cerenkov", (fd, phys, ck_gs, 100, 1))))
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -4,6 +4,8 @@
 * ``_ref/libref_csg.so``  the reference's own CSG intersector compiled for the CPU
 * ``_ref/libref_sim.so``  the reference's own qsim/CSG device code driven on the GPU
 * ``_ref/libref_spm.so``  the reference's own hit merge (sysrap/SPM.cu) on the GPU
+* ``_ref/libref_cpu_sim.so`` the reference's own qsim/CSG path compiled for the CPU (MOCK_CURAND)
+* ``_ref/libref_npfold.so`` arrays written by the reference's own NP.hh (loader fixtures)
 * ``merge.py``            numpy restatement of the hit merge
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and
@@ -293,6 +295,50 @@ def have_ref_csg() -> bool:
 
 def have_ref_sim() -> bool:
     return os.path.exists(REF_SIM)
+
+
+REF_CPU_SIM = os.path.join(HERE, "_ref", "libref_cpu_sim.so")
+
+
+def have_ref_cpu_sim() -> bool:
+    return os.path.exists(REF_CPU_SIM)
+
+
+def ref_simulate_cpu(geom: dict, phys: dict, gs: np.ndarray, nthreads: int = 0, seed: int = 1, max_bounce: int = 31,
+                     max_time: float = 1e27, tmin: float = 0.05, tmin0: float = 0.05,
+                     eps0_mask: int = 0x4 | 0x1 | 0x2 | 0x20 | 0x10, outputs: bool = True):
+    """the reference's qsim/CSG path compiled for the CPU (ref_cpu_sim.cc): its own generation and
+    propagation with its CPU random generator (mt19937_64 per thread, so not the GPU streams) and
+    its nearest-sample mock textures; returns (photon (N,4,4), seq (N,2,2), seconds, threads)"""
+    L = C.CDLL(REF_CPU_SIM)
+    f = L.ref_cpu_sim_run
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p] * 4 + [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p] + \
+                 [C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_float, C.c_float, C.c_float,
+                                                            C.c_uint] + \
+                 [C.c_ulonglong, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+    node = np.ascontiguousarray(geom["node"], np.float32)
+    itra = geom.get("itra")
+    itra = np.ascontiguousarray(itra if itra is not None and len(itra) else np.zeros((1, 4, 4)), np.float32)
+    pl = _plan(geom.get("plan"))
+    inv, pin, pnode, pgb, pid = instance_pairs(geom)
+    bbox = np.ascontiguousarray(pair_world_boxes(geom, pin, pnode), np.float32)
+    bnd = np.ascontiguousarray(phys["bnd"], np.float32)
+    optical = np.ascontiguousarray(phys["optical"], np.uint32)
+    icdf = phys.get("icdf")
+    icdf = None if icdf is None else np.ascontiguousarray(icdf, np.float32)
+    gs = np.ascontiguousarray(gs, np.float32).reshape(-1, 6, 4)
+    N = int(gs.view(np.int32)[:, 0, 3].clip(0).sum())
+    photon = np.zeros((N, 4, 4), np.float32) if outputs else None
+    seq = np.zeros((N, 2, 2), np.uint64) if outputs else None
+    secs = C.c_double(0.0)
+    nt = f(_p(node), _p(itra), _p(pl), _p(inv), _p(pin), _p(pnode), _p(pgb), _p(pid), _p(bbox), len(pin),
+           _p(bnd), bnd.shape[0], bnd.shape[3], float(phys.get("wl_low", 60.0)), float(phys.get("wl_step", 1.0)), _p(optical),
+           _p(icdf), 0 if icdf is None else icdf.shape[1], 0 if icdf is None else icdf.shape[0], int(phys.get("hd_factor", 20)),
+           _p(gs), len(gs), N, max_bounce, max_time, tmin, tmin0, eps0_mask, seed, nthreads, _p(photon), _p(seq), C.byref(secs))
+    if nt < 0:
+        raise RuntimeError(f"ref_cpu_sim_run failed {nt}")
+    return photon, seq, secs.value, nt
 
 
 def have_ref_spm() -> bool:

@@ -1,0 +1,3 @@
+// TEST INFRASTRUCTURE ONLY: see glm.hpp
+#pragma once
+#include "../glm.hpp"
