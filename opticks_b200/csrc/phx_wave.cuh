@@ -58,19 +58,31 @@ struct WaveArgs {
 // needs: bit 31 of the stored q1.w carries the choice of tmin (the last flag against the epsilon0
 // mask), and the photon's own bit 31 of q1.w rides in bit 30 of the bounce word.  `first`: the
 // slot takes a new photon (its index is written once).
-PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L, bool first)
+// the slot's eight 16 B chunks of a path (PhxWaveSlot order)
+PHX_D void wave_pack(const WaveArgs& W, const PhxLane& L, float4 (&c)[8])
 {
-    PhxWaveSlot* o = W.slot + s;
     const PhxPhoton& p = L.p;
     const unsigned eps0 = (p.obf & W.A.C.eps0_mask) ? 0x80000000u : 0u;
-    o->q0 = make_float4(p.pos.x, p.pos.y, p.pos.z, p.time);
-    o->q1 = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float((p.hitcount_iindex & 0x7fffffffu) | eps0));
-    o->q2 = make_float4(p.pol.x, p.pol.y, p.pol.z, p.wavelength);
-    o->q3 = make_float4(__uint_as_float(p.obf), __uint_as_float(p.identity), __uint_as_float(p.index), __uint_as_float(p.flagmask));
-    o->ra = make_uint4(L.rng.d, L.rng.v[0], L.rng.v[1], L.rng.v[2]);
-    o->rb = make_uint4(L.rng.v[3], L.rng.v[4], (unsigned)L.bounce | ((p.hitcount_iindex >> 1) & 0x40000000u), (unsigned)L.ev);
-    o->his = make_ulonglong2(L.seqhis[0], L.seqhis[1]);
-    o->bnd = make_ulonglong2(L.seqbnd[0], L.seqbnd[1]);
+    c[0] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.time);
+    c[1] = make_float4(p.mom.x, p.mom.y, p.mom.z, __uint_as_float((p.hitcount_iindex & 0x7fffffffu) | eps0));
+    c[2] = make_float4(p.pol.x, p.pol.y, p.pol.z, p.wavelength);
+    c[3] = make_float4(__uint_as_float(p.obf), __uint_as_float(p.identity), __uint_as_float(p.index), __uint_as_float(p.flagmask));
+    c[4] = make_float4(__uint_as_float(L.rng.d), __uint_as_float(L.rng.v[0]), __uint_as_float(L.rng.v[1]), __uint_as_float(L.rng.v[2]));
+    c[5] = make_float4(__uint_as_float(L.rng.v[3]), __uint_as_float(L.rng.v[4]),
+                       __uint_as_float((unsigned)L.bounce | ((p.hitcount_iindex >> 1) & 0x40000000u)), __uint_as_float((unsigned)L.ev));
+    c[6] = make_float4(__uint_as_float((unsigned)L.seqhis[0]), __uint_as_float((unsigned)(L.seqhis[0] >> 32)),
+                       __uint_as_float((unsigned)L.seqhis[1]), __uint_as_float((unsigned)(L.seqhis[1] >> 32)));
+    c[7] = make_float4(__uint_as_float((unsigned)L.seqbnd[0]), __uint_as_float((unsigned)(L.seqbnd[0] >> 32)),
+                       __uint_as_float((unsigned)L.seqbnd[1]), __uint_as_float((unsigned)(L.seqbnd[1] >> 32)));
+}
+
+PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L, bool first)
+{
+    float4 c[8];
+    wave_pack(W, L, c);
+    float4* o = reinterpret_cast<float4*>(W.slot + s);
+#pragma unroll
+    for (int k = 0; k < 8; k++) o[k] = c[k];
     if (first) W.sidx[s] = L.idx;
 }
 
@@ -80,26 +92,90 @@ PHX_D float wave_tmin(const WaveArgs& W, const float4& q1)
     return (__float_as_uint(q1.w) & 0x80000000u) ? W.A.C.tmin0 : W.A.C.tmin;
 }
 
-PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
+// a path from its slot's eight 16 B chunks
+PHX_D void wave_unpack(const float4 (&c)[8], PhxLane& L)
 {
-    const PhxWaveSlot* o = W.slot + s;
-    const float4 q0 = o->q0, q1 = o->q1, q2 = o->q2, q3 = o->q3;
     PhxPhoton& p = L.p;
-    p.pos = make_float3(q0.x, q0.y, q0.z); p.time = q0.w;
-    p.mom = make_float3(q1.x, q1.y, q1.z);
-    p.pol = make_float3(q2.x, q2.y, q2.z); p.wavelength = q2.w;
-    p.obf = __float_as_uint(q3.x); p.identity = __float_as_uint(q3.y);
-    p.index = __float_as_uint(q3.z); p.flagmask = __float_as_uint(q3.w);
-    const uint4 ra = o->ra, rb = o->rb;
-    L.rng.d = ra.x; L.rng.v[0] = ra.y; L.rng.v[1] = ra.z; L.rng.v[2] = ra.w;
-    L.rng.v[3] = rb.x; L.rng.v[4] = rb.y;
+    p.pos = make_float3(c[0].x, c[0].y, c[0].z); p.time = c[0].w;
+    p.mom = make_float3(c[1].x, c[1].y, c[1].z);
+    p.pol = make_float3(c[2].x, c[2].y, c[2].z); p.wavelength = c[2].w;
+    p.obf = __float_as_uint(c[3].x); p.identity = __float_as_uint(c[3].y);
+    p.index = __float_as_uint(c[3].z); p.flagmask = __float_as_uint(c[3].w);
+    L.rng.d = __float_as_uint(c[4].x); L.rng.v[0] = __float_as_uint(c[4].y);
+    L.rng.v[1] = __float_as_uint(c[4].z); L.rng.v[2] = __float_as_uint(c[4].w);
+    L.rng.v[3] = __float_as_uint(c[5].x); L.rng.v[4] = __float_as_uint(c[5].y);
     L.rng.boxmuller_flag = 0; L.rng.boxmuller_flag_double = 0;
     L.rng.boxmuller_extra = 0.f; L.rng.boxmuller_extra_double = 0.0;
-    L.bounce = (int)(rb.z & 0x3fffffffu); L.ev = (int)rb.w;
-    p.hitcount_iindex = (__float_as_uint(q1.w) & 0x7fffffffu) | ((rb.z & 0x40000000u) << 1);
-    const ulonglong2 h = o->his, b = o->bnd;
-    L.seqhis[0] = h.x; L.seqhis[1] = h.y; L.seqbnd[0] = b.x; L.seqbnd[1] = b.y;
+    const unsigned bz = __float_as_uint(c[5].z);
+    L.bounce = (int)(bz & 0x3fffffffu); L.ev = (int)__float_as_uint(c[5].w);
+    p.hitcount_iindex = (__float_as_uint(c[1].w) & 0x7fffffffu) | ((bz & 0x40000000u) << 1);
+    L.seqhis[0] = (unsigned long long)__float_as_uint(c[6].x) | ((unsigned long long)__float_as_uint(c[6].y) << 32);
+    L.seqhis[1] = (unsigned long long)__float_as_uint(c[6].z) | ((unsigned long long)__float_as_uint(c[6].w) << 32);
+    L.seqbnd[0] = (unsigned long long)__float_as_uint(c[7].x) | ((unsigned long long)__float_as_uint(c[7].y) << 32);
+    L.seqbnd[1] = (unsigned long long)__float_as_uint(c[7].z) | ((unsigned long long)__float_as_uint(c[7].w) << 32);
+}
+
+PHX_D void wave_load(const WaveArgs& W, uint32_t s, PhxLane& L)
+{
+    const float4* o = reinterpret_cast<const float4*>(W.slot + s);
+    float4 c[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = o[k];
+    wave_unpack(c, L);
     L.idx = W.sidx[s];
+}
+
+// Slots of a whole warp moved through shared memory (`st`: 256 float4 of the warp's own): lane j
+// moves 16 B chunk j & 7 of the slot of lane 4k + (j >> 3), so one instruction reads or writes
+// four whole 128 B slots where per-lane accesses touch 16 B of 32 different slots.  Chunk c of
+// lane l's slot sits at st[8l + (c ^ (l & 7))], which keeps both sides free of bank conflicts.
+// Warp-collective; `take` selects the lanes whose slots move.
+PHX_D void wave_gather(const WaveArgs& W, float4* st, uint32_t s, bool take)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned c = lane & 7u;
+    const unsigned m = __ballot_sync(FULL, take);
+    const float4* src = reinterpret_cast<const float4*>(W.slot);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const unsigned l = 4u * (unsigned)k + (lane >> 3);
+        const uint32_t sl = __shfl_sync(FULL, s, (int)l);
+        if ((m >> l) & 1u) st[8u * l + (c ^ (l & 7u))] = src[(size_t)sl * 8u + c];
+    }
+    __syncwarp();
+}
+
+PHX_D void wave_scatter(const WaveArgs& W, float4* st, uint32_t s, bool take)
+{
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned c = lane & 7u;
+    const unsigned m = __ballot_sync(FULL, take);
+    __syncwarp();
+    float4* dst = reinterpret_cast<float4*>(W.slot);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const unsigned l = 4u * (unsigned)k + (lane >> 3);
+        const uint32_t sl = __shfl_sync(FULL, s, (int)l);
+        if ((m >> l) & 1u) dst[(size_t)sl * 8u + c] = st[8u * l + (c ^ (l & 7u))];
+    }
+    __syncwarp();
+}
+
+// this lane's slot chunks in the warp's staging area
+PHX_D void wave_stage_get(const float4* st, float4 (&c)[8])
+{
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = st[8u * lane + ((unsigned)k ^ (lane & 7u))];
+}
+
+PHX_D void wave_stage_put(float4* st, const float4 (&c)[8])
+{
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < 8; k++) st[8u * lane + ((unsigned)k ^ (lane & 7u))] = c[k];
 }
 
 // the 32 score terms and the refraction tangent (pos, mom, pol) of a path: PHX_WAVE_SCORE_F4 float4
@@ -131,6 +207,39 @@ PHX_D void wave_load_score(const WaveArgs& W, uint32_t s, PhxScore* sc)
 PHX_D void wave_score_setup(PhxScore& score, const PersistArgs& A)
 {
     score_setup(score, A);
+}
+
+// The slot kernels move whole warps of slots through shared memory (wave_gather / wave_scatter);
+// 0 gives per-lane 16 B accesses instead (the same bytes in the same places).
+#ifndef PHX_WAVE_STAGED
+#define PHX_WAVE_STAGED 1
+#endif
+
+// this warp's staging area (the slot kernels run 128-thread blocks), or null without staging
+PHX_D float4* wave_stage_area()
+{
+#if PHX_WAVE_STAGED
+    __shared__ float4 stage[128 * 8];
+    return stage + 256u * (threadIdx.x >> 5);
+#else
+    return nullptr;
+#endif
+}
+
+// a live path back into its slot (`first`: the slot took a new photon).  Warp-collective.
+PHX_D void wave_put(const WaveArgs& W, float4* st, uint32_t s, const PhxLane& L, bool live, bool first)
+{
+#if PHX_WAVE_STAGED
+    if (live) {
+        float4 c[8];
+        wave_pack(W, L, c);
+        wave_stage_put(st, c);
+        if (first) W.sidx[s] = L.idx;
+    }
+    wave_scatter(W, st, s, live);
+#else
+    if (live) wave_store(W, s, L, first);
+#endif
 }
 
 // a path may take another bounce (the loop condition of CSGOptiX/CSGOptiX7.cu:477)
@@ -214,22 +323,27 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
     return live;
 }
 
+// resident 128-thread blocks per SM asked for the generating kernels (k_wave_init, k_wave_fill;
+// not the adjoint forms)
+#ifndef PHX_WAVE_FILL_MINB
+#define PHX_WAVE_FILL_MINB 6
+#endif
+
 // fill the pool: every slot takes photons until it holds a live path or the queue is empty
 template <int CV, bool ADJ = false>
-__global__ void __launch_bounds__(128) k_wave_init(WaveArgs W)
+__global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_FILL_MINB) k_wave_init(WaveArgs W)
 {
     unsigned status = 0;
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
+    float4* st = wave_stage_area();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < W.pool; base += stride) {
         const long long s = base + (threadIdx.x & 31);
         const bool live = wave_refill<CV, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
-        if (live) {
-            wave_store(W, (uint32_t)s, L, true);
-            if (ADJ) wave_store_score(W, (uint32_t)s, &score);
-        }
+        wave_put(W, st, (uint32_t)s, L, live, true);
+        if (ADJ && live) wave_store_score(W, (uint32_t)s, &score);
         wave_append(W, live, (uint32_t)s);
     }
     if (status) atomicOr(W.A.status, status);
@@ -392,13 +506,14 @@ __global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
 // physics of every live path after its closest hit (CSGOptiX/CSGOptiX7.cu:491-509), finishing
 // and refilling slots; live slots go to the next round's list
 // resident 128-thread blocks per SM asked for the physics kernel (its loads of path state are
-// latency-bound, so occupancy matters more than registers)
+// latency-bound, so occupancy matters more than registers); the adjoint form carries the score
+// terms as well and is left to the compiler
 #ifndef PHX_WAVE_SHADE_MINB
-#define PHX_WAVE_SHADE_MINB 1
+#define PHX_WAVE_SHADE_MINB 7
 #endif
 
 template <int CV, bool ADJ = false>
-__global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
+__global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0 && W.trace_ctr) *W.trace_ctr = 0u;   // for the next round's closest-hit kernel
     const unsigned n = *W.n_in;
@@ -406,18 +521,28 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
+    float4* st = wave_stage_area();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
         const long long i = base + (threadIdx.x & 31);
         const bool valid = i < (long long)n;
-        uint32_t s = 0u;
+        const uint32_t s = valid ? W.act_in[i] : 0u;
         bool live = false;
+        float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint4 lgi = make_uint4(0u, 0u, 0u, 0u);
+        if (valid) { nd = W.prd[s].nd; lgi = W.prd[s].lgi; }     // in flight with the slot reads
+#if PHX_WAVE_STAGED
+        wave_gather(W, st, s, valid);
+#endif
         if (valid) {
-            s = W.act_in[i];
+#if PHX_WAVE_STAGED
+            float4 c[8];
+            wave_stage_get(st, c);
+            wave_unpack(c, L);           // the photon index is read only when the path finishes
+#else
             wave_load(W, s, L);
+#endif
             if (ADJ) wave_load_score(W, s, &score);
-            const float4 nd = W.prd[s].nd;
-            const uint4 lgi = W.prd[s].lgi;
             PhxPRD prd;
             prd.normal = make_float3(nd.x, nd.y, nd.z);
             prd.distance = nd.w;
@@ -437,13 +562,16 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
                 seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
                 done = command == PHX_BREAK || !wave_can_trace(L, W.A);
             }
-            if (done) persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
+            if (done) {
+#if PHX_WAVE_STAGED
+                L.idx = W.sidx[s];
+#endif
+                persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
+            }
             live = !done;
         }
-        if (live) {
-            wave_store(W, s, L, false);
-            if (ADJ) wave_store_score(W, s, &score);
-        }
+        wave_put(W, st, s, L, live, false);
+        if (ADJ && live) wave_store_score(W, s, &score);
         wave_append(W, live, s);
         wave_push(W.free_list, W.n_free, valid && !live, s);
     }
@@ -452,7 +580,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArg
 
 // new photons from the queue into the slots freed this round (warp-coherent generation)
 template <int CV, bool ADJ = false>
-__global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
+__global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_FILL_MINB) k_wave_fill(WaveArgs W)
 {
     const unsigned n = *W.n_free;
     if ((long long)*W.A.queue >= W.A.N) return;
@@ -460,16 +588,15 @@ __global__ void __launch_bounds__(128) k_wave_fill(WaveArgs W)
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
+    float4* st = wave_stage_area();
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
         const long long i = base + (threadIdx.x & 31);
         const bool valid = i < (long long)n;
         const uint32_t s = valid ? W.free_list[i] : 0u;
         const bool live = wave_refill<CV, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
-        if (live) {
-            wave_store(W, s, L, true);
-            if (ADJ) wave_store_score(W, s, &score);
-        }
+        wave_put(W, st, s, L, live, true);
+        if (ADJ && live) wave_store_score(W, s, &score);
         wave_append(W, live, s);
     }
     if (status) atomicOr(W.A.status, status);
