@@ -7,6 +7,11 @@
 #include "phx_physics.cuh"
 
 #define PHX_BVH_STACK 48
+// phx_visit_node orders the hit children with a sorting network on integer keys (0: insertion
+// sort on the distances)
+#ifndef PHX_VISIT_SORTNET
+#define PHX_VISIT_SORTNET 1
+#endif
 // leaf steps are taken when leaf-ready lanes x this weight >= node-ready lanes (or no node work is left)
 #ifndef PHX_TRACE_LEAF_WEIGHT
 #define PHX_TRACE_LEAF_WEIGHT 1
@@ -97,6 +102,36 @@ PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const fl
         tn[c] = tnear;
         if (cha[c] != 0 && tnear <= tfar * 1.00001f + 1e-4f) hitmask |= 1 << c;
     }
+#if PHX_VISIT_SORTNET
+    // order by a 4-key sorting network: key = the near distance's magnitude bits with the child
+    // slot in the two low bits, all ones for a missed child (sorts last).  For tnear >= 0 the bits
+    // order like the floats; the pushed distance itself is the exact tnear.
+    unsigned k0, k1, k2, k3;
+    {
+        unsigned kk[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            kk[c] = (hitmask >> c) & 1 ? ((__float_as_uint(tn[c]) & 0x7ffffffcu) | (unsigned)c) : 0xffffffffu;
+        k0 = kk[0]; k1 = kk[1]; k2 = kk[2]; k3 = kk[3];
+    }
+    unsigned t;
+    t = min(k0, k1); k1 = max(k0, k1); k0 = t;
+    t = min(k2, k3); k3 = max(k2, k3); k2 = t;
+    t = min(k0, k2); k2 = max(k0, k2); k0 = t;
+    t = min(k1, k3); k3 = max(k1, k3); k1 = t;
+    t = min(k1, k2); k2 = max(k1, k2); k1 = t;
+    const unsigned ks[4] = { k0, k1, k2, k3 };
+#pragma unroll
+    for (int j = 3; j >= 0; j--) {
+        const unsigned key = ks[j];
+        if (key == 0xffffffffu) continue;
+        if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
+        const unsigned c = key & 3u;
+        stk[sp] = c == 0u ? cha[0] : c == 1u ? cha[1] : c == 2u ? cha[2] : cha[3];
+        stt[sp] = c == 0u ? tn[0] : c == 1u ? tn[1] : c == 2u ? tn[2] : tn[3];
+        sp++;
+    }
+#else
     int order[4] = { 0, 1, 2, 3 };
 #pragma unroll
     for (int i = 1; i < 4; i++)
@@ -111,6 +146,7 @@ PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const fl
         if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
         stk[sp] = cha[c]; stt[sp] = tn[c]; sp++;
     }
+#endif
 }
 
 // ray set-up shared by both traversal loops: reciprocal direction (zero components nudged) and
