@@ -76,16 +76,6 @@ PHX_D void wave_pack(const WaveArgs& W, const PhxLane& L, float4 (&c)[8])
                        __uint_as_float((unsigned)L.seqbnd[1]), __uint_as_float((unsigned)(L.seqbnd[1] >> 32)));
 }
 
-PHX_D void wave_store(const WaveArgs& W, uint32_t s, const PhxLane& L, bool first)
-{
-    float4 c[8];
-    wave_pack(W, L, c);
-    float4* o = reinterpret_cast<float4*>(W.slot + s);
-#pragma unroll
-    for (int k = 0; k < 8; k++) o[k] = c[k];
-    if (first) W.sidx[s] = L.idx;
-}
-
 // the tmin of a slot's next closest hit, from its first sector
 PHX_D float wave_tmin(const WaveArgs& W, const float4& q1)
 {
@@ -209,27 +199,17 @@ PHX_D void wave_score_setup(PhxScore& score, const PersistArgs& A)
     score_setup(score, A);
 }
 
-// The slot kernels move whole warps of slots through shared memory (wave_gather / wave_scatter);
-// 0 gives per-lane 16 B accesses instead (the same bytes in the same places).
-#ifndef PHX_WAVE_STAGED
-#define PHX_WAVE_STAGED 1
-#endif
-
-// this warp's staging area (the slot kernels run 128-thread blocks), or null without staging
+// The slot kernels move whole warps of slots through shared memory (wave_gather / wave_scatter).
+// this warp's staging area: 256 float4 (the slot kernels run 128-thread blocks)
 PHX_D float4* wave_stage_area()
 {
-#if PHX_WAVE_STAGED
     __shared__ float4 stage[128 * 8];
     return stage + 256u * (threadIdx.x >> 5);
-#else
-    return nullptr;
-#endif
 }
 
 // a live path back into its slot (`first`: the slot took a new photon).  Warp-collective.
 PHX_D void wave_put(const WaveArgs& W, float4* st, uint32_t s, const PhxLane& L, bool live, bool first)
 {
-#if PHX_WAVE_STAGED
     if (live) {
         float4 c[8];
         wave_pack(W, L, c);
@@ -237,9 +217,6 @@ PHX_D void wave_put(const WaveArgs& W, float4* st, uint32_t s, const PhxLane& L,
         if (first) W.sidx[s] = L.idx;
     }
     wave_scatter(W, st, s, live);
-#else
-    if (live) wave_store(W, s, L, first);
-#endif
 }
 
 // a path may take another bounce (the loop condition of CSGOptiX/CSGOptiX7.cu:477)
@@ -512,6 +489,41 @@ __global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
 #define PHX_WAVE_SHADE_MINB 7
 #endif
 
+// the physics of one path whose slot is in the warp's staging area; true when it goes on
+template <int CV, bool ADJ>
+PHX_D bool wave_shade_path(const WaveArgs& W, const float4* st, uint32_t s, const float4 nd, const uint4 lgi, PhxLane& L,
+                           PhxScore* sc, unsigned& status)
+{
+    float4 c[8];
+    wave_stage_get(st, c);
+    wave_unpack(c, L);                   // the photon index is read only when the path finishes
+    if (ADJ) wave_load_score(W, s, sc);
+    PhxPRD prd;
+    prd.normal = make_float3(nd.x, nd.y, nd.z);
+    prd.distance = nd.w;
+    prd.lposcost = __uint_as_float(lgi.x);
+    prd.gp_bd = lgi.y;
+    prd.ii_id = lgi.z;
+    bool done = true;
+    if (prd.boundary() != 0xffffu) {
+        int command;
+        if (ADJ) {
+            prd.normal = normalize(prd.normal);
+            command = propagate<true>(L.p, L.rng, prd, W.A.P, status, sc);
+        } else {
+            command = phx_propagate_step(L.p, L.rng, prd, W.A.P, status);
+        }
+        L.bounce++;
+        seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
+        done = command == PHX_BREAK || !wave_can_trace(L, W.A);
+    }
+    if (done) {
+        L.idx = W.sidx[s];
+        persist_finish<CV, ADJ>(L, W.A, sc);
+    }
+    return !done;
+}
+
 template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
@@ -521,55 +533,19 @@ __global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_SHADE_MINB) k_wave_sha
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
-    float4* st = wave_stage_area();
+    const unsigned lane = threadIdx.x & 31u;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
-        const long long i = base + (threadIdx.x & 31);
+    long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    float4* st = wave_stage_area();
+    for (; base < (long long)n; base += stride) {
+        const long long i = base + lane;
         const bool valid = i < (long long)n;
         const uint32_t s = valid ? W.act_in[i] : 0u;
-        bool live = false;
         float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
         uint4 lgi = make_uint4(0u, 0u, 0u, 0u);
         if (valid) { nd = W.prd[s].nd; lgi = W.prd[s].lgi; }     // in flight with the slot reads
-#if PHX_WAVE_STAGED
         wave_gather(W, st, s, valid);
-#endif
-        if (valid) {
-#if PHX_WAVE_STAGED
-            float4 c[8];
-            wave_stage_get(st, c);
-            wave_unpack(c, L);           // the photon index is read only when the path finishes
-#else
-            wave_load(W, s, L);
-#endif
-            if (ADJ) wave_load_score(W, s, &score);
-            PhxPRD prd;
-            prd.normal = make_float3(nd.x, nd.y, nd.z);
-            prd.distance = nd.w;
-            prd.lposcost = __uint_as_float(lgi.x);
-            prd.gp_bd = lgi.y;
-            prd.ii_id = lgi.z;
-            bool done = true;
-            if (prd.boundary() != 0xffffu) {
-                int command;
-                if (ADJ) {
-                    prd.normal = normalize(prd.normal);
-                    command = propagate<true>(L.p, L.rng, prd, W.A.P, status, &score);
-                } else {
-                    command = phx_propagate_step(L.p, L.rng, prd, W.A.P, status);
-                }
-                L.bounce++;
-                seq_add_nibble(L.seqhis, L.seqbnd, (unsigned)L.bounce, L.p.flag(), L.p.boundary());
-                done = command == PHX_BREAK || !wave_can_trace(L, W.A);
-            }
-            if (done) {
-#if PHX_WAVE_STAGED
-                L.idx = W.sidx[s];
-#endif
-                persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
-            }
-            live = !done;
-        }
+        const bool live = valid && wave_shade_path<CV, ADJ>(W, st, s, nd, lgi, L, ADJ ? &score : nullptr, status);
         wave_put(W, st, s, L, live, false);
         if (ADJ && live) wave_store_score(W, s, &score);
         wave_append(W, live, s);
