@@ -78,7 +78,7 @@ PHX_D void phx_test_leaf(const PhxScene& S, const int4 L, const float4 ball, con
 
 // Visit BVH4 node ni: slab-test its four children against [tmin, tmax] and push the hit ones
 // (inner nodes and leaf ranges) far-to-near, so that the nearest is taken next.
-PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const float3& oi, float tmin, float tmax, int* stk, float* stt,
+PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const float3& oi, float tmin, float tmax, int2* stk,
                           int& sp, unsigned& status)
 {
     const float4* nf = reinterpret_cast<const float4*>(S.bvh + ni);
@@ -127,8 +127,8 @@ PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const fl
         if (key == 0xffffffffu) continue;
         if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
         const unsigned c = key & 3u;
-        stk[sp] = c == 0u ? cha[0] : c == 1u ? cha[1] : c == 2u ? cha[2] : cha[3];
-        stt[sp] = c == 0u ? tn[0] : c == 1u ? tn[1] : c == 2u ? tn[2] : tn[3];
+        stk[sp] = make_int2(c == 0u ? cha[0] : c == 1u ? cha[1] : c == 2u ? cha[2] : cha[3],
+                            __float_as_int(c == 0u ? tn[0] : c == 1u ? tn[1] : c == 2u ? tn[2] : tn[3]));
         sp++;
     }
 #else
@@ -144,7 +144,7 @@ PHX_D void phx_visit_node(const PhxScene& S, int ni, const float3& inv, const fl
         const int c = order[k];
         if (!(hitmask & (1 << c))) continue;
         if (sp >= PHX_BVH_STACK) { status |= PHX_STATUS_BVH_STACK; continue; }
-        stk[sp] = cha[c]; stt[sp] = tn[c]; sp++;
+        stk[sp] = make_int2(cha[c], __float_as_int(tn[c])); sp++;
     }
 #endif
 }
@@ -215,25 +215,24 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
     if (!S.bvh_empty && !phx_culled(S, o, d, tmin, B.t)) {
         float3 inv, oi;
         phx_ray_slabs(o, d, inv, oi);
-        int stk[PHX_BVH_STACK];
-        float stt[PHX_BVH_STACK];
+        int2 stk[PHX_BVH_STACK];     // node or leaf range, near distance bits
         int sp = 0;
-        stk[sp] = 0; stt[sp] = tmin; sp++;
+        stk[sp] = make_int2(0, __float_as_int(tmin)); sp++;
         // Each step the lanes of the warp that traverse together vote: either the lanes whose next
         // entry is an inner node visit it, or the lanes whose next entry is a leaf range test it.
         // Every lane still takes its own entries in its own near-first order; the vote only
         // gathers the expensive leaf tests into steps where many lanes run them.
         const unsigned mask = __activemask();
         for (;;) {
-            while (sp > 0 && stt[sp - 1] > B.t) sp--;
-            const bool leaf_top = sp > 0 && stk[sp - 1] < 0;
+            while (sp > 0 && __int_as_float(stk[sp - 1].y) > B.t) sp--;
+            const bool leaf_top = sp > 0 && stk[sp - 1].x < 0;
             const unsigned want_leaf = __ballot_sync(mask, leaf_top);
             const unsigned want_node = __ballot_sync(mask, sp > 0 && !leaf_top);
             if (!(want_leaf | want_node)) break;
             const bool leaf_step = want_node == 0u || __popc(want_leaf) * PHX_TRACE_LEAF_WEIGHT >= __popc(want_node);
             if (sp == 0 || leaf_top != leaf_step) continue;
             sp--;
-            const int ni = stk[sp];
+            const int ni = stk[sp].x;
             if (leaf_step) {
                 const int enc = -ni - 1;
                 const int first = enc >> 3;
@@ -243,7 +242,7 @@ PHX_D bool phx_trace(const PhxScene& S, const float3& o, const float3& d, float 
                                           B, status);
                 continue;
             }
-            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, stt, sp, status);
+            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, sp, status);
         }
     }
     phx_best_prd(S, B, prd);

@@ -381,8 +381,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
     float tmin = 0.f;
     PhxBest B;
     B.t = 0.f; B.L = make_int4(-1, 0, 0, 0); B.isect = make_float4(0.f, 0.f, 0.f, 0.f); B.lposcost = 0.f;
-    int stk[PHX_BVH_STACK];
-    float stt[PHX_BVH_STACK];
+    int2 stk[PHX_BVH_STACK];         // node or leaf range, near distance bits
     int sp = 0;
     for (;;) {
         // hand new rays to the idle lanes (at most a window and a fresh window per step)
@@ -414,7 +413,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
                 for (int g = 0; g < S.num_global; g++)
                     phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.globals + g)), __ldg(S.global_sph + g), o, d, tmin, B,
                                       status);
-                if (!S.bvh_empty && !phx_culled(S, o, d, tmin, B.t)) { stk[0] = 0; stt[0] = tmin; sp = 1; }
+                if (!S.bvh_empty && !phx_culled(S, o, d, tmin, B.t)) { stk[0] = make_int2(0, __float_as_int(tmin)); sp = 1; }
                 has = true;
             }
             wnext += take;
@@ -422,7 +421,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
         }
         // finish the rays whose stacks are empty
         if (has) {
-            while (sp > 0 && stt[sp - 1] > B.t) sp--;
+            while (sp > 0 && __int_as_float(stk[sp - 1].y) > B.t) sp--;
             if (sp == 0) {
                 PhxPRD prd;
                 phx_best_prd(S, B, prd);
@@ -431,7 +430,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
                 has = false;
             }
         }
-        const bool leaf_top = has && stk[sp - 1] < 0;
+        const bool leaf_top = has && stk[sp - 1].x < 0;
         const unsigned want_leaf = __ballot_sync(FULL, leaf_top);
         const unsigned want_node = __ballot_sync(FULL, has && !leaf_top);
         if (!(want_leaf | want_node)) {
@@ -442,7 +441,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
         const bool leaf_step = want_node == 0u || __popc(want_leaf) * PHX_TRACE_LEAF_WEIGHT >= __popc(want_node);
         if (!has || leaf_top != leaf_step) continue;
         sp--;
-        const int ni = stk[sp];
+        const int ni = stk[sp].x;
         if (leaf_step) {
             const int enc = -ni - 1;
             const int first = enc >> 3;
@@ -450,7 +449,7 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
             for (int li = first; li < first + count; li++)
                 phx_test_leaf<CV>(S, __ldg(reinterpret_cast<const int4*>(S.leaves + li)), __ldg(S.leaf_sph + li), o, d, tmin, B, status);
         } else {
-            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, stt, sp, status);
+            phx_visit_node(S, ni, inv, oi, tmin, B.t, stk, sp, status);
         }
     }
     if (status) atomicOr(W.A.status, status);
