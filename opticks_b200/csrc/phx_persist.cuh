@@ -120,8 +120,40 @@ struct PhxLane {
     int ev;
 };
 
-// the XORWOW state of RNG slot `slot` advanced by skipahead(event * skip) (qudarap/qrng.h:85-90)
-PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, long long slot, unsigned long long ev, unsigned& status)
+// the 4-bit group tables of a single-event jump matrix staged in shared memory as five word planes
+// (plane w holds word w of every entry), so a warp's 32 lookups in one group read 16 consecutive
+// words of each plane: no bank conflicts.  The same entries are XOR-ed as by phx_rng_jump4.
+#define PHX_JUMP_PLANE (PHX_JUMP_BITS / 4 * 16)
+PHX_D void phx_jump_planes_load(uint32_t* P, const uint32_t* __restrict__ T)
+{
+    for (int i = threadIdx.x; i < 5 * PHX_JUMP_PLANE; i += blockDim.x) {
+        const int w = i / PHX_JUMP_PLANE, e = i - w * PHX_JUMP_PLANE;
+        P[i] = __ldg(T + (size_t)e * PHX_JUMP_COLW + w);
+    }
+}
+
+PHX_D void phx_rng_jump4_planes(curandStateXORWOW& s, const uint32_t* P, unsigned long long n)
+{
+    uint32_t o0 = 0u, o1 = 0u, o2 = 0u, o3 = 0u, o4 = 0u;
+    const uint32_t in[5] = { s.v[0], s.v[1], s.v[2], s.v[3], s.v[4] };
+#pragma unroll 1
+    for (int w = 0; w < 5; w++) {
+        const uint32_t x = in[w];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int e = (8 * w + q) * 16 + (int)((x >> (4 * q)) & 15u);
+            o0 ^= P[e]; o1 ^= P[PHX_JUMP_PLANE + e]; o2 ^= P[2 * PHX_JUMP_PLANE + e];
+            o3 ^= P[3 * PHX_JUMP_PLANE + e]; o4 ^= P[4 * PHX_JUMP_PLANE + e];
+        }
+    }
+    s.v[0] = o0; s.v[1] = o1; s.v[2] = o2; s.v[3] = o3; s.v[4] = o4;
+    s.d += (unsigned int)((362437ull * n) & 0xffffffffull);
+}
+
+// the XORWOW state of RNG slot `slot` advanced by skipahead(event * skip) (qudarap/qrng.h:85-90);
+// `planes`: the single-event group tables staged in shared memory, or null
+PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, long long slot, unsigned long long ev, unsigned& status,
+                         const uint32_t* planes = nullptr)
 {
     if (slot < A.rng_slots) {
         phx_load_rng(s, A.rng, A.rng_slots, slot);
@@ -131,14 +163,16 @@ PHX_D void phx_event_rng(curandStateXORWOW& s, const PersistArgs& A, int gi, lon
         curand_init(A.seed, (unsigned long long)slot, A.rng_offset, &s);
     }
     if (ev > 0ull) {
-        if (A.jump4) phx_rng_jump4(s, A.jump4 + (A.gs_event ? (size_t)gi * PHX_JUMP_NIBW : 0), A.skip * ev);
+        if (planes) phx_rng_jump4_planes(s, planes, A.skip * ev);
+        else if (A.jump4) phx_rng_jump4(s, A.jump4 + (A.gs_event ? (size_t)gi * PHX_JUMP_NIBW : 0), A.skip * ev);
         else if (A.jump) phx_rng_jump(s, A.jump + (A.gs_event ? (size_t)gi * PHX_JUMP_MATW : 0), A.skip * ev);
         else skipahead(A.skip * ev, &s);
     }
 }
 
 template <int CV, bool ADJ>
-PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status, PhxScore* sc)
+PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsigned& status, PhxScore* sc,
+                         const uint32_t* planes = nullptr)
 {
     if (ADJ) {
 #pragma unroll
@@ -159,7 +193,7 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
     if (A.ev_rng) {
         phx_load_rng(L.rng, A.ev_rng, A.ev_rng_n, idx);
     } else {
-        phx_event_rng(L.rng, A, gi, slot, ev, status);
+        phx_event_rng(L.rng, A, gi, slot, ev, status, planes);
     }
     memset(&L.p, 0, sizeof(L.p));
     generate_photon(L.p, L.rng, g, (unsigned long long)slot, A.P, status);

@@ -274,7 +274,8 @@ __global__ void k_wave_act(uint32_t* bits, long long nword, const uint32_t* word
 // (photons that cannot take a first bounce are finished at once) or the queue is empty.
 // Returns true in the lanes that hold a live path.  Warp-collective.
 template <int CV, bool ADJ = false>
-PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status, PhxScore* sc = nullptr)
+PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& status, PhxScore* sc = nullptr,
+                       const uint32_t* planes = nullptr)
 {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
@@ -291,13 +292,24 @@ PHX_D bool wave_refill(PhxLane& L, const PersistArgs& A, bool need, unsigned& st
             if (idx >= A.N) {
                 need = false;
             } else {
-                persist_start<CV, ADJ>(L, A, idx, status, sc);
+                persist_start<CV, ADJ>(L, A, idx, status, sc, planes);
                 if (wave_can_trace(L, A)) { live = true; need = false; }
                 else persist_finish<CV, ADJ>(L, A, sc);
             }
         }
     }
     return live;
+}
+
+// the generating kernels' copy of a single-event jump table (block-collective; null when the call
+// advances its states some other way)
+PHX_D const uint32_t* wave_jump_planes(const PersistArgs& A)
+{
+    __shared__ uint32_t planes[5 * PHX_JUMP_PLANE];
+    if (!A.jump4 || A.gs_event || A.ev_rng || A.event_index == 0ull) return nullptr;
+    phx_jump_planes_load(planes, A.jump4);
+    __syncthreads();
+    return planes;
 }
 
 // resident 128-thread blocks per SM asked for the generating kernels (k_wave_init, k_wave_fill;
@@ -315,10 +327,11 @@ __global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_FILL_MINB) k_wave_init
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
     float4* st = wave_stage_area();
+    const uint32_t* planes = wave_jump_planes(W.A);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < W.pool; base += stride) {
         const long long s = base + (threadIdx.x & 31);
-        const bool live = wave_refill<CV, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr);
+        const bool live = wave_refill<CV, ADJ>(L, W.A, s < W.pool, status, ADJ ? &score : nullptr, planes);
         wave_put(W, st, (uint32_t)s, L, live, true);
         if (ADJ && live) wave_store_score(W, (uint32_t)s, &score);
         wave_append(W, live, (uint32_t)s);
@@ -558,18 +571,23 @@ template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_FILL_MINB) k_wave_fill(WaveArgs W)
 {
     const unsigned n = *W.n_free;
-    if ((long long)*W.A.queue >= W.A.N) return;
+    // the whole block leaves or stays (other blocks move the queue head meanwhile)
+    __shared__ int drained;
+    if (threadIdx.x == 0) drained = (long long)*W.A.queue >= W.A.N;
+    __syncthreads();
+    if (drained) return;
     unsigned status = 0;
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
     float4* st = wave_stage_area();
+    const uint32_t* planes = wave_jump_planes(W.A);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < (long long)n; base += stride) {
         const long long i = base + (threadIdx.x & 31);
         const bool valid = i < (long long)n;
         const uint32_t s = valid ? W.free_list[i] : 0u;
-        const bool live = wave_refill<CV, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr);
+        const bool live = wave_refill<CV, ADJ>(L, W.A, valid, status, ADJ ? &score : nullptr, planes);
         wave_put(W, st, s, L, live, true);
         if (ADJ && live) wave_store_score(W, s, &score);
         wave_append(W, live, s);
