@@ -2,9 +2,12 @@
 //
 // The reference hands one AABB per CSGPrim to OptiX (CSGOptiX/GAS_Builder.cc:112-130) and
 // one instance per qat4 transform (CSGOptiX/SBT.cc:393-460); OptiX builds the hierarchy.
-// Here every (instance, prim) pair becomes one leaf with a world-space box, a binned-SAH
-// binary BVH is built over the leaves and collapsed to 4-wide nodes whose child boxes are
-// stored per axis (phx_bvh4_node) so the traversal tests four boxes with coalesced loads.
+// Here every (instance, prim) pair becomes one leaf with a world-space box (the corner box of the
+// prim's box under the instance transform, overlapped with a box built from the prim's CSG tree
+// when the engine supplies one: a tilted PMT's cap and neck bound it far more tightly than its
+// whole box does), a binned-SAH binary BVH is built over the leaves and collapsed to 4-wide nodes
+// whose child boxes are stored per axis (phx_bvh4_node) so the traversal tests four boxes with
+// coalesced loads.
 // Boxes are padded so that FP32 slab tests never cull a leaf that the CSG intersector hits.
 #include "phx_bvh.h"
 #include <algorithm>
@@ -166,6 +169,13 @@ int phx_build_bvh4(const std::vector<PhxLeafInput>& in, PhxBvh4Result& out, doub
     Box scene;
     for (int i = 0; i < n_all; i++) {
         Box b = world_box(in[i].bbox, in[i].xform);
+        if (in[i].has_wbox) {
+            Box t = b;
+            for (int k = 0; k < 3; k++) { t.lo[k] = std::max(b.lo[k], in[i].wbox[k]); t.hi[k] = std::min(b.hi[k], in[i].wbox[3 + k]); }
+            bool ok = true;
+            for (int k = 0; k < 3; k++) ok = ok && t.lo[k] <= t.hi[k];
+            if (ok) b = t;
+        }
         // pad: relative to extent and to coordinate magnitude so FP32 slabs stay conservative
         double ext = std::max(b.hi[0] - b.lo[0], std::max(b.hi[1] - b.lo[1], b.hi[2] - b.lo[2]));
         double mag = 0.0;

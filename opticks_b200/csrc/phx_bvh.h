@@ -7,6 +7,8 @@ struct PhxLeafInput {
     float bbox[6];      // prim box in the instance (object) frame : mn.xyz, mx.xyz
     float xform[16];    // instance transform, row-vector convention (rows q0..q3), object -> world
     float sphere[4];    // world-space bounding sphere of the leaf: centre xyz, radius
+    double wbox[6];     // a world box from the prim's CSG tree (lo xyz, hi xyz), when has_wbox
+    int has_wbox;       //   the leaf's box is the overlap of this and the prim box's corner box
     phx_leaf leaf;
 };
 

@@ -549,7 +549,7 @@ static PhxSph node_sphere(const phx_geometry* geo, int no, int i, int num)
             break;
         case PHX_CSG_CYLINDER: {
             const double r = q[3], z1 = q[4], z2 = q[5];
-            s = { { q[0], q[1], 0.5 * (z1 + z2) }, std::sqrt(r * r + 0.25 * (z2 - z1) * (z2 - z1)) };
+            s = { { 0, 0, 0.5 * (z1 + z2) }, std::sqrt(r * r + 0.25 * (z2 - z1) * (z2 - z1)) };   // axis on local z
             break;
         }
         case PHX_CSG_BOX3:
@@ -663,6 +663,117 @@ static PhxSph prim_sphere(const phx_geometry* geo, int p)
     b.r = std::sqrt(h2);
     const PhxSph t = node_sphere(geo, no, 0, std::max(1, nn));
     return t.r < b.r ? t : b;
+}
+
+// World box of node i of a prim's tree under the instance matrix `inst` (row-vector, object ->
+// world), tighter than the corner box of the prim's box: each leaf's own bounds (the exact box of a
+// sphere, and of a cylinder's disc swept along its axis, under an affine map; the corner box of a
+// box3 and of a zsphere's z slab, the zsphere's clipped to its sphere's) through its node transform
+// and the instance, combined as the operators combine point sets (union: union; intersection:
+// overlap; difference: the first operand).  false: a complemented or unhandled leaf, or an empty
+// overlap; the caller keeps the prim's box then.
+struct PhxBox {
+    double lo[3], hi[3];
+};
+
+static void mat_mul_rows(const double* a, const double* b, double* o)   // o = a b (4x4)
+{
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) o[r * 4 + c] = a[r * 4 + 0] * b[0 * 4 + c] + a[r * 4 + 1] * b[1 * 4 + c] + a[r * 4 + 2] * b[2 * 4 + c] + a[r * 4 + 3] * b[3 * 4 + c];
+}
+
+static void box_of_corners(const double* lo, const double* hi, const double* m, PhxBox& b)
+{
+    for (int k = 0; k < 3; k++) { b.lo[k] = 1e300; b.hi[k] = -1e300; }
+    for (int i = 0; i < 8; i++) {
+        const double p[3] = { (i & 1) ? hi[0] : lo[0], (i & 2) ? hi[1] : lo[1], (i & 4) ? hi[2] : lo[2] };
+        for (int k = 0; k < 3; k++) {
+            const double w = p[0] * m[0 * 4 + k] + p[1] * m[1 * 4 + k] + p[2] * m[2 * 4 + k] + m[3 * 4 + k];
+            b.lo[k] = std::min(b.lo[k], w);
+            b.hi[k] = std::max(b.hi[k], w);
+        }
+    }
+}
+
+static bool node_box(const phx_geometry* geo, int no, int i, int num, const double* inst, PhxBox& out)
+{
+    if (i >= num || no + i >= geo->num_node) return false;
+    const float* q = geo->node + 16 * (size_t)(no + i);
+    uint32_t tc, tw;
+    memcpy(&tc, q + 14, 4);
+    memcpy(&tw, q + 15, 4);
+    if (tc == PHX_CSG_UNION || tc == PHX_CSG_INTERSECTION || tc == PHX_CSG_DIFFERENCE) {
+        PhxBox a, b;
+        if (!node_box(geo, no, 2 * i + 1, num, inst, a)) return false;
+        if (tc == PHX_CSG_DIFFERENCE) { out = a; return true; }
+        if (!node_box(geo, no, 2 * i + 2, num, inst, b)) return false;
+        for (int k = 0; k < 3; k++) {
+            out.lo[k] = tc == PHX_CSG_UNION ? std::min(a.lo[k], b.lo[k]) : std::max(a.lo[k], b.lo[k]);
+            out.hi[k] = tc == PHX_CSG_UNION ? std::max(a.hi[k], b.hi[k]) : std::min(a.hi[k], b.hi[k]);
+            if (!(out.lo[k] <= out.hi[k])) return false;
+        }
+        return true;
+    }
+    if (tw & 0x80000000u) return false;
+    double m[16];
+    const uint32_t g = tw & 0x7fffffffu;
+    if (g > 0) {
+        if ((int)g > geo->num_itra || !geo->itra) return false;
+        float fwd[16];
+        if (!invert_affine(geo->itra + 16 * (size_t)(g - 1), fwd)) return false;
+        double f[16];
+        for (int k = 0; k < 16; k++) f[k] = fwd[k];
+        mat_mul_rows(f, inst, m);
+    } else {
+        memcpy(m, inst, sizeof(m));
+    }
+    // half extent along world axis k of a unit ball / unit disc in the local xy plane
+    double ball[3], disc[3];
+    for (int k = 0; k < 3; k++) {
+        disc[k] = std::sqrt(m[0 * 4 + k] * m[0 * 4 + k] + m[1 * 4 + k] * m[1 * 4 + k]);
+        ball[k] = std::sqrt(disc[k] * disc[k] + m[2 * 4 + k] * m[2 * 4 + k]);
+    }
+    auto at = [&](double x, double y, double z, int k) { return x * m[0 * 4 + k] + y * m[1 * 4 + k] + z * m[2 * 4 + k] + m[3 * 4 + k]; };
+    switch (tc) {
+        case PHX_CSG_SPHERE:
+        case PHX_CSG_ZSPHERE: {
+            const double r = std::fabs((double)q[3]);
+            for (int k = 0; k < 3; k++) {
+                const double c = at(q[0], q[1], q[2], k);
+                out.lo[k] = c - r * ball[k];
+                out.hi[k] = c + r * ball[k];
+            }
+            if (tc == PHX_CSG_ZSPHERE) {
+                const double lo[3] = { q[0] - r, q[1] - r, q[2] + std::min(q[4], q[5]) };
+                const double hi[3] = { q[0] + r, q[1] + r, q[2] + std::max(q[4], q[5]) };
+                PhxBox s;
+                box_of_corners(lo, hi, m, s);
+                for (int k = 0; k < 3; k++) {
+                    out.lo[k] = std::max(out.lo[k], s.lo[k]);
+                    out.hi[k] = std::min(out.hi[k], s.hi[k]);
+                    if (!(out.lo[k] <= out.hi[k])) return false;
+                }
+            }
+            return true;
+        }
+        case PHX_CSG_CYLINDER: {
+            const double r = std::fabs((double)q[3]);
+            for (int k = 0; k < 3; k++) {
+                const double c1 = at(0.0, 0.0, q[4], k), c2 = at(0.0, 0.0, q[5], k);
+                out.lo[k] = std::min(c1, c2) - r * disc[k];
+                out.hi[k] = std::max(c1, c2) + r * disc[k];
+            }
+            return true;
+        }
+        case PHX_CSG_BOX3: {
+            const double lo[3] = { -0.5 * std::fabs((double)q[0]), -0.5 * std::fabs((double)q[1]), -0.5 * std::fabs((double)q[2]) };
+            const double hi[3] = { -lo[0], -lo[1], -lo[2] };
+            box_of_corners(lo, hi, m, out);
+            return true;
+        }
+        default:
+            return false;
+    }
 }
 
 // QPlanck's table (qudarap/QPlanck.cc:36-48): sblackbody<double>(4096, 4096, 6500 K, 80 nm, 800 nm)
@@ -971,6 +1082,12 @@ int phx_create(const phx_geometry* geo, const phx_physics* phys, const phx_confi
             {
                 double md[16];
                 for (int k = 0; k < 16; k++) md[k] = m[k];
+                int32_t nn, no;
+                memcpy(&nn, pr + 0, 4);
+                memcpy(&no, pr + 1, 4);
+                PhxBox tb;
+                L.has_wbox = node_box(geo, no, 0, std::max(1, nn), md, tb) ? 1 : 0;
+                for (int k = 0; k < 3; k++) { L.wbox[k] = L.has_wbox ? tb.lo[k] : 0.0; L.wbox[3 + k] = L.has_wbox ? tb.hi[k] : 0.0; }
                 const PhxSph w = sph_transform(psph[p], md);
                 const double cn = std::sqrt(w.c[0] * w.c[0] + w.c[1] * w.c[1] + w.c[2] * w.c[2]);
                 // pad: relative, plus absolute for FP32 rays at these coordinates (never excludes a hit)
