@@ -15,11 +15,17 @@
 #include <cstring>
 #include <limits>
 
-// SAH build parameters: centroid bins per axis, largest leaf range a node may keep, and the cost of
-// visiting a node relative to one leaf test (0: split whenever the SAH sum does not grow).  On
+// SAH build parameters: centroid bins per axis (for nodes above PHX_BVH_EXACT_MAX leaves), largest
+// leaf range a node may keep, and the cost of visiting a node relative to one leaf test (0: split
+// whenever the SAH sum does not grow).  On
 // the 17,612-PMT detector the tree splits down to single leaves for any of these settings.
 #ifndef PHX_BVH_BINS
-#define PHX_BVH_BINS 16
+#define PHX_BVH_BINS 64
+#endif
+// nodes of at most this many leaves take the exact SAH sweep (all split positions) instead of bins;
+// the sweep sorts each axis, so it is kept for the lower levels of very large scenes
+#ifndef PHX_BVH_EXACT_MAX
+#define PHX_BVH_EXACT_MAX 65536
 #endif
 #ifndef PHX_BVH_MAX_LEAF
 #define PHX_BVH_MAX_LEAF 4
@@ -57,6 +63,49 @@ struct Builder {
     std::vector<Node2> nodes;
     int max_leaf = PHX_BVH_MAX_LEAF;
 
+    // Exact SAH: every split between consecutive centroids along each axis (prefix and suffix box
+    // areas over the sorted leaves); a node of one leaf, or of at most max_leaf leaves whose split
+    // does not lower the cost, stays a leaf range.
+    int split_exact(int me, int first, int count, int depth)
+    {
+        double best_cost = std::numeric_limits<double>::infinity();
+        int best_axis = -1, best_pos = -1;
+        std::vector<int> ord(idx.begin() + first, idx.begin() + first + count);
+        std::vector<double> right_area((size_t)count + 1, 0.0);
+        for (int ax = 0; ax < 3; ax++) {
+            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cent[3 * a + ax] < cent[3 * b + ax]; });
+            Box r;
+            for (int k = count - 1; k >= 1; k--) { r.grow(boxes[ord[k]]); right_area[k] = r.area(); }
+            Box l;
+            for (int k = 1; k < count; k++) {      // left = ord[0, k), right = ord[k, count)
+                l.grow(boxes[ord[k - 1]]);
+                const double cost = l.area() * k + right_area[k] * (count - k);
+                if (cost < best_cost) { best_cost = cost; best_axis = ax; best_pos = k; }
+            }
+        }
+        const double leaf_cost = nodes[me].box.area() * count;
+        best_cost += PHX_BVH_TRAV_COST * nodes[me].box.area();
+        if (best_axis < 0 || (count <= max_leaf && best_cost >= leaf_cost)) {
+            if (count <= max_leaf || best_axis < 0) {
+                if (count > max_leaf) {
+                    const int half = count / 2;
+                    const int l = build(first, half, depth + 1);
+                    const int r = build(first + half, count - half, depth + 1);
+                    nodes[me].left = l; nodes[me].right = r;
+                    return me;
+                }
+                nodes[me].first = first; nodes[me].count = count;
+                return me;
+            }
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cent[3 * a + best_axis] < cent[3 * b + best_axis]; });
+        std::copy(ord.begin(), ord.end(), idx.begin() + first);
+        const int l = build(first, best_pos, depth + 1);
+        const int r = build(first + best_pos, count - best_pos, depth + 1);
+        nodes[me].left = l; nodes[me].right = r;
+        return me;
+    }
+
     int build(int first, int count, int depth)
     {
         Node2 n;
@@ -70,17 +119,18 @@ struct Builder {
         const int NB = PHX_BVH_BINS;
         double best_cost = std::numeric_limits<double>::infinity();
         int best_axis = -1, best_split = -1;
+        if (NB <= 0 || count <= PHX_BVH_EXACT_MAX) return split_exact(me, first, count, depth);
         for (int ax = 0; ax < 3; ax++) {
             double lo = cb.lo[ax], hi = cb.hi[ax];
             if (!(hi > lo)) continue;
-            Box bb[NB]; int bc[NB] = {0};
+            Box bb[PHX_BVH_BINS > 0 ? PHX_BVH_BINS : 1]; int bc[PHX_BVH_BINS > 0 ? PHX_BVH_BINS : 1] = {0};
             double scale = NB / (hi - lo);
             for (int i = first; i < first + count; i++) {
                 int b = (int)((cent[3 * idx[i] + ax] - lo) * scale);
                 b = std::min(NB - 1, std::max(0, b));
                 bc[b]++; bb[b].grow(boxes[idx[i]]);
             }
-            Box lb[NB]; int lc[NB];
+            Box lb[PHX_BVH_BINS > 0 ? PHX_BVH_BINS : 1]; int lc[PHX_BVH_BINS > 0 ? PHX_BVH_BINS : 1];
             Box acc; int ac = 0;
             for (int b = 0; b < NB; b++) { acc.grow(bb[b]); ac += bc[b]; lb[b] = acc; lc[b] = ac; }
             Box racc; int rc = 0;
