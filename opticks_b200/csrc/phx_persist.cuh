@@ -105,11 +105,46 @@ PHX_STEPFN_T PhxPRD phx_trace_step(const PhxScene S, const float3 o, const float
 }
 
 // the PRD normal is normalised here (CSGOptiX/CSGOptiX7.cu:491-498) as part of the shared step
+#ifndef PHX_PROP_IO
+#define PHX_PROP_IO 1
+#endif
+#if PHX_PROP_IO
+// The photon and its RNG state go in and come back by value: the out-of-line step then takes no
+// address of the caller's copies, which stay in registers (by reference they live in local
+// memory for the whole caller).  Every caller shares this one compiled step.
+struct PhxStepIO {
+    PhxPhoton p;
+    curandStateXORWOW rng;
+    unsigned status;
+    int command;
+};
+PHX_STEPFN_P PhxStepIO phx_propagate_io(PhxStepIO io, PhxPRD prd, const PhxProps P)
+{
+    prd.normal = normalize(prd.normal);
+    io.command = propagate<false>(io.p, io.rng, prd, P, io.status, nullptr);
+    return io;
+}
+
+PHX_D int phx_propagate_step(PhxPhoton& p, curandStateXORWOW& rng, PhxPRD prd, const PhxProps& P, unsigned& status)
+{
+    PhxStepIO io;
+    io.p = p;
+    io.rng = rng;
+    io.status = 0u;
+    io.command = 0;
+    io = phx_propagate_io(io, prd, P);
+    p = io.p;
+    rng = io.rng;
+    status |= io.status;
+    return io.command;
+}
+#else
 PHX_STEPFN_P int phx_propagate_step(PhxPhoton& p, curandStateXORWOW& rng, PhxPRD prd, const PhxProps P, unsigned& status)
 {
     prd.normal = normalize(prd.normal);
     return propagate<false>(p, rng, prd, P, status, nullptr);
 }
+#endif
 
 struct PhxLane {
     PhxPhoton p;
