@@ -56,12 +56,12 @@ BYTES_PER_PHOTON_FIXED = 48 + 64 + 32
 SAMPLE_PER_GENSTEP = 30        # CPU sample: this many photons of every genstep of the event
 # DRAM bytes (read + write) of all kernels of one simulate call of this 10M-photon event, from a
 # one-pass ncu capture of the bench's own launches (profiles/launches_dram_wavefront_detector_10M.md)
-DRAM_TRAFFIC = {"bytes_per_call": 19.131e9, "photons": 10_000_000,
+DRAM_TRAFFIC = {"bytes_per_call": 18.807e9, "photons": 10_000_000,
                 "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 32 launches of one "
                           "10M-photon simulate call of this workload (profiles/launches_dram_wavefront_detector_10M.md)"}
-# issue figures of the dominant kernel (k_wave_trace_df, 63 % of the step) from its ncu --set full
+# issue figures of the dominant kernel (k_wave_trace_df, 56 % of the step) from its ncu --set full
 # capture (profiles/k_wave_trace_df_detector_2M_ncu_full.md)
-ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.63, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
+ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.56, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
          "warps_active": 0.185, "lane_issue_frac": 0.376 * 11.90 / 32,
          "source": "profiles/k_wave_trace_df_detector_2M_ncu_full.md"}
 
