@@ -1409,7 +1409,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st, b
         if (!done && queue_done && (long long)live <= e->cfg.wave_tail) {
             // few paths left and none queued: finish them in one kernel
             W.act_in = act[cur]; W.n_in = cnt[cur];
-            k_wave_tail<CV, ADJ><<<(unsigned)((live + 127) / 128), 128, 0, st>>>(W);
+            k_wave_tail<CV, ADJ><<<(unsigned)std::min<long long>(g_tail[dev], (live + 127) / 128), 128, 0, st>>>(W);
             PHX_CU(cudaGetLastError());
             e->last_tail = 1;
             nl += 1;

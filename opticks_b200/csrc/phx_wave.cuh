@@ -468,26 +468,47 @@ __global__ void __launch_bounds__(128, PHX_WAVE_TRACE_MINB) k_wave_trace_df(Wave
     if (status) atomicOr(W.A.status, status);
 }
 
-// The last live paths of a call, once few remain and no photons wait in the queue: each thread
-// takes one path and runs its remaining bounces to the end with the one-kernel loop's step
-// (persist_step: the shared closest-hit and physics code), so a long chain no longer costs two
-// launches per bounce.  Photons, seq and hits are the same as the rounds would give.
+// The last live paths of a call, once few remain and no photons wait in the queue: persistent
+// warps run them to the end with the one-kernel loop's step (persist_step: the shared closest-hit
+// and physics code), so a long chain no longer costs two launches per bounce.  A lane whose path
+// ends takes the next one of the list at once (one atomic per warp on the round's ray counter,
+// which the physics kernel left at zero), so the lanes of a warp do not wait for its longest path.
+// Photons, seq and hits are the same as the rounds would give.
 template <int CV, bool ADJ = false>
 __global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
 {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31u;
     const unsigned n = *W.n_in;
     unsigned status = 0;
     PhxLane L;
     PhxScore score;
     if (ADJ) wave_score_setup(score, W.A);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)n; i += stride) {
-        const uint32_t s = W.act_in[i];
-        wave_load(W, s, L);
-        if (ADJ) wave_load_score(W, s, &score);
-        for (int b = 0; b <= W.A.C.max_bounce + 1; b++)        // persist_step ends the path within max_bounce
-            if (persist_step<CV, ADJ>(L, W.A, status, ADJ ? &score : nullptr)) break;
-        persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
+    bool has = false, drained = false;
+    for (;;) {
+        const unsigned idle = drained ? 0u : __ballot_sync(FULL, !has);
+        if (idle) {
+            const unsigned leader = __ffs(idle) - 1u;
+            unsigned base = 0u;
+            if (lane == leader) base = atomicAdd(W.trace_ctr, (unsigned)__popc(idle));
+            base = __shfl_sync(FULL, base, (int)leader);
+            if (base >= n) drained = true;
+            if (!has) {
+                const unsigned k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    const uint32_t s = W.act_in[k];
+                    wave_load(W, s, L);
+                    if (ADJ) wave_load_score(W, s, &score);
+                    has = true;
+                }
+            }
+        }
+        if (!__any_sync(FULL, has)) break;
+        // persist_step ends a path within max_bounce steps
+        if (has && persist_step<CV, ADJ>(L, W.A, status, ADJ ? &score : nullptr)) {
+            persist_finish<CV, ADJ>(L, W.A, ADJ ? &score : nullptr);
+            has = false;
+        }
     }
     if (status) atomicOr(W.A.status, status);
 }
