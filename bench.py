@@ -33,6 +33,7 @@ ranks (genstep slices) and gathers its hits and sensor counts over NCCL.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -56,14 +57,14 @@ BYTES_PER_PHOTON_FIXED = 48 + 64 + 32
 SAMPLE_PER_GENSTEP = 30        # CPU sample: this many photons of every genstep of the event
 # DRAM bytes (read + write) of all kernels of one simulate call of this 10M-photon event, from a
 # one-pass ncu capture of the bench's own launches (profiles/launches_dram_wavefront_detector_10M.md)
-DRAM_TRAFFIC = {"bytes_per_call": 18.807e9, "photons": 10_000_000,
-                "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 32 launches of one "
+DRAM_TRAFFIC = {"bytes_per_call": 12.723e9, "photons": 10_000_000,
+                "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the 12 launches of one "
                           "10M-photon simulate call of this workload (profiles/launches_dram_wavefront_detector_10M.md)"}
-# issue figures of the dominant kernel (k_wave_trace_df, 56 % of the step) from its ncu --set full
-# capture (profiles/k_wave_trace_df_detector_2M_ncu_full.md)
-ISSUE = {"kernel": "k_wave_trace_df", "share_of_step": 0.56, "issue_active": 0.376, "threads_per_warp_inst": 11.90,
-         "warps_active": 0.185, "lane_issue_frac": 0.376 * 11.90 / 32,
-         "source": "profiles/k_wave_trace_df_detector_2M_ncu_full.md"}
+# issue figures of the dominant kernel (k_wave_tail, 68 % of the step) from its ncu --set full
+# capture (profiles/k_wave_tail_detector_2M_ncu_full.md)
+ISSUE = {"kernel": "k_wave_tail", "share_of_step": 0.68, "issue_active": 0.387, "threads_per_warp_inst": 9.71,
+         "warps_active": 0.184, "lane_issue_frac": 0.387 * 9.71 / 32,
+         "source": "profiles/k_wave_tail_detector_2M_ncu_full.md"}
 
 
 def load_peaks():
@@ -85,23 +86,33 @@ def detector_workload(num_genstep, per_genstep, seed=0):
 
 
 class Clocks:
-    """nvidia-smi sampling during a timed region"""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    """nvidia-smi sampling around a timed region: the sampler starts before the warm-up (so it is
+    running when the region opens), every sample carries its time, and the summary keeps the
+    samples taken inside the region (window marked with begin/end)"""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 20
 
     def __init__(self, device):
         self.device = device
         self.p = None
+        self.t0 = self.t1 = None
         self.path = os.path.join(tempfile.gettempdir(), f"phx_bench_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", str(self.PERIOD_MS)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def __exit__(self, *a):
         if self.p:
@@ -117,15 +128,23 @@ class Clocks:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
         except Exception:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 10]
+
+        def when(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return None
+        if self.t0 is not None and self.t1 is not None:
+            rows = [r for r in rows if when(r) is not None and self.t0 <= when(r) <= self.t1]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "period_ms": self.PERIOD_MS}
 
 
 def stride_sample(gs, per_genstep=SAMPLE_PER_GENSTEP):
@@ -528,8 +547,6 @@ def relaunch(n):
 
 def check_ranks():
     """every rank joins a gloo group and sums its rank; rank 0 prints what it saw"""
-    import datetime
-
     import torch
     import torch.distributed as dist
     dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
@@ -544,7 +561,7 @@ def check_ranks():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--gensteps", type=int, default=1000)
@@ -586,7 +603,6 @@ def main():
     work_stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(work_stream)
     if world > 1:
-        import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     fd, lib, phys, gs = detector_workload(args.gensteps, args.per_genstep)
@@ -605,16 +621,14 @@ def main():
                                    hit_capacity=N if with_hits else 0, sensor_hits=sensor if with_hits else None, stream=sp)
 
     base_event = rank * 1000 + 1          # every rank simulates its own events (event > 0: jumped streams)
-    for w in range(args.warmup):
-        step(base_event + w)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     hits_total = 0
     with Clocks(local) as clk:
+        for w in range(args.warmup):
+            step(base_event + w)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
+        clk.begin()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         launches = 0
@@ -624,6 +638,7 @@ def main():
             launches += eng.last_call_stats()["kernel_launches"]
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.end()
         if world > 1:
             dist.barrier()
     ms = e0.elapsed_time(e1)
@@ -725,7 +740,7 @@ def main():
                            "photons_per_step": N, "outputs": "photon+seq+hits(SD)+sensor counts",
                            "l2": "inputs larger than L2 (RNG states 240 MB read + 960 MB written per step)",
                            "kernel": (f"wavefront: closest-hit and physics kernels over every photon of the event "
-                                      f"in flight, {rounds} rounds per step" if mode == 2 else
+                                      f"in flight, {rounds} rounds per step, then the tail kernel" if mode == 2 else
                                       "persistent work queue, block 64, refill every bounce"),
                            "parallelism": f"{world} independent event streams" if world > 1 else "1 GPU"},
                 "gpu_launches": launches,
@@ -735,7 +750,7 @@ def main():
                              "traffic_source": DRAM_TRAFFIC["source"] if mode == 2 else None,
                              "issue": ISSUE if mode == 2 else None,
                              "kernel_ms": k_ms,
-                             "kernel": ("k_wave_init + k_wave_trace_df/k_wave_shade rounds (whole simulate launch sequence)"
+                             "kernel": ("k_wave_init + 2 k_wave_trace_df/k_wave_shade rounds + k_wave_tail (whole simulate launch sequence)"
                                         if mode == 2 else "k_sim_persistent (whole simulate launch sequence)"),
                              "bytes_per_photon": bytes_per_photon, "peak_kind": f"{peak_kind} hbm_gbs",
                              "note": "issue/latency-bound divergent ray tracing + physics; HBM roof far from binding"},

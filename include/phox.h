@@ -83,13 +83,12 @@ typedef struct {
                                          slots until phx_destroy (or phx_trim) */
     int32_t  wave_refill;             /* wavefront closest-hit kernel: idle lanes a warp waits for before
                                          it takes new rays (1..32; 12) */
-    int32_t  wave_rounds;             /* wavefront loop of batched calls (phx_simulate_batched_device;
-                                         single-event calls always read the count): 0 = the host reads the live
-                                         count every few rounds and starts the tail kernel below
-                                         wave_tail paths; n > 0 = a fixed schedule of n rounds and then
-                                         the tail kernel for whatever is left, with no host read, so the
-                                         call is captured as a CUDA graph (use_graph) when every photon
-                                         of it is in flight at once (0) */
+    int32_t  wave_rounds;             /* wavefront schedule: n > 0 = n rounds and then the tail kernel
+                                         for whatever is left, with no host read (a batched call is then
+                                         captured as a CUDA graph, use_graph), when every photon of the
+                                         call is in flight at once; 0, or a call that refills slots =
+                                         the host reads the live count every few rounds and starts the
+                                         tail kernel below wave_tail paths (2) */
     int64_t  wave_tail;               /* live paths at or below which the tail kernel finishes them
                                          (host-read schedule; 262144) */
 } phx_config;

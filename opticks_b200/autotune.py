@@ -87,7 +87,7 @@ def tune_batched(engine, gs: np.ndarray, ev: np.ndarray, torch, reps: int = 2, s
 
 WAVE_REFILLS = (12,)
 WAVE_TAILS = (1 << 18,)                          # host-read schedule
-WAVE_ROUNDS = (12, 14, 16, 18, 20, 24)           # fixed schedule, graph-captured
+WAVE_ROUNDS = (2, 3, 4, 6, 8, 12, 16, 20)         # fixed schedule, graph-captured
 
 
 def tune_wavefront(engine, gs: np.ndarray, ev: np.ndarray, torch, reps: int = 1, sample_photons: int | None = None,

@@ -908,7 +908,7 @@ void phx_config_default(phx_config* c)
     c->use_graph = 1;
     c->wave_pool = 0;
     c->wave_refill = 12;
-    c->wave_rounds = 0;
+    c->wave_rounds = 2;
     c->wave_tail = 1 << 18;
 }
 
@@ -1246,9 +1246,14 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
     }
 }
 
-// Wavefront form (phx_wave.cuh): fill a pool of paths, then rounds of trace + shade launches
-// until no path is live.  The live count is read back every PHX_WAVE_ROUNDS rounds, so the call
-// synchronises the stream; it cannot be captured into a graph.
+// Wavefront form (phx_wave.cuh): fill a pool of paths, then rounds of trace + shade launches, then
+// the tail kernel for the paths still live.  When every photon of the call fits in the pool the
+// schedule is fixed (phx_config.wave_rounds rounds, 2 by default: the rounds that carry every path
+// through the scintillator and acrylic, where the wavefront's coherent launches pay; the longer,
+// divergent chains after them run faster in the tail kernel's registers than through the pool), with
+// no host read, so the call can be captured into a graph.  Otherwise (refill, or wave_rounds 0) the
+// live count is read back every PHX_WAVE_ROUNDS rounds and the tail kernel starts below
+// wave_tail paths; that call synchronises the stream.
 // Paths in flight: unless phx_config.wave_pool fixes the count, every photon of a call starts at
 // once (generation in one coherent pass, no refill) as long as its slots fit in half of the device
 // memory still free, and never fewer than PHX_WAVE_POOL slots start; a larger call refills slots
@@ -1279,7 +1284,9 @@ static long long wave_pool_for(const phx_engine* e, long long N, bool adj)
 // calls of at most this many photons get their event-advanced RNG states in one coherent pass
 // ahead of the loop (24 B per photon of scratch); larger ones advance each state as it starts
 #define PHX_EV_RNG_MAX (1LL << 26)
+#ifndef PHX_WAVE_ROUNDS
 #define PHX_WAVE_ROUNDS 4
+#endif
 
 template <typename K>
 static int wave_grid(K kernel, int dev, int* cache)
@@ -1294,7 +1301,7 @@ static int wave_grid(K kernel, int dev, int* cache)
 }
 
 template <int CV, bool ADJ = false>
-static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st, bool batched)
+static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
     static int g_init[128] = {}, g_trace[128] = {}, g_shade[128] = {}, g_fill[128] = {}, g_tail[128] = {};
     const int dev = e->device;
@@ -1340,7 +1347,7 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st, b
     W.live_bits = refill ? e->wlive.p : nullptr;
     PHX_CU(cudaGetLastError());
     int cur = 0;
-    if (batched && e->cfg.wave_rounds > 0 && !refill) {
+    if (e->cfg.wave_rounds > 0 && !refill) {
         // fixed schedule, no host read: wave_rounds rounds, then the tail kernel finishes whatever is
         // still live (it reads the count on the device; a grid-stride loop over any count), so the
         // whole call can be captured as a CUDA graph
@@ -1422,14 +1429,14 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st, b
 }
 
 template <bool ADJ = false>
-static int launch_wave_cv(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st, bool batched = false)
+static int launch_wave_cv(phx_engine* e, const PersistArgs& A, int cv, cudaStream_t st)
 {
-    PHX_CV_RETURN(cv, (launch_wave_t<CVK, ADJ>(e, A, st, batched)));
+    PHX_CV_RETURN(cv, (launch_wave_t<CVK, ADJ>(e, A, st)));
 }
 
-static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st, bool batched = false)
+static int launch_wave(phx_engine* e, const PersistArgs& A, cudaStream_t st)
 {
-    return launch_wave_cv(e, A, cv_of(e, e->cfg.root_polish != 0), st, batched);
+    return launch_wave_cv(e, A, cv_of(e, e->cfg.root_polish != 0), st);
 }
 
 template <int CV>
@@ -1804,7 +1811,7 @@ static int batched_enqueue(phx_engine* e, const PhxBatchCall& c, phx_photon* pho
         A.ev_rng_n = N;
     }
     if (N > 0) {
-        int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st, true) : launch_persistent(e, A, c.block, st);
+        int rc = e->cfg.kernel_mode == 2 ? launch_wave(e, A, st) : launch_persistent(e, A, c.block, st);
         if (rc) return rc;
     }
     if (want_hits && N > 0) {
