@@ -23,8 +23,9 @@ Also on the line:
                (16,777,216 rays vs the 15-node tree with torus, rays/s)
 
 --impl reference: the reference's CPU implementation of the path on the host cores, on the same
-stride sample.  Its qsim headers need glm/plog (absent) to build for the CPU, so the oracle port
-stands in (kind: port).
+stride sample: its own qsim/CSG headers compiled for the CPU under MOCK_CURAND with small GLM and
+plog stand-ins (oracle/_ref, kind: reference); the C restatement (kind: port) only where that
+build is absent.
 Multi-GPU (`--gpus N` re-launches itself under torch.distributed.run when WORLD_SIZE is unset):
 each rank simulates its own events (no data-path collective); value = photons of all ranks / max
 over ranks of the device time.  A second line item, `sharded`, splits one C3 event across the

@@ -91,6 +91,9 @@ typedef struct {
                                          tail kernel below wave_tail paths (2) */
     int64_t  wave_tail;               /* live paths at or below which the tail kernel finishes them
                                          (host-read schedule; 262144) */
+    int32_t  adj_wave_rounds;         /* wave_rounds of phx_adjoint_device calls (6): its tail kernel
+                                         carries the score terms and the tangent at 8 warps per SM,
+                                         so more bounces pay in the rounds than for plain calls */
 } phx_config;
 
 typedef struct {
@@ -122,7 +125,7 @@ int phx_destroy(phx_engine* e);
 int phx_trim(phx_engine* e, int64_t* bytes_released);
 
 /* Change the launch shape of later calls (no reference counterpart): kernel_mode, block, regroup,
- * chunk, use_graph, wave_pool, wave_refill, wave_rounds and wave_tail are taken from *cfg (a smaller
+ * chunk, use_graph, wave_pool, wave_refill, wave_rounds, wave_tail and adj_wave_rounds are taken from *cfg (a smaller
  * wave_pool takes effect when the engine's pool is next released or grown), every other field is
  * ignored.  None of them changes results (every loop form gives the same photons, seq and hits);
  * they are the knobs the autotuner sets. */

@@ -43,6 +43,7 @@ class PhxConfig(C.Structure):
         ("kernel_mode", C.c_int32), ("block", C.c_int32), ("regroup", C.c_int32), ("chunk", C.c_int32),
         ("use_graph", C.c_int32), ("wave_pool", C.c_int64),
         ("wave_refill", C.c_int32), ("wave_rounds", C.c_int32), ("wave_tail", C.c_int64),
+        ("adj_wave_rounds", C.c_int32),
     ]
 
 

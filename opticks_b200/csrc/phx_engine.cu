@@ -910,6 +910,7 @@ void phx_config_default(phx_config* c)
     c->wave_refill = 12;
     c->wave_rounds = 2;
     c->wave_tail = 1 << 18;
+    c->adj_wave_rounds = 6;
 }
 
 // the launch-shape fields a captured batched graph depends on, packed into one word
@@ -928,6 +929,8 @@ static int check_launch_config(const phx_config* c)
     if (c->wave_refill < 1 || c->wave_refill > 32) return phx_fail(-1, "wave_refill %d not in 1..32", c->wave_refill);
     if (c->wave_rounds < 0 || c->wave_rounds > 4096) return phx_fail(-1, "wave_rounds %d not in 0..4096", c->wave_rounds);
     if (c->wave_tail < 0) return phx_fail(-1, "wave_tail %lld is negative", (long long)c->wave_tail);
+    if (c->adj_wave_rounds < 0 || c->adj_wave_rounds > 4096)
+        return phx_fail(-1, "adj_wave_rounds %d not in 0..4096", c->adj_wave_rounds);
     return 0;
 }
 
@@ -984,6 +987,7 @@ int phx_set_launch_config(phx_engine* e, const phx_config* cfg)
     e->cfg.wave_rounds = cfg->wave_rounds;
     e->cfg.wave_tail = cfg->wave_tail;
     e->cfg.wave_pool = cfg->wave_pool;
+    e->cfg.adj_wave_rounds = cfg->adj_wave_rounds;
     return 0;
 }
 
@@ -1250,8 +1254,9 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // the tail kernel for the paths still live.  When every photon of the call fits in the pool the
 // schedule is fixed (phx_config.wave_rounds rounds, 2 by default: the rounds that carry every path
 // through the scintillator and acrylic, where the wavefront's coherent launches pay; the longer,
-// divergent chains after them run faster in the tail kernel's registers than through the pool), with
-// no host read, so the call can be captured into a graph.  Otherwise (refill, or wave_rounds 0) the
+// divergent chains after them run faster in the tail kernel's registers than through the pool;
+// adjoint passes take phx_config.adj_wave_rounds, 6 by default), with no host read, so the call can
+// be captured into a graph.  Otherwise (refill, or wave_rounds 0) the
 // live count is read back every PHX_WAVE_ROUNDS rounds and the tail kernel starts below
 // wave_tail paths; that call synchronises the stream.
 // Paths in flight: unless phx_config.wave_pool fixes the count, every photon of a call starts at
@@ -1347,11 +1352,12 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
     W.live_bits = refill ? e->wlive.p : nullptr;
     PHX_CU(cudaGetLastError());
     int cur = 0;
-    if (e->cfg.wave_rounds > 0 && !refill) {
+    const int rounds = ADJ ? e->cfg.adj_wave_rounds : e->cfg.wave_rounds;
+    if (rounds > 0 && !refill) {
         // fixed schedule, no host read: wave_rounds rounds, then the tail kernel finishes whatever is
         // still live (it reads the count on the device; a grid-stride loop over any count), so the
         // whole call can be captured as a CUDA graph
-        for (int r = 0; r < e->cfg.wave_rounds; r++) {
+        for (int r = 0; r < rounds; r++) {
             W.act_in = act[cur]; W.n_in = cnt[cur]; W.act_out = act[1 - cur]; W.n_out = cnt[1 - cur];
 #if PHX_WAVE_TRACE_DF
             k_wave_trace_df<CV><<<(unsigned)g_trace[dev], 128, 0, st>>>(W);
@@ -1364,9 +1370,9 @@ static int launch_wave_t(phx_engine* e, const PersistArgs& A, cudaStream_t st)
         W.act_in = act[cur]; W.n_in = cnt[cur];
         k_wave_tail<CV, ADJ><<<(unsigned)g_tail[dev], 128, 0, st>>>(W);
         PHX_CU(cudaGetLastError());
-        e->last_rounds = e->cfg.wave_rounds;
+        e->last_rounds = rounds;
         e->last_tail = 1;
-        e->last_wave_launches = 2 + 2LL * e->cfg.wave_rounds;
+        e->last_wave_launches = 2 + 2LL * rounds;
         return 0;
     }
     const long long max_rounds = (N / pool + 1) * (long long)(A.C.max_bounce + 1) + 2 * PHX_WAVE_ROUNDS;

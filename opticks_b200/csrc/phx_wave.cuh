@@ -521,6 +521,9 @@ __global__ void __launch_bounds__(128) k_wave_tail(WaveArgs W)
 #ifndef PHX_WAVE_SHADE_MINB
 #define PHX_WAVE_SHADE_MINB 7
 #endif
+#ifndef PHX_WAVE_SHADE_ADJ_MINB
+#define PHX_WAVE_SHADE_ADJ_MINB 1
+#endif
 
 // the physics of one path whose slot is in the warp's staging area; true when it goes on
 template <int CV, bool ADJ>
@@ -558,7 +561,7 @@ PHX_D bool wave_shade_path(const WaveArgs& W, const float4* st, uint32_t s, cons
 }
 
 template <int CV, bool ADJ = false>
-__global__ void __launch_bounds__(128, ADJ ? 1 : PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
+__global__ void __launch_bounds__(128, ADJ ? PHX_WAVE_SHADE_ADJ_MINB : PHX_WAVE_SHADE_MINB) k_wave_shade(WaveArgs W)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0 && W.trace_ctr) *W.trace_ctr = 0u;   // for the next round's closest-hit kernel
     const unsigned n = *W.n_in;

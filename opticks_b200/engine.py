@@ -116,7 +116,7 @@ class Engine:
             self._h = None
 
     LAUNCH_FIELDS = ("kernel_mode", "block", "regroup", "chunk", "use_graph", "wave_pool", "wave_refill", "wave_rounds",
-                     "wave_tail")
+                     "wave_tail", "adj_wave_rounds")
 
     def set_launch_config(self, **kw) -> None:
         """change the launch shape of later calls (fields of LAUNCH_FIELDS); results do not change"""
