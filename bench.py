@@ -473,6 +473,10 @@ def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=1
         return e0.elapsed_time(e1) / reps
 
     ms_adj = timed(lambda: ADJ.adjoint_device(eng, g, N, 7, theta0, mat_line, *wl, hits, grad, st.cuda_stream))
+    # the score-function estimator alone (every kind's score terms, the Fresnel branch probabilities
+    # included), without the refractive index's pathwise tangent
+    ms_adj_score = timed(lambda: ADJ.adjoint_device(eng, g, N, 7, theta0, mat_line, *wl, hits, grad, st.cuda_stream,
+                                                    pathwise=False))
     ms_fwd = timed(lambda: eng.simulate_device(g, N, 7, photon=photon, seq=seq, hit=hit, hit_capacity=N, stream=st.cuda_stream))
     ms_fwd_bare = timed(lambda: eng.simulate_device(g, N, 7, stream=st.cuda_stream))
 
@@ -525,6 +529,8 @@ def measure_adjoint(torch, E, fd, lib, phys, dev, num_genstep=100, per_genstep=1
     return {"workload": f"{N} photons from {num_genstep} scintillation gensteps, theta = 4 properties x 8 bins of LS over 300-620 nm",
             "adjoint_ms": ms_adj, "forward_ms_with_outputs": ms_fwd, "forward_ms_no_outputs": ms_fwd_bare,
             "adjoint_over_forward": ms_adj / ms_fwd, "adjoint_over_forward_no_outputs": ms_adj / ms_fwd_bare,
+            "adjoint_score_terms_only_ms": ms_adj_score, "adjoint_score_terms_only_over_forward": ms_adj_score / ms_fwd,
+            "adj_wave_rounds": int(eng.config.adj_wave_rounds),
             "fd": {"common_random_numbers": True,
                    "note": "rindex rows include the pathwise refraction term (tangent of the refracted direction "
                            "carried through later segments, Fresnel probabilities and Rayleigh densities; terms "
