@@ -910,7 +910,7 @@ void phx_config_default(phx_config* c)
     c->wave_refill = 12;
     c->wave_rounds = 2;
     c->wave_tail = 1 << 18;
-    c->adj_wave_rounds = 6;
+    c->adj_wave_rounds = 8;
 }
 
 // the launch-shape fields a captured batched graph depends on, packed into one word
@@ -1255,7 +1255,7 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // schedule is fixed (phx_config.wave_rounds rounds, 2 by default: the rounds that carry every path
 // through the scintillator and acrylic, where the wavefront's coherent launches pay; the longer,
 // divergent chains after them run faster in the tail kernel's registers than through the pool;
-// adjoint passes take phx_config.adj_wave_rounds, 6 by default), with no host read, so the call can
+// adjoint passes take phx_config.adj_wave_rounds, 8 by default), with no host read, so the call can
 // be captured into a graph.  Otherwise (refill, or wave_rounds 0) the
 // live count is read back every PHX_WAVE_ROUNDS rounds and the tail kernel starts below
 // wave_tail paths; that call synchronises the stream.

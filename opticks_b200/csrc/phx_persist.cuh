@@ -55,9 +55,17 @@ struct PersistArgs {
     const int* adj_prim_node;       // root node of each prim, for the tangent's probe intersections
 };
 
+// the block's shared score area (32 terms x PHX_SCORE_LANES threads, 16 KB), this thread's column
+PHX_D float* score_area()
+{
+    __shared__ float sg[32 * PHX_SCORE_LANES];
+    return sg + threadIdx.x;
+}
+
 // the adjoint accumulator's constant fields for one kernel
 PHX_D void score_setup(PhxScore& score, const PersistArgs& A)
 {
+    score.g = score_area();
     score.mat = A.adj_mat; score.nm0 = A.adj_nm0; score.nms = A.adj_nms;
     score.wl_lo = A.adj_wl_lo; score.binw = A.adj_binw;
     score.pathwise = A.adj_pathwise;
@@ -211,7 +219,7 @@ PHX_D void persist_start(PhxLane& L, const PersistArgs& A, long long idx, unsign
 {
     if (ADJ) {
 #pragma unroll
-        for (int k = 0; k < 32; k++) sc->g[k] = 0.f;
+        for (int k = 0; k < 32; k++) PHX_SG(*sc, k) = 0.f;
         score_tangent_reset(*sc);
     }
     const int gi = phx_find_genstep(A.gs_off, A.G, idx);
@@ -250,7 +258,7 @@ PHX_D void persist_finish(PhxLane& L, const PersistArgs& A, const PhxScore* sc)
             const unsigned s = id - 1u;
             atomicAdd(A.adj_hits + s, 1.0);
             for (int k = 0; k < 32; k++)
-                if (sc->g[k] != 0.f) atomicAdd(A.adj_grad + (size_t)s * 32 + k, (double)sc->g[k]);
+                if (PHX_SG(*sc, k) != 0.f) atomicAdd(A.adj_grad + (size_t)s * 32 + k, (double)PHX_SG(*sc, k));
         }
     }
     if (A.photon) phx_store_photon(A.photon + idx, L.p);
@@ -305,6 +313,7 @@ PHX_D bool persist_step(PhxLane& L, const PersistArgs& A, unsigned& status, PhxS
 template <int CV, int BLOCK, bool ADJ = false>
 __global__ void __launch_bounds__(BLOCK, PHX_PERSIST_MINB(BLOCK)) k_sim_persistent(PersistArgs A)
 {
+    static_assert(!ADJ || BLOCK <= PHX_SCORE_LANES, "score-carrying blocks hold at most PHX_SCORE_LANES threads");
     PhxScore score;
     if (ADJ) score_setup(score, A);
     PhxScore* sc = ADJ ? &score : nullptr;

@@ -80,8 +80,15 @@ struct PhxState {
 // polarisation with respect to nu, the parametrised index at the photon's current wavelength.
 // A hit point's tangent and the change of the surface normal come from a probe: the same prim
 // intersected along the ray moved a small step along the tangent.
+// The 32 score terms of a path live in shared memory, term-major with one word per thread of the
+// block (term k of thread t at word k * PHX_SCORE_LANES + t: a warp's accesses to one term hit 32
+// banks), not in the thread's local memory: they are indexed by wavelength bin at run time, and as
+// local memory (128 B of a 1.4 KB stack frame per thread, over 56k resident threads) every update
+// missed L1.  Kernels that carry scores run blocks of at most PHX_SCORE_LANES threads.
+#define PHX_SCORE_LANES 128
+#define PHX_SG(S, k) ((S).g[(k) * PHX_SCORE_LANES])
 struct PhxScore {
-    float g[32];
+    float* g;                  // this thread's first term in the block's shared score area
     unsigned mat;              // 1-based material index of the parametrised material
     float nm0, nms;            // texture wavelength domain
     float wl_lo, binw;         // bins [wl_lo + b binw, wl_lo + (b+1) binw), b < 8
@@ -115,8 +122,8 @@ PHX_D void score_add(PhxScore& S, int kind, float wl, float v)
     const float l0 = S.nm0 + f * S.nms, l1 = l0 + S.nms;
     const int b0 = (int)floorf((l0 - S.wl_lo) / S.binw);
     const int b1 = (int)floorf((l1 - S.wl_lo) / S.binw);
-    if (b0 >= 0 && b0 < 8) S.g[kind * 8 + b0] += (1.f - a) * v;
-    if (b1 >= 0 && b1 < 8) S.g[kind * 8 + b1] += a * v;
+    if (b0 >= 0 && b0 < 8) PHX_SG(S, kind * 8 + b0) += (1.f - a) * v;
+    if (b1 >= 0 && b1 < 8) PHX_SG(S, kind * 8 + b1) += a * v;
 }
 
 // a refractive-index term of the path: clipped at PHX_ADJ_SCORE_CAP (terms near the critical angle, at

@@ -174,7 +174,8 @@ PHX_D void wave_store_score(const WaveArgs& W, uint32_t s, const PhxScore* sc)
 {
     float4* o = W.score + PHX_WAVE_SCORE_F4 * (size_t)s;
 #pragma unroll
-    for (int k = 0; k < 8; k++) o[k] = make_float4(sc->g[4 * k], sc->g[4 * k + 1], sc->g[4 * k + 2], sc->g[4 * k + 3]);
+    for (int k = 0; k < 8; k++)
+        o[k] = make_float4(PHX_SG(*sc, 4 * k), PHX_SG(*sc, 4 * k + 1), PHX_SG(*sc, 4 * k + 2), PHX_SG(*sc, 4 * k + 3));
     o[8] = make_float4(sc->tpos.x, sc->tpos.y, sc->tpos.z, sc->tdir.x);
     o[9] = make_float4(sc->tdir.y, sc->tdir.z, sc->tpol.x, sc->tpol.y);
     o[10] = make_float4(sc->tpol.z, 0.f, 0.f, 0.f);
@@ -186,7 +187,7 @@ PHX_D void wave_load_score(const WaveArgs& W, uint32_t s, PhxScore* sc)
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         const float4 v = o[k];
-        sc->g[4 * k] = v.x; sc->g[4 * k + 1] = v.y; sc->g[4 * k + 2] = v.z; sc->g[4 * k + 3] = v.w;
+        PHX_SG(*sc, 4 * k) = v.x; PHX_SG(*sc, 4 * k + 1) = v.y; PHX_SG(*sc, 4 * k + 2) = v.z; PHX_SG(*sc, 4 * k + 3) = v.w;
     }
     const float4 a = o[8], b = o[9], c = o[10];
     sc->tpos = make_float3(a.x, a.y, a.z);

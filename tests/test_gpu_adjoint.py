@@ -136,6 +136,29 @@ def test_adjoint_wavefront_equals_persistent(det, pool):
     assert np.all(np.abs(out[0][1].sum(0) - out[1][1].sum(0)) <= 2e-3 * scale)
 
 
+@pytest.mark.parametrize("rounds", [0, 2])
+def test_adjoint_schedule_changes_no_result(det, rounds):
+    """adj_wave_rounds (8 by default) against the 2-round schedule and the host-read one: identical
+    hits, and score sums equal to float rounding (the adjoint step is inlined into the physics and
+    the tail kernels, whose fast-math contractions differ in the last bits of the pathwise terms:
+    about 1e-7 of a term's scale)"""
+    gs = scenes.detector_gensteps(6, 3000, seed=33, lib=det["lib"])
+    h0, j0 = _adj(det, gs, det["theta"], event=4)
+    eng = det["eng"]
+    default = int(eng.config.adj_wave_rounds)
+    assert default == int(det["E"].default_config().adj_wave_rounds) and default != rounds
+    try:
+        eng.set_launch_config(adj_wave_rounds=rounds)
+        h1, j1 = _adj(det, gs, det["theta"], event=4)
+        assert eng.last_call_stats()["wave_rounds"] >= (rounds if rounds else 1)
+    finally:
+        eng.set_launch_config(adj_wave_rounds=default)
+    np.testing.assert_array_equal(h0, h1)
+    assert h0.sum() > 500
+    scale = np.abs(j0).sum(0) + 1e-12
+    assert np.all(np.abs(j0.sum(0) - j1.sum(0)) <= 1e-5 * scale)
+
+
 def test_refractive_index_gradient_with_pathwise_term(det):
     """d(total hits)/d n in the bin holding the emission peak (420-460 nm): the pathwise tangent of the
     refracted direction carries most of it (the Fresnel score alone is a few per cent of it); the
