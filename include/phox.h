@@ -91,7 +91,7 @@ typedef struct {
                                          tail kernel below wave_tail paths (2) */
     int64_t  wave_tail;               /* live paths at or below which the tail kernel finishes them
                                          (host-read schedule; 262144) */
-    int32_t  adj_wave_rounds;         /* wave_rounds of phx_adjoint_device calls (8): its tail kernel
+    int32_t  adj_wave_rounds;         /* wave_rounds of phx_adjoint_device calls (12): its tail kernel
                                          carries the score terms and the tangent, so more bounces pay
                                          in the rounds than for plain calls */
 } phx_config;

@@ -115,6 +115,8 @@ struct phx_engine {
     std::vector<uint32_t> optical_host;
     cudaArray_t adj_arr = nullptr;
     cudaTextureObject_t adj_tex = 0;
+    float* adj_tab_h = nullptr;    // pinned staging of the adjoint's re-tabulated property table
+    cudaEvent_t adj_up = nullptr;  // recorded after its upload
     int num_wl = 0;
     // rng
     DevBuf<uint32_t> rng;
@@ -910,7 +912,7 @@ void phx_config_default(phx_config* c)
     c->wave_refill = 12;
     c->wave_rounds = 2;
     c->wave_tail = 1 << 18;
-    c->adj_wave_rounds = 8;
+    c->adj_wave_rounds = 12;
 }
 
 // the launch-shape fields a captured batched graph depends on, packed into one word
@@ -952,6 +954,8 @@ int phx_destroy(phx_engine* e)
     if (e->bnd_tex) cudaDestroyTextureObject(e->bnd_tex);
     if (e->adj_tex) cudaDestroyTextureObject(e->adj_tex);
     if (e->adj_arr) cudaFreeArray(e->adj_arr);
+    if (e->adj_up) cudaEventDestroy(e->adj_up);
+    if (e->adj_tab_h) cudaFreeHost(e->adj_tab_h);
     if (e->icdf_tex) cudaDestroyTextureObject(e->icdf_tex);
     if (e->bnd_arr) cudaFreeArray(e->bnd_arr);
     if (e->icdf_arr) cudaFreeArray(e->icdf_arr);
@@ -1255,7 +1259,7 @@ static int launch_persistent(phx_engine* e, const PersistArgs& A, int block, cud
 // schedule is fixed (phx_config.wave_rounds rounds, 2 by default: the rounds that carry every path
 // through the scintillator and acrylic, where the wavefront's coherent launches pay; the longer,
 // divergent chains after them run faster in the tail kernel's registers than through the pool;
-// adjoint passes take phx_config.adj_wave_rounds, 8 by default), with no host read, so the call can
+// adjoint passes take phx_config.adj_wave_rounds, 12 by default), with no host read, so the call can
 // be captured into a graph.  Otherwise (refill, or wave_rounds 0) the
 // live count is read back every PHX_WAVE_ROUNDS rounds and the tail kernel starts below
 // wave_tail paths; that call synchronises the stream.
@@ -1933,15 +1937,23 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
     cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
     const uint32_t mat = e->optical_host[(size_t)mat_line * 4];
     if (mat == 0) return phx_fail(-1, "phx_adjoint_device: line %d is not a material line", mat_line);
-    // re-tabulate every material line (omat/imat) of this material with theta, in 8 bins
+    // re-tabulate every material line (omat/imat) of this material with theta, in 8 bins, into a
+    // pinned staging copy of the table, once the previous call's upload from it has completed
     const float binw = (wl_hi - wl_lo) / 8.f;
-    std::vector<float> tab(e->bnd_host);
+    if (!e->adj_tab_h) {
+        PHX_CU(cudaMallocHost((void**)&e->adj_tab_h, e->bnd_host.size() * sizeof(float)));
+        PHX_CU(cudaEventCreateWithFlags(&e->adj_up, cudaEventDisableTiming));
+    } else {
+        PHX_CU(cudaEventSynchronize(e->adj_up));
+    }
+    float* const tab = e->adj_tab_h;
+    memcpy(tab, e->bnd_host.data(), e->bnd_host.size() * sizeof(float));
     const int nwl = e->num_wl;
     for (int b = 0; b < e->num_bnd; b++)
         for (int j = 0; j < 4; j += 3) {
             if (e->optical_host[(size_t)(4 * b + j) * 4] != mat) continue;
-            float* g0 = tab.data() + (size_t)((b * 4 + j) * 2 + 0) * nwl * 4;
-            float* g1 = tab.data() + (size_t)((b * 4 + j) * 2 + 1) * nwl * 4;
+            float* g0 = tab + (size_t)((b * 4 + j) * 2 + 0) * nwl * 4;
+            float* g1 = tab + (size_t)((b * 4 + j) * 2 + 1) * nwl * 4;
             for (int i = 0; i < nwl; i++) {
                 const float lam = e->nm0 + i * e->nms;
                 if (!(lam >= wl_lo && lam < wl_hi)) continue;
@@ -1954,11 +1966,13 @@ int phx_adjoint_device(phx_engine* e, const float* d_gensteps, int32_t num_genst
             }
         }
     if (!e->adj_arr) {
-        int rc = make_texture_f4(e->adj_arr, e->adj_tex, tab.data(), (int)e->nx, (int)e->ny);
+        int rc = make_texture_f4(e->adj_arr, e->adj_tex, tab, (int)e->nx, (int)e->ny);
         if (rc) return rc;
     } else {
-        PHX_CU(cudaMemcpy2DToArray(e->adj_arr, 0, 0, tab.data(), e->nx * sizeof(float4), e->nx * sizeof(float4), e->ny, cudaMemcpyHostToDevice));
+        PHX_CU(cudaMemcpy2DToArrayAsync(e->adj_arr, 0, 0, tab, e->nx * sizeof(float4), e->nx * sizeof(float4), e->ny,
+                                        cudaMemcpyHostToDevice, st));
     }
+    PHX_CU(cudaEventRecord(e->adj_up, st));
     int rc = ensure_rng(e, num_photon);
     if (rc) return rc;
     const int G = num_genstep;

@@ -138,7 +138,7 @@ def test_adjoint_wavefront_equals_persistent(det, pool):
 
 @pytest.mark.parametrize("rounds", [0, 2])
 def test_adjoint_schedule_changes_no_result(det, rounds):
-    """adj_wave_rounds (8 by default) against the 2-round schedule and the host-read one: identical
+    """adj_wave_rounds (12 by default) against the 2-round schedule and the host-read one: identical
     hits, and score sums equal to float rounding (the adjoint step is inlined into the physics and
     the tail kernels, whose fast-math contractions differ in the last bits of the pathwise terms:
     about 1e-7 of a term's scale)"""
