@@ -110,6 +110,17 @@ class Clocks:
         return self
 
     def begin(self):
+        # the timed region opens once the sampler has written its first row (nvidia-smi can take
+        # longer to start than the warm-up steps last); at most 5 s
+        deadline = time.time() + 5.0
+        while self.p is not None and self.p.poll() is None and time.time() < deadline:
+            try:
+                self.f.flush()
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
         self.t0 = time.time()
 
     def end(self):
